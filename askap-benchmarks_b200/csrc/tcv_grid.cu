@@ -1,0 +1,134 @@
+// tcv_grid.cu -- gridding (Benchmark::gridKernel, attic/tConvolveMPI/Benchmark.cc:125-155).
+//
+// Output-stationary tiles.  One CTA owns a 64 x 64 tile of the grid; each of its 8 warps owns a
+// 32-column x RH-row block with one accumulator per point held in registers (lane = column).
+// The CTA walks the tile's sample list (from the plan, ordered by w-plane/oversampling kernel),
+// staging sample records in shared memory; for each sample a warp whose block meets the
+// footprint reads the table rows it needs (32 consecutive entries per row: one coalesced
+// 256-byte load for the complex64 table) and accumulates data * C into its registers.  When the
+// list is done the tile is added into the grid with coalesced read-modify-writes.
+//
+// Every grid point has exactly one owner thread, so there are no atomics and the result is the
+// same on every run.  HBM traffic is the table entries each sample needs plus one read and one
+// write of each touched tile, instead of a read and a write of the grid per update.
+#include "tcv_internal.cuh"
+
+namespace tcv {
+namespace {
+
+constexpr int kTileW = 64;
+constexpr int kTileH = 64;
+constexpr int kRowsPerWarp = 16;
+constexpr int kWarps = (kTileW / 32) * (kTileH / kRowsPerWarp);
+constexpr int kThreads = kWarps * 32;
+constexpr int kChunk = kThreads;  // samples staged per round
+
+struct GridArgs {
+    int support, s, g_size, ntx;
+    float c_scale;
+};
+
+template <class Tab>
+__global__ void __launch_bounds__(kThreads, 3)
+grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
+                 const int32_t* __restrict__ iu, const int32_t* __restrict__ iv,
+                 const int32_t* __restrict__ coff, const uint32_t* __restrict__ order,
+                 const uint32_t* __restrict__ tile_start, const uint32_t* __restrict__ tile_count,
+                 float2* __restrict__ grid, GridArgs a)
+{
+    const int tile = blockIdx.x;
+    const uint32_t cnt = tile_count[tile];
+    if (cnt == 0) return;
+    const uint32_t start = tile_start[tile];
+    const int tx = tile % a.ntx, ty = tile / a.ntx;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bx0 = tx * kTileW + (warp % (kTileW / 32)) * 32;  // first column of this warp
+    const int gx = bx0 + lane;
+    const int gy0 = ty * kTileH + (warp / (kTileW / 32)) * kRowsPerWarp;
+    const int s = a.s;
+
+    __shared__ float4 sm_rec[kChunk];  // (data.re, data.im, first column, first row)
+    __shared__ int sm_coff[kChunk];
+
+    float2 acc[kRowsPerWarp];
+#pragma unroll
+    for (int r = 0; r < kRowsPerWarp; ++r) acc[r] = make_float2(0.f, 0.f);
+
+    for (uint32_t base = 0; base < cnt; base += kChunk) {
+        const int m = int(cnt - base < uint32_t(kChunk) ? cnt - base : uint32_t(kChunk));
+        __syncthreads();
+        if (threadIdx.x < m) {
+            const uint32_t k = order[start + base + threadIdx.x];
+            const float2 d = data[k];
+            sm_rec[threadIdx.x] = make_float4(d.x * a.c_scale, d.y * a.c_scale,
+                                              __int_as_float(iu[k] - a.support), __int_as_float(iv[k]));
+            sm_coff[threadIdx.x] = coff[k];
+        }
+        __syncthreads();
+        for (int j = 0; j < m; ++j) {
+            const float4 q = sm_rec[j];
+            const int fx = __float_as_int(q.z), fy = __float_as_int(q.w);
+            const int dy0 = gy0 - fy;  // footprint row of this warp's first row
+            if (dy0 >= s || dy0 + kRowsPerWarp <= 0) continue;   // warp-uniform
+            if (fx > bx0 + 31 || fx + s <= bx0) continue;          // warp-uniform
+            const int dx = gx - fx;
+            const bool colok = unsigned(dx) < unsigned(s);
+            const float2 dv = make_float2(q.x, q.y);
+            const typename Tab::elem* cp = ctab + (sm_coff[j] + dy0 * s + dx);
+#pragma unroll
+            for (int r = 0; r < kRowsPerWarp; ++r) {
+                if (colok && unsigned(dy0 + r) < unsigned(s)) {
+                    const float2 c = Tab::load(cp + r * s);
+                    cmac<Tab::kReal>(acc[r], dv, c);
+                }
+            }
+        }
+    }
+    if (gx < a.g_size) {
+#pragma unroll
+        for (int r = 0; r < kRowsPerWarp; ++r) {
+            const int gy = gy0 + r;
+            if (gy < a.g_size) {
+                float2* gp = grid + (size_t(gy) * a.g_size + gx);
+                float2 v = *gp;
+                v.x += acc[r].x;
+                v.y += acc[r].y;
+                *gp = v;
+            }
+        }
+    }
+}
+
+template <class Tab>
+tcv_status launch(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
+                  cudaStream_t st)
+{
+    const PlanGeom& g = p->g;
+    if (g.tw != kTileW || g.th != kTileH) return TCV_ERR_UNSUPPORTED;
+    const int ntiles = g.ntx * g.nty;
+    if (g.n == 0 || ntiles == 0) return TCV_OK;
+    GridArgs a{g.support, g.s, g.g_size, g.ntx, c_scale};
+    grid_tile_kernel<Tab><<<ntiles, kThreads, 0, st>>>(
+        data, static_cast<const typename Tab::elem*>(c), p->iu, p->iv, p->coff, p->vals[p->sel],
+        p->tile_start, p->tile_count, grid, a);
+    TCV_CUDA(cudaGetLastError());
+    return TCV_OK;
+}
+
+}  // namespace
+
+tcv_status launch_grid(const tcv_plan* p, const float2* data, const void* c, int c_type,
+                       float c_scale, float2* grid, cudaStream_t st)
+{
+    switch (c_type) {
+        case TCV_C_C64: return launch<TabC64>(p, data, c, c_scale, grid, st);
+        case TCV_C_R32: return launch<TabR32>(p, data, c, c_scale, grid, st);
+        case TCV_C_CBF16: return launch<TabCBF16>(p, data, c, c_scale, grid, st);
+        case TCV_C_RBF16: return launch<TabRBF16>(p, data, c, c_scale, grid, st);
+        case TCV_C_CF16: return launch<TabCF16>(p, data, c, c_scale, grid, st);
+        case TCV_C_RF16: return launch<TabRF16>(p, data, c, c_scale, grid, st);
+        default: return TCV_ERR_ARG;
+    }
+}
+
+}  // namespace tcv

@@ -1,0 +1,139 @@
+// tcv_internal.cuh -- shared device helpers and the plan layout of libtconvolve.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+#include <cstddef>
+
+#include "tconvolve.h"
+
+namespace tcv {
+
+// ------------------------------------------------------------------------------------------
+// Table loaders.  Every storage form returns the entry as (re, im) floats; the real forms
+// return im = 0 and tell the multiply-accumulate to skip the imaginary products, which gives
+// exactly the same result as the complex form on a table whose imaginary parts are zero
+// (fma(-d.im, 0, acc) == acc).
+// ------------------------------------------------------------------------------------------
+struct TabC64 {
+    static constexpr bool kReal = false;
+    using elem = float2;
+    __device__ __forceinline__ static float2 load(const elem* p) { return __ldg(p); }
+};
+struct TabR32 {
+    static constexpr bool kReal = true;
+    using elem = float;
+    __device__ __forceinline__ static float2 load(const elem* p) { return make_float2(__ldg(p), 0.f); }
+};
+struct TabCBF16 {
+    static constexpr bool kReal = false;
+    using elem = uint32_t;  // (re, im) bfloat16 pair, re in the low half
+    __device__ __forceinline__ static float2 load(const elem* p)
+    {
+        const uint32_t u = __ldg(p);
+        return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
+    }
+};
+struct TabRBF16 {
+    static constexpr bool kReal = true;
+    using elem = uint16_t;
+    __device__ __forceinline__ static float2 load(const elem* p)
+    {
+        const uint32_t u = __ldg(p);
+        return make_float2(__uint_as_float(u << 16), 0.f);
+    }
+};
+struct TabCF16 {
+    static constexpr bool kReal = false;
+    using elem = __half2;
+    __device__ __forceinline__ static float2 load(const elem* p) { return __half22float2(__ldg(p)); }
+};
+struct TabRF16 {
+    static constexpr bool kReal = true;
+    using elem = __half;
+    __device__ __forceinline__ static float2 load(const elem* p) { return make_float2(__half2float(__ldg(p)), 0.f); }
+};
+
+// acc += a * b (complex), FP32 fused multiply-adds.  With a real table (b.y == 0 by construction)
+// only the two real-by-complex products are issued.
+template <bool kReal>
+__device__ __forceinline__ void cmac(float2& acc, const float2 a, const float2 b)
+{
+    acc.x = fmaf(a.x, b.x, acc.x);
+    acc.y = fmaf(a.y, b.x, acc.y);
+    if (!kReal) {
+        acc.x = fmaf(-a.y, b.y, acc.x);
+        acc.y = fmaf(a.x, b.y, acc.y);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Plan: binning of samples into grid tiles (gridding) and anchor tiles (degridding).
+// ------------------------------------------------------------------------------------------
+struct PlanGeom {
+    int64_t n;          // samples
+    int support, s;     // support, sSize = 2*support+1
+    int g_size;
+    int64_t c_len;      // table entries
+    int kid_bits;       // bits of the kernel index cOffset / sSize^2
+    // gridding: output-stationary tiles
+    int tw, th, ntx, nty, max_tiles;   // max_tiles = tiles one footprint can touch
+    int tile_bits, key_bits;
+    // degridding: anchor tiles (footprint top-left corner), tile + halo staged in shared memory
+    int ta, natx, naty, atile_bits, akey_bits;
+    int box_w, box_h;   // staged region (elements), box_w even
+    int degrid_mode;    // 0 staged (TMA), 1 direct from global
+    int degrid_parts;   // warps sharing one sample's footprint in the staged kernel
+    bool key64;         // 64-bit sort keys
+};
+
+}  // namespace tcv
+
+struct tcv_plan {
+    tcv::PlanGeom g;
+    const int32_t *iu, *iv, *coff;  // the sample arrays the plan was built from (device)
+    // device arrays inside the caller's workspace
+    void* keys[2];                 // grid pair keys (double buffer), n * max_tiles
+    uint32_t* vals[2];             // grid pair sample indices
+    void* akeys[2];                // anchor keys, n
+    uint32_t* avals[2];            // anchor sample indices
+    uint32_t* tile_count;          // ntx*nty
+    uint32_t* tile_start;
+    uint32_t* atile_count;         // natx*naty
+    uint32_t* atile_start;
+    unsigned long long* rejected;  // samples left out as out of bounds
+    unsigned int* status;          // device status word: bit 0 = a bounded wait timed out
+    void* cub_temp;
+    size_t cub_bytes;
+    int sel;                       // which buffer holds the sorted grid pairs
+    int asel;                      // which buffer holds the sorted anchor pairs
+};
+
+namespace tcv {
+
+// Host helpers implemented in tcv_plan.cu / tcv_api.cu
+PlanGeom make_geom(int64_t n, int support, int g_size, int64_t c_len);
+size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out);
+
+// Launchers implemented in tcv_grid.cu / tcv_degrid.cu
+tcv_status launch_grid(const tcv_plan* p, const float2* data, const void* c, int c_type,
+                       float c_scale, float2* grid, cudaStream_t st);
+tcv_status launch_degrid(const tcv_plan* p, const float2* grid, const void* c, int c_type,
+                         float c_scale, float2* out, cudaStream_t st);
+
+inline tcv_status cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return TCV_OK;
+    if (e == cudaErrorMemoryAllocation) return TCV_ERR_OOM;
+    return TCV_ERR_CUDA;
+}
+
+}  // namespace tcv
+
+#define TCV_CUDA(call)                                         \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return ::tcv::cuda_status(_e);  \
+    } while (0)

@@ -1,0 +1,12 @@
+"""tconvolve -- B200 (sm_100a) W-projection gridding and degridding behind the reference's
+Benchmark interface (attic/tConvolveMPI/Benchmark.h).
+
+The computation is in libtconvolve.so (C ABI: include/tconvolve.h); this package is the host-side
+mirror of the reference interface plus thin torch wrappers of the raw entry points.
+"""
+from ._lib import (C64, R32, CBF16, RBF16, CF16, RF16, CTYPE_BY_NAME, CTYPE_NAMES, TcvError,
+                   build, lib, LIB_PATH, BUILD_DIR)
+from .benchmark import Benchmark
+
+__all__ = ["Benchmark", "TcvError", "build", "lib", "C64", "R32", "CBF16", "RBF16", "CF16", "RF16",
+           "CTYPE_BY_NAME", "CTYPE_NAMES", "LIB_PATH", "BUILD_DIR"]

@@ -1,0 +1,155 @@
+"""ctypes binding of libtconvolve.so (the C ABI declared in include/tconvolve.h).
+
+The library is the only implementation: if it is missing or fails to load, every call raises.
+There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BUILD_DIR = os.path.join(PKG_ROOT, "_build")
+CSRC_DIR = os.path.join(PKG_ROOT, "csrc")
+LIB_PATH = os.path.join(BUILD_DIR, "libtconvolve.so")
+
+TCV_OK = 0
+STATUS_NAMES = {
+    0: "TCV_OK", 1: "TCV_ERR_ARG", 2: "TCV_ERR_BOUNDS", 3: "TCV_ERR_OOM", 4: "TCV_ERR_CUDA",
+    5: "TCV_ERR_TIMEOUT", 6: "TCV_ERR_STATE", 7: "TCV_ERR_WORKSPACE", 8: "TCV_ERR_UNSUPPORTED",
+}
+
+# table storage types (tcv_ctype)
+C64, R32, CBF16, RBF16, CF16, RF16 = range(6)
+CTYPE_NAMES = {C64: "c64", R32: "r32", CBF16: "cbf16", RBF16: "rbf16", CF16: "cf16", RF16: "rf16"}
+CTYPE_BY_NAME = {v: k for k, v in CTYPE_NAMES.items()}
+
+
+class TcvError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)}")
+
+
+class TcvConfig(ctypes.Structure):
+    _fields_ = [
+        ("n_samples", ctypes.c_int64),
+        ("w_size", ctypes.c_int32),
+        ("n_chan", ctypes.c_int32),
+        ("g_size", ctypes.c_int32),
+        ("baseline", ctypes.c_int32),
+        ("cell_size", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+        ("c_type", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class TcvDeviceBuffers(ctypes.Structure):
+    _fields_ = [
+        ("data", ctypes.c_void_p), ("outdata", ctypes.c_void_p), ("grid", ctypes.c_void_p),
+        ("c64", ctypes.c_void_p), ("c_active", ctypes.c_void_p), ("iu", ctypes.c_void_p),
+        ("iv", ctypes.c_void_p), ("coff", ctypes.c_void_p), ("u", ctypes.c_void_p),
+        ("v", ctypes.c_void_p), ("w", ctypes.c_void_p), ("plan", ctypes.c_void_p),
+        ("c_scale", ctypes.c_float), ("c_type", ctypes.c_int32),
+    ]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_F = ctypes.c_float
+_S = ctypes.c_size_t
+_PP = ctypes.POINTER(ctypes.c_void_p)
+
+# name -> (restype, argtypes); every symbol declared in include/tconvolve.h
+SIGNATURES = {
+    "tcv_status_string": (ctypes.c_char_p, [_I]),
+    "tcv_ctype_bytes": (_S, [_I]),
+    "tcv_version": (ctypes.c_char_p, []),
+    "tcv_c_geometry": (_I, [_D, _D, _I, _I, _P, _P, _P, _P]),
+    "tcv_init_c_scratch_bytes": (_S, []),
+    "tcv_init_c_raw": (_I, [_D, _D, _I, _I, _P, _P, _P, _P]),
+    "tcv_convert_c": (_I, [_P, _I64, _I, _P, _P, _P, _P]),
+    "tcv_init_uvw_raw": (_I, [_I64, _I, ctypes.c_uint64, _P, _P, _P, _P]),
+    "tcv_init_offsets_raw": (_I, [_P, _P, _P, _I64, _P, _I, _D, _D, _I, _I, _I, _I, _P, _P, _P, _P]),
+    "tcv_plan_workspace_bytes": (_S, [_I64, _I, _I, _I64]),
+    "tcv_plan_build": (_I, [_PP, _P, _P, _P, _I64, _I, _I, _I64, _P, _S, _P]),
+    "tcv_plan_grid": (_I, [_P, _P, _P, _I, _F, _P, _P]),
+    "tcv_plan_degrid": (_I, [_P, _P, _P, _I, _F, _P, _P]),
+    "tcv_plan_rejected": (_I, [_P, _P, _P]),
+    "tcv_plan_status": (_I, [_P, _P]),
+    "tcv_plan_info": (_I, [_P, _P, _P, _P, _P, _P]),
+    "tcv_plan_destroy": (None, [_P]),
+    "tcv_grid_raw": (_I, [_P, _I64, _I, _P, _I, _F, _I64, _P, _P, _P, _P, _I, _P, _S, _P]),
+    "tcv_degrid_raw": (_I, [_P, _I, _I, _P, _I, _F, _I64, _P, _P, _P, _P, _I64, _P, _S, _P]),
+    "tcv_grid_host_raw": (_I, [_P, _I64, _I, _P, _I64, _P, _P, _P, _P, _I, _I, _P]),
+    "tcv_degrid_host_raw": (_I, [_P, _I, _I, _P, _I64, _P, _P, _P, _P, _I64, _I, _P]),
+    "tcv_init_c_host": (_I, [_D, _D, _I, _I, _P, _I64, _I, _P, _P, _P, _P]),
+    "tcv_config_default": (None, [_P]),
+    "tcv_create": (_I, [_P, _PP]),
+    "tcv_destroy": (None, [_P]),
+    "tcv_last_error": (ctypes.c_char_p, [_P]),
+    "tcv_set_stream": (_I, [_P, _P]),
+    "tcv_get_stream": (_P, [_P]),
+    "tcv_sync": (_I, [_P]),
+    "tcv_init": (_I, [_P]),
+    "tcv_run_grid": (_I, [_P]),
+    "tcv_run_degrid": (_I, [_P]),
+    "tcv_support": (_I, [_P]),
+    "tcv_over_sample": (_I, [_P]),
+    "tcv_w_cell_size": (_D, [_P]),
+    "tcv_sum_c": (_F, [_P]),
+    "tcv_c_len": (_I64, [_P]),
+    "tcv_n_data": (_I64, [_P]),
+    "tcv_updates_per_pass": (_D, [_P]),
+    "tcv_set_ctype": (_I, [_P, _I]),
+    "tcv_set_data": (_I, [_P, _P, _I64]),
+    "tcv_get_data": (_I, [_P, _P, _I64]),
+    "tcv_get_outdata": (_I, [_P, _P, _I64]),
+    "tcv_set_grid": (_I, [_P, _P]),
+    "tcv_get_grid": (_I, [_P, _P]),
+    "tcv_zero_grid": (_I, [_P]),
+    "tcv_get_c": (_I, [_P, _P, _I64]),
+    "tcv_get_offsets": (_I, [_P, _P, _P, _P]),
+    "tcv_get_uvw": (_I, [_P, _P, _P, _P]),
+    "tcv_set_uvw": (_I, [_P, _P, _P, _P]),
+    "tcv_get_device_buffers": (_I, [_P, _P]),
+}
+
+_lib = None
+
+
+def build(quiet: bool = True) -> str:
+    """Compile the CUDA library and host programs for sm_100a (make in csrc/)."""
+    cmd = ["make", "-C", CSRC_DIR, f"-j{min(8, os.cpu_count() or 1)}"]
+    if quiet:
+        cmd.insert(1, "-s")
+    subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library.  Raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libtconvolve.so not built ({LIB_PATH}); run build() first")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int, what: str, ctx=None) -> None:
+    if status != TCV_OK:
+        extra = ""
+        if ctx:
+            msg = lib().tcv_last_error(ctx)
+            extra = f" ({msg.decode()})" if msg else ""
+        raise TcvError(status, what + extra)

@@ -1,0 +1,77 @@
+"""Problem definitions of the tConvolve benchmark and the synthetic visibility generator.
+
+Named problems (the constants of attic/tConvolveMPI/Benchmark.h:39-46):
+
+    c2  the reference default: 160000 samples, 33 w-planes, 4096^2 grid, 5 wavelength cells,
+        2000 m baseline (support 64, 129^2 footprint, 2.66e9 updates per pass)
+    c1  the CPU-sized case: 16000 samples, 9 w-planes, 1024^2 grid, 5 arcsec cells
+        (1/(1024 * 5 arcsec) = 40.286 wavelengths; support 22, 45^2 footprint)
+    g1, g2  small test problems (support 10 and 14; g2 has 4 channels)
+
+Visibilities: the reference sets every sample to 1+0i (Benchmark.cc:76-79).  The N(0,1) form
+draws real then imaginary parts as float32 standard normals from numpy's PCG64 generator seeded
+with `seed` (normal_vis), so every consumer sees the same bytes.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, replace
+
+import numpy as np
+
+ARCSEC_CELL_1024 = 1.0 / (1024 * 5.0 * math.pi / 648000.0)
+
+
+@dataclass(frozen=True)
+class Problem:
+    name: str
+    n_samples: int
+    w_size: int
+    n_chan: int
+    g_size: int
+    cell_size: float
+    baseline: int = 2000
+    seed: int = 0
+
+    @property
+    def freq0(self) -> float:
+        return 1.4e9 / 2.998e8
+
+    def support(self) -> int:
+        return int(1.5 * math.sqrt(abs(self.baseline) * self.cell_size * self.freq0) / self.cell_size)
+
+    def s_size(self) -> int:
+        return 2 * self.support() + 1
+
+    def n_data(self) -> int:
+        return self.n_samples * self.n_chan
+
+    def updates_per_pass(self) -> float:
+        return float(self.n_data()) * self.s_size() ** 2
+
+    def kwargs(self) -> dict:
+        return dict(n_samples=self.n_samples, w_size=self.w_size, n_chan=self.n_chan,
+                    g_size=self.g_size, cell_size=self.cell_size, baseline=self.baseline,
+                    seed=self.seed)
+
+    def with_(self, **kw) -> "Problem":
+        return replace(self, **kw)
+
+
+PROBLEMS = {
+    "g1": Problem("g1", 200, 5, 1, 128, 200.0),
+    "g2": Problem("g2", 1000, 9, 4, 256, 100.0),
+    "c1": Problem("c1", 16000, 9, 1, 1024, ARCSEC_CELL_1024),
+    "c2": Problem("c2", 160000, 33, 1, 4096, 5.0),
+}
+
+
+def normal_vis(n: int, seed: int) -> np.ndarray:
+    """n complex64 visibilities with N(0,1) real and imaginary parts (PCG64(seed))."""
+    rng = np.random.default_rng(seed)
+    re = rng.standard_normal(n, dtype=np.float32)
+    im = rng.standard_normal(n, dtype=np.float32)
+    out = np.empty(n, np.complex64)
+    out.real = re
+    out.imag = im
+    return out

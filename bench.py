@@ -1,0 +1,434 @@
+#!/usr/bin/env python
+"""Benchmark: tConvolve W-projection gridding + degridding on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--form c64|r32|...]
+
+Workload: the reference's default problem (attic/tConvolveMPI/Benchmark.h:39-46): 160000 samples,
+33 w-planes, 4096^2 grid, 5-wavelength cells, support 64 (129^2 footprints), u,v,w from the
+reference generator, N(0,1) complex64 visibilities.  One step = one binning plan (device sort of
+this batch's samples) + one gridding pass + one degridding pass (2 x 2.66e9 updates).
+
+Multi-GPU: one process per GPU, each an independent replica of the workload (the reference's MPI
+ranks are replicas that only meet at barriers); value = all ranks' updates / max-over-ranks time.
+
+Prints one JSON line (rank 0).  The `reference` arm times the reference's own CPU code
+(attic/tConvolveMPI/Benchmark.cc compiled from source into oracle/_ref) on the host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "askap-benchmarks_b200"))
+
+from tconvolve.workload import PROBLEMS, normal_vis  # noqa: E402
+
+METRIC = "grid+degrid updates/s at rel-L2<=1e-5"
+UNIT = "updates/s"
+VIS_SEED = 1234
+ALG_BYTES = {"grid": 24, "degrid": 16}  # per update: C 8 + grid read 8 (+ grid write 8)
+FALLBACK_HBM_GBS = 6650.0
+L2_FLUSH_BYTES = 512 << 20
+REF_DRIVER = os.path.join(REPO, "oracle", "_ref", "c2", "ref_driver")
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--workload", default="c2", choices=sorted(PROBLEMS))
+    p.add_argument("--form", default="c64", help="table storage form (c64 = plain FP32)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=4.0, help="target wall time of the CPU sample")
+    return p.parse_args()
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU reference timing (oracle/_ref: the reference's Benchmark.cc built from source)
+# ------------------------------------------------------------------------------------------------
+def run_reference_cpu(threads: int, per_thread: int, steps: int, warmup: int):
+    if not os.path.exists(REF_DRIVER):
+        raise RuntimeError(f"reference build missing: {REF_DRIVER}")
+    out = subprocess.run([REF_DRIVER, "time", str(threads), str(per_thread), str(steps), str(warmup)],
+                         check=True, capture_output=True, text=True).stdout
+    rates, step_s = [], []
+    for line in out.splitlines():
+        if line.startswith("step "):
+            f = line.split()
+            g, d, u = float(f[3]), float(f[5]), float(f[7])
+            rates.append(2 * u / (g + d))
+            step_s.append(g + d)
+    return rates, step_s
+
+
+def cpu_sample_size(threads: int, seconds: float) -> int:
+    # about 3e8 updates/s per core for the reference loop; 16641 updates per sample per pass, 2 passes
+    per = int(seconds * 3e8 / (2 * 16641))
+    return max(200, min(per, 160000))
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = host_threads()
+    per_thread = cpu_sample_size(threads, 1.0)
+    rates, step_s = run_reference_cpu(threads, per_thread, args.steps, args.warmup)
+    value = statistics.mean(rates)
+    prob = PROBLEMS[args.workload]
+    sample = (f"{threads} thread replicas x first {per_thread} samples of the {args.workload} workload, "
+              f"reference gridKernel then degridKernel per step (tConvolveMT-style)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * statistics.mean(step_s), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (reference generator, vis = 1+0i)",
+        "config": {"workload": f"{args.workload}: {prob.n_samples} samples, gSize {prob.g_size}, "
+                               f"wSize {prob.w_size}, support {prob.support()}",
+                   "form": "reference CPU (std::complex<float>)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch from the committed ncu summary (profiles/), or None."""
+    path = os.path.join(REPO, "profiles", f"{kernel}_c2_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------------------------------------
+# B200 arm
+# ------------------------------------------------------------------------------------------------
+def b200_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import tconvolve
+    from tconvolve import raw
+    from tconvolve._lib import check, lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local))
+    prob = PROBLEMS[args.workload]
+    form = tconvolve.CTYPE_BY_NAME[args.form]
+    n = prob.n_data()
+    stream = torch.cuda.Stream()  # a non-default stream: every launch and event below goes to it
+    torch.cuda.set_stream(stream)
+
+    b = tconvolve.Benchmark(**prob.kwargs(), device=local)
+    b.set_stream(stream.cuda_stream)
+    b.init()
+    if form != tconvolve.C64:
+        b.set_ctype(form)
+    vis = normal_vis(n, VIS_SEED)
+    b.set_data(vis)
+    b.sync()
+    bufs = b.device_buffers()
+    support = b.getSupport()
+    updates = b.updates_per_pass()
+    c_len = b.c_len
+    L = lib()
+    wbytes = L.tcv_plan_workspace_bytes(n, support, prob.g_size, c_len)
+    work = torch.empty(wbytes, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    P = ctypes.c_void_p
+
+    def step(evs=None):
+        sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)  # the capture stream too
+        plan = ctypes.c_void_p()
+        if evs:
+            evs[0].record(stream)
+        check(L.tcv_plan_build(ctypes.byref(plan), P(bufs.iu), P(bufs.iv), P(bufs.coff), n, support,
+                               prob.g_size, c_len, P(work.data_ptr()), wbytes, sp), "plan")
+        if evs:
+            evs[1].record(stream)
+        check(L.tcv_plan_grid(plan, P(bufs.data), P(bufs.c_active), bufs.c_type, bufs.c_scale,
+                              P(bufs.grid), sp), "grid")
+        if evs:
+            evs[2].record(stream)
+        check(L.tcv_plan_degrid(plan, P(bufs.grid), P(bufs.c_active), bufs.c_type, bufs.c_scale,
+                                P(bufs.outdata), sp), "degrid")
+        if evs:
+            evs[3].record(stream)
+        L.tcv_plan_destroy(plan)
+
+    # kernels launched by one step, counted from a CUDA-graph capture of it
+    step()
+    torch.cuda.synchronize()
+    launches_per_step = count_step_kernels(torch, step)
+
+    for _ in range(args.warmup):
+        step()
+        flush.zero_()
+    torch.cuda.synchronize()
+
+    gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    clocks = ClockSampler(gpu_uuid)
+    clocks.start()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_wall0 = time.perf_counter()
+    for k in range(args.steps):
+        step(evs[k])
+        flush.zero_()  # L2 flush between timed steps (outside the events)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t_wall = time.perf_counter() - t_wall0
+    plan_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    grid_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    degrid_ms = [e[2].elapsed_time(e[3]) for e in evs]
+    step_ms = [e[0].elapsed_time(e[3]) for e in evs]
+
+    # e2e: the same step through the C ABI with host buffers: H2D of the batch's samples from
+    # pinned memory, plan, grid, degrid, D2H of the degridded visibilities, every step
+    iu_h, iv_h, co_h = b.offsets()
+    h_vis = torch.from_numpy(vis).pin_memory()
+    h_iu = torch.from_numpy(iu_h).pin_memory()
+    h_iv = torch.from_numpy(iv_h).pin_memory()
+    h_co = torch.from_numpy(co_h).pin_memory()
+    h_out = torch.empty(n, dtype=torch.complex64).pin_memory()
+    d_vis = torch.empty(n, dtype=torch.complex64, device="cuda")
+    d_iu = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_iv = torch.empty_like(d_iu)
+    d_co = torch.empty_like(d_iu)
+    d_out = torch.empty(n, dtype=torch.complex64, device="cuda")
+
+    def e2e_step():
+        d_vis.copy_(h_vis, non_blocking=True)
+        d_iu.copy_(h_iu, non_blocking=True)
+        d_iv.copy_(h_iv, non_blocking=True)
+        d_co.copy_(h_co, non_blocking=True)
+        plan = ctypes.c_void_p()
+        check(L.tcv_plan_build(ctypes.byref(plan), P(d_iu.data_ptr()), P(d_iv.data_ptr()),
+                               P(d_co.data_ptr()), n, support, prob.g_size, c_len,
+                               P(work.data_ptr()), wbytes, sp), "plan")
+        check(L.tcv_plan_grid(plan, P(d_vis.data_ptr()), P(bufs.c_active), bufs.c_type, bufs.c_scale,
+                              P(bufs.grid), sp), "grid")
+        check(L.tcv_plan_degrid(plan, P(bufs.grid), P(bufs.c_active), bufs.c_type, bufs.c_scale,
+                                P(d_out.data_ptr()), sp), "degrid")
+        h_out.copy_(d_out, non_blocking=True)
+        L.tcv_plan_destroy(plan)
+
+    for _ in range(args.warmup):
+        e2e_step()
+        flush.zero_()
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for _ in range(max(args.steps // 4, 3)):
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e2e_step()
+        z.record(stream)
+        z.synchronize()  # the result is on the host when the step ends
+        e2e_ms.append(a.elapsed_time(z))
+        flush.zero_()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if int(torch.count_nonzero(torch.isnan(torch.view_as_real(h_out)))) != 0:
+        raise RuntimeError("non-finite degridded output")
+
+    # max over ranks of the device time
+    mean_step = statistics.mean(step_ms)
+    e2e_mean = statistics.mean(e2e_ms)
+    if world > 1:
+        t = torch.tensor([mean_step, e2e_mean, t_wall], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        mean_step, e2e_mean, t_wall = (float(x) for x in t.tolist())
+    value = world * 2 * updates / (mean_step * 1e-3)
+    e2e_value = world * 2 * updates / (e2e_mean * 1e-3)
+
+    g_ms, d_ms = statistics.mean(grid_ms), statistics.mean(degrid_ms)
+    dom = "grid" if g_ms >= d_ms else "degrid"
+    dom_ms = max(g_ms, d_ms)
+    peak, peak_kind = measured_hbm_peak()
+    achieved = ALG_BYTES[dom] * updates / (dom_ms * 1e-3) / 1e9
+    traffic = ncu_traffic(dom)
+    kname = {"grid": "grid_tile_kernel", "degrid": "degrid_staged_kernel"}[dom]
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mean_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": f"synthetic: reference generator u,v,w (seed 0); N(0,1) complex64 visibilities "
+                    f"(PCG64 seed {VIS_SEED})",
+            "config": {"workload": f"{args.workload}: {prob.n_samples} samples x {prob.n_chan} chan, "
+                                   f"gSize {prob.g_size}, wSize {prob.w_size}, support {support} "
+                                   f"({2 * support + 1}^2 footprint), cellSize {prob.cell_size}",
+                       "form": args.form, "parallelism": f"replicas x{world}",
+                       "l2": f"{L2_FLUSH_BYTES >> 20} MiB buffer written between timed steps",
+                       "step": "binning plan + gridding pass + degridding pass"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": kname,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",
+                         "alg_bytes_per_update": ALG_BYTES[dom], "launch_ms": dom_ms},
+            "kernels": {"plan_ms": statistics.mean(plan_ms), "grid_ms": g_ms, "degrid_ms": d_ms,
+                        "grid_alg_GBps": ALG_BYTES["grid"] * updates / (g_ms * 1e-3) / 1e9,
+                        "degrid_alg_GBps": ALG_BYTES["degrid"] * updates / (d_ms * 1e-3) / 1e9,
+                        "grid_updates_per_s": updates / (g_ms * 1e-3),
+                        "degrid_updates_per_s": updates / (d_ms * 1e-3)},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * (8 + 4 * 3),
+                    "d2h_bytes_per_step": n * 8, "ms_per_step": e2e_mean},
+            "gpu_launches": launches_per_step * args.steps if launches_per_step else None,
+            "launches_per_step": launches_per_step,
+            "wall_s_timed_loop": t_wall,
+            "clocks": clk,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    b.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def count_step_kernels(torch, step):
+    """Kernel nodes in a CUDA-graph capture of one step (0 if capture is unavailable)."""
+    try:
+        import cuda.bindings.runtime as rt
+    except ImportError:
+        return 0
+    g = torch.cuda.CUDAGraph(keep_graph=True)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.graph(g, stream=s):
+        step()
+    torch.cuda.synchronize()
+    handle = g.raw_cuda_graph()
+    err, _, count = rt.cudaGraphGetNodes(handle, 0)
+    err, nodes, count = rt.cudaGraphGetNodes(handle, count)
+    kernels = 0
+    for nd in nodes:
+        err, t = rt.cudaGraphNodeGetType(nd)
+        if t == rt.cudaGraphNodeType.cudaGraphNodeTypeKernel:
+            kernels += 1
+    del g
+    return kernels
+
+
+def cpu_baseline(args):
+    threads = host_threads()
+    per_thread = cpu_sample_size(threads, args.cpu_seconds)
+    try:
+        rates, _ = run_reference_cpu(threads, per_thread, 1, 0)
+        return {"value": rates[0], "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"{threads} thread replicas x first {per_thread} samples of the workload, "
+                          f"one gridKernel + degridKernel pass of the reference's Benchmark.cc"}
+    except (RuntimeError, subprocess.CalledProcessError, OSError) as e:
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"unavailable: {e}"}
+
+
+def main():
+    args = parse_args()
+    if args.warmup < 3:
+        print("warmup must be >= 3", file=sys.stderr)
+        return 2
+    if args.impl == "reference":
+        return reference_arm(args)
+    return b200_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,246 @@
+/*
+ * tconvolve.h -- C ABI of the B200 (sm_100a) W-projection convolutional resampling library
+ * (libtconvolve.so).  Plain pointers, sizes and status codes only: no C++ or torch types.
+ *
+ * Reference interfaces replaced (paths relative to the reference project root):
+ *   - class Benchmark                       attic/tConvolveMPI/Benchmark.h:55-99
+ *       Benchmark(), init(), runGrid(), runDegrid(), getSupport()  -> tcv_create, tcv_init,
+ *       tcv_run_grid, tcv_run_degrid, tcv_support (context API below)
+ *   - Benchmark::gridKernel / degridKernel  attic/tConvolveMPI/Benchmark.cc:125-195
+ *   - cuda_gridKernel / cuda_degridKernel   attic/tConvolveCuda/CudaGridKernel.h:33-42
+ *       (raw device-pointer kernels)       -> tcv_grid_raw, tcv_degrid_raw, tcv_plan_*
+ *   - Benchmark::initC                      attic/tConvolveMPI/Benchmark.cc:206-270 -> tcv_c_geometry, tcv_init_c_raw
+ *   - Benchmark::initCOffset                attic/tConvolveMPI/Benchmark.cc:281-324 -> tcv_init_offsets_raw
+ *   - Benchmark::randomInt + init's u,v,w   attic/tConvolveMPI/Benchmark.cc:46-80   -> tcv_init_uvw_raw
+ *
+ * Data layout (identical to the reference's memory layout):
+ *   complex values are interleaved float pairs (std::complex<float>, cuComplex);
+ *   the grid is row-major [v][u], gSize x gSize;
+ *   the table C is [k][osj][osi][j][i] flattened, entry index i + sSize*(j + sSize*(osi + os*(osj + os*k)));
+ *   per-sample arrays (data, iu, iv, cOffset) are indexed dind = sample * nChan + chan.
+ *   A sample grids onto columns iu-support .. iu+support and rows iv .. iv+2*support (the
+ *   reference's footprint, Benchmark.cc:133).
+ *
+ * Errors: every call returns a tcv_status.  Calls taking a `stream` are asynchronous on that
+ * stream (NULL = the legacy default stream) and validate host-visible arguments before launching;
+ * samples whose footprint or table range falls outside the grid or table are counted as rejected
+ * on the device and skipped (the reference has no checks and would write out of bounds).
+ * tcv_plan_rejected reads that count; the context API turns it into TCV_ERR_BOUNDS.
+ */
+#ifndef TCONVOLVE_H
+#define TCONVOLVE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tcv_status {
+    TCV_OK = 0,
+    TCV_ERR_ARG = 1,        /* invalid argument: null pointer, bad size or type code */
+    TCV_ERR_BOUNDS = 2,     /* one or more samples fell outside the grid or the table */
+    TCV_ERR_OOM = 3,        /* device memory allocation failed */
+    TCV_ERR_CUDA = 4,       /* a CUDA runtime or driver call failed */
+    TCV_ERR_TIMEOUT = 5,    /* a bounded device-side wait gave up (status word set by a kernel) */
+    TCV_ERR_STATE = 6,      /* call out of order, e.g. run_grid before init */
+    TCV_ERR_WORKSPACE = 7,  /* caller-provided workspace smaller than required */
+    TCV_ERR_UNSUPPORTED = 8 /* shape outside what the kernels handle (reported, never faked) */
+} tcv_status;
+
+/* Storage type of the convolution table C on the device. */
+typedef enum tcv_ctype {
+    TCV_C_C64 = 0,  /* complex64, the reference's std::complex<float> (8 B/entry): the plain form */
+    TCV_C_R32 = 1,  /* real float (4 B/entry); exact when every imaginary part is zero (attic table) */
+    TCV_C_CBF16 = 2,/* complex bfloat16 (4 B/entry) */
+    TCV_C_RBF16 = 3,/* real bfloat16 (2 B/entry) */
+    TCV_C_CF16 = 4, /* complex float16 x 2^e (4 B/entry), power-of-two scale passed as c_scale */
+    TCV_C_RF16 = 5  /* real float16 x 2^e (2 B/entry) */
+} tcv_ctype;
+
+const char *tcv_status_string(tcv_status s);
+/* Bytes per table entry of a tcv_ctype, 0 for an unknown code. */
+size_t tcv_ctype_bytes(int c_type);
+/* Library version string and the compute capability it was built for ("sm_100a"). */
+const char *tcv_version(void);
+
+/* ------------------------------------------------------------------------------------------
+ * Set-up functions (the untimed part of Benchmark::init)
+ * ---------------------------------------------------------------------------------------- */
+
+/* support, overSample, wCellSize and table length exactly as Benchmark::initC derives them
+ * (attic/tConvolveMPI/Benchmark.cc:212-217, 226-230).  Host only. */
+tcv_status tcv_c_geometry(double freq0, double cell_size, int baseline, int w_size,
+                          int *support, int *over_sample, double *w_cell_size, int64_t *c_len);
+
+/* Fill the table on the device: FP64 arithmetic for r^2 and the cos/exp w-term, float store,
+ * then the reference's normalisation by a *sequential float* sum of |C| (Benchmark.cc:260-269),
+ * so that the table matches the reference's.  d_c receives c_len complex64 entries.
+ * d_scratch: device buffer of at least tcv_init_c_scratch_bytes() bytes.  *sum_c_out (host,
+ * may be NULL) receives sumC after a stream synchronisation. */
+size_t tcv_init_c_scratch_bytes(void);
+tcv_status tcv_init_c_raw(double freq0, double cell_size, int baseline, int w_size, float *d_c,
+                          void *d_scratch, float *sum_c_out, void *stream);
+
+/* Convert the complex64 table into another storage type (TCV_C_R32 and the reduced forms).
+ * *c_scale_out receives the factor the kernels must be given as c_scale (2^-e for the FP16
+ * forms, 1 otherwise).  For the real forms the imaginary parts must be zero; *imag_nonzero_out
+ * (may be NULL) receives the number of entries that were not (synchronises the stream). */
+tcv_status tcv_convert_c(const float *d_c64, int64_t c_len, int c_type, void *d_out,
+                         float *c_scale_out, int64_t *imag_nonzero_out, void *stream);
+
+/* u, v, w for n_samples samples from the reference's K&R generator (Benchmark.cc:46-80), state0 =
+ * generator state before the first draw (1 in the reference), computed in parallel by jump-ahead. */
+tcv_status tcv_init_uvw_raw(int64_t n_samples, int baseline, uint64_t state0, double *d_u,
+                            double *d_v, double *d_w, void *stream);
+
+/* iu, iv, cOffset for n_samples x n_chan samples (Benchmark.cc:281-324), FP64 with the
+ * reference's truncations.  d_freq: device array of n_chan inverse wavelengths. */
+tcv_status tcv_init_offsets_raw(const double *d_u, const double *d_v, const double *d_w,
+                                int64_t n_samples, const double *d_freq, int n_chan,
+                                double cell_size, double w_cell_size, int w_size, int g_size,
+                                int support, int over_sample, int32_t *d_iu, int32_t *d_iv,
+                                int32_t *d_coff, void *stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Raw device-pointer kernels (replace cuda_gridKernel / cuda_degridKernel)
+ *
+ * A plan bins samples into grid tiles (gridding) and anchor tiles (degridding) with a device
+ * radix sort on (tile, w-plane/oversample kernel); it depends only on iu, iv, cOffset, so one
+ * plan serves any number of grid and degrid passes over the same samples.  The plan lives in a
+ * caller-provided device workspace of tcv_plan_workspace_bytes() bytes.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct tcv_plan tcv_plan;
+
+size_t tcv_plan_workspace_bytes(int64_t n, int support, int g_size, int64_t c_len);
+/* Build (asynchronously) a plan for n samples.  *plan_out is a small host object; free it with
+ * tcv_plan_destroy.  c_len: number of entries in the table (bounds for cOffset). */
+tcv_status tcv_plan_build(tcv_plan **plan_out, const int32_t *d_iu, const int32_t *d_iv,
+                          const int32_t *d_coff, int64_t n, int support, int g_size,
+                          int64_t c_len, void *d_work, size_t work_bytes, void *stream);
+/* grid += gridding of d_data (n complex64) with table d_c of type c_type (Benchmark.cc:125-155). */
+tcv_status tcv_plan_grid(const tcv_plan *plan, const float *d_data, const void *d_c, int c_type,
+                         float c_scale, float *d_grid, void *stream);
+/* d_data[n] = degridding of d_grid (Benchmark.cc:158-195); overwrites d_data. */
+tcv_status tcv_plan_degrid(const tcv_plan *plan, const float *d_grid, const void *d_c, int c_type,
+                           float c_scale, float *d_data, void *stream);
+/* Number of samples the plan rejected as out of bounds (synchronises the stream). */
+tcv_status tcv_plan_rejected(const tcv_plan *plan, int64_t *rejected_out, void *stream);
+/* TCV_ERR_TIMEOUT if a kernel run with this plan gave up a bounded wait, else TCV_OK
+ * (synchronises the stream). */
+tcv_status tcv_plan_status(const tcv_plan *plan, void *stream);
+/* Tile geometry chosen for the plan: grid tile width/height, anchor tile, degrid mode
+ * (0 = TMA-staged tiles, 1 = direct), number of grid tiles, max samples in one grid tile. */
+tcv_status tcv_plan_info(const tcv_plan *plan, int *tile_w, int *tile_h, int *anchor,
+                         int *degrid_mode, int *n_tiles);
+void tcv_plan_destroy(tcv_plan *plan);
+
+/* One-call forms: plan_build + grid (or degrid) in the given workspace. */
+tcv_status tcv_grid_raw(const float *d_data, int64_t n, int support, const void *d_c, int c_type,
+                        float c_scale, int64_t c_len, const int32_t *d_coff, const int32_t *d_iu,
+                        const int32_t *d_iv, float *d_grid, int g_size, void *d_work,
+                        size_t work_bytes, void *stream);
+tcv_status tcv_degrid_raw(const float *d_grid, int g_size, int support, const void *d_c,
+                          int c_type, float c_scale, int64_t c_len, const int32_t *d_coff,
+                          const int32_t *d_iu, const int32_t *d_iv, float *d_data, int64_t n,
+                          void *d_work, size_t work_bytes, void *stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Host-buffer one-call forms (the reference's libCudaGridder seam,
+ * attic/tConvolveCuda/CudaGridder.cc:54-207 behind CudaGridder.h:32-50): allocate, upload,
+ * plan, run, download, free.  *device_seconds (may be NULL) receives the CUDA-event time of the
+ * plan plus the kernel.  Returns TCV_ERR_BOUNDS (after computing the in-bounds samples) when
+ * samples were skipped.
+ * ---------------------------------------------------------------------------------------- */
+tcv_status tcv_grid_host_raw(const float *data, int64_t n, int support, const float *c,
+                             int64_t c_len, const int32_t *coff, const int32_t *iu,
+                             const int32_t *iv, float *grid, int g_size, int device,
+                             double *device_seconds);
+tcv_status tcv_degrid_host_raw(const float *grid, int g_size, int support, const float *c,
+                               int64_t c_len, const int32_t *coff, const int32_t *iu,
+                               const int32_t *iv, float *data, int64_t n, int device,
+                               double *device_seconds);
+/* Benchmark::initC into host memory (computed on the device). */
+tcv_status tcv_init_c_host(double freq0, double cell_size, int baseline, int w_size, float *c,
+                           int64_t c_len, int device, int *support, int *over_sample,
+                           double *w_cell_size, float *sum_c);
+
+/* ------------------------------------------------------------------------------------------
+ * Context API: the Benchmark object (attic/tConvolveMPI/Benchmark.h:55-99) with every buffer
+ * resident on one GPU.  One context per host thread; calls on one context are serialised on
+ * its stream.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct tcv_config {
+    int64_t n_samples;  /* nSamples (Benchmark.h:39) */
+    int32_t w_size;     /* wSize (Benchmark.h:40) */
+    int32_t n_chan;     /* nChan (Benchmark.h:41) */
+    int32_t g_size;     /* gSize (Benchmark.h:44) */
+    int32_t baseline;   /* baseline in metres (Benchmark.h:46) */
+    double cell_size;   /* cellSize in wavelengths (Benchmark.h:45) */
+    uint64_t seed;      /* generator start state = seed + 1; seed 0 reproduces the reference */
+    int32_t c_type;     /* tcv_ctype used by run_grid / run_degrid (TCV_C_C64 = plain form) */
+    int32_t device;     /* CUDA device ordinal */
+} tcv_config;
+
+typedef struct tcv_ctx tcv_ctx;
+
+/* Fill *cfg with the reference defaults (attic/tConvolveMPI/Benchmark.h:39-46). */
+void tcv_config_default(tcv_config *cfg);
+tcv_status tcv_create(const tcv_config *cfg, tcv_ctx **ctx_out);
+void tcv_destroy(tcv_ctx *ctx);
+const char *tcv_last_error(const tcv_ctx *ctx);
+/* Use an external stream (e.g. the caller's); NULL restores the context's own stream. */
+tcv_status tcv_set_stream(tcv_ctx *ctx, void *stream);
+void *tcv_get_stream(const tcv_ctx *ctx);
+tcv_status tcv_sync(tcv_ctx *ctx);
+
+/* Benchmark::init: u,v,w from the generator, data = 1+0i, grid = 0, freq, initC, initCOffset,
+ * then the binning plan. */
+tcv_status tcv_init(tcv_ctx *ctx);
+/* Benchmark::runGrid: grid += gridding of the samples. */
+tcv_status tcv_run_grid(tcv_ctx *ctx);
+/* Benchmark::runDegrid: outdata = degridding of the grid. */
+tcv_status tcv_run_degrid(tcv_ctx *ctx);
+int tcv_support(const tcv_ctx *ctx);
+int tcv_over_sample(const tcv_ctx *ctx);
+double tcv_w_cell_size(const tcv_ctx *ctx);
+float tcv_sum_c(const tcv_ctx *ctx);
+int64_t tcv_c_len(const tcv_ctx *ctx);
+int64_t tcv_n_data(const tcv_ctx *ctx);        /* nSamples * nChan */
+double tcv_updates_per_pass(const tcv_ctx *ctx); /* nSamples * nChan * sSize^2 */
+/* Switch the table storage type used by run_grid / run_degrid (converts once, keeps the C64 table). */
+tcv_status tcv_set_ctype(tcv_ctx *ctx, int c_type);
+
+/* Host <-> device transfers of the context's buffers (synchronous; host pointers). */
+tcv_status tcv_set_data(tcv_ctx *ctx, const float *vis, int64_t n);          /* n complex */
+tcv_status tcv_get_data(tcv_ctx *ctx, float *vis, int64_t n);                /* samples' data */
+tcv_status tcv_get_outdata(tcv_ctx *ctx, float *vis, int64_t n);             /* degridded */
+tcv_status tcv_set_grid(tcv_ctx *ctx, const float *grid);                    /* gSize^2 complex */
+tcv_status tcv_get_grid(tcv_ctx *ctx, float *grid);
+tcv_status tcv_zero_grid(tcv_ctx *ctx);
+tcv_status tcv_get_c(tcv_ctx *ctx, float *c, int64_t n_entries);             /* complex64 table */
+tcv_status tcv_get_offsets(tcv_ctx *ctx, int32_t *iu, int32_t *iv, int32_t *coff);
+tcv_status tcv_get_uvw(tcv_ctx *ctx, double *u, double *v, double *w);
+/* Replace u, v, w (host arrays of nSamples) and recompute offsets and plan. */
+tcv_status tcv_set_uvw(tcv_ctx *ctx, const double *u, const double *v, const double *w);
+
+/* Device pointers of the context's buffers, for callers that drive the raw API themselves. */
+typedef struct tcv_device_buffers {
+    float *data;      /* nSamples*nChan complex64 */
+    float *outdata;   /* nSamples*nChan complex64 */
+    float *grid;      /* gSize^2 complex64 */
+    float *c64;       /* c_len complex64 */
+    const void *c_active; /* table in the active c_type */
+    int32_t *iu, *iv, *coff;
+    double *u, *v, *w;
+    const tcv_plan *plan;
+    float c_scale;
+    int32_t c_type;
+} tcv_device_buffers;
+tcv_status tcv_get_device_buffers(tcv_ctx *ctx, tcv_device_buffers *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TCONVOLVE_H */

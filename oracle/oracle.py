@@ -1,0 +1,209 @@
+"""numpy front end for the C restatement in tconvolve_oracle.c.
+
+TEST INFRASTRUCTURE ONLY: the parity checker.  tests/, the smoke check and the cpu_baseline leg
+of bench.py may import this module; the product package never does.
+
+Each function names the reference lines it restates (paths relative to the reference project
+root).  Parity status: pinned against the reference's own attic/tConvolveMPI/Benchmark.cc
+(tests/golden/, tests/test_oracle.py).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle_tcv.so")
+_lib = None
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_I32 = ctypes.c_int
+_F64 = ctypes.c_double
+
+
+def build() -> str:
+    """Compile the restatement (make restatement) and return the library path."""
+    subprocess.run(["make", "-s", "-C", _HERE, "restatement"], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_init_uvw.argtypes = [_I64, _I32, ctypes.c_uint64, _P, _P, _P]
+        L.orc_init_freq.argtypes = [_I32, _P]
+        L.orc_c_geometry.argtypes = [_F64, _F64, _I32, _I32, _P, _P, _P]
+        L.orc_init_c.argtypes = [_F64, _F64, _I32, _I32, _P, _P, _P, _P, _P]
+        L.orc_init_c.restype = ctypes.c_float
+        L.orc_init_offsets.argtypes = [_I64, _I32, _P, _P, _P, _P, _F64, _F64, _I32, _I32, _I32,
+                                       _I32, _P, _P, _P]
+        L.orc_grid_f32.argtypes = [_P, _I64, _I32, _P, _P, _P, _P, _P, _I32, _I32]
+        L.orc_degrid_f32.argtypes = [_P, _I32, _I32, _P, _P, _P, _P, _P, _I64, _I32]
+        L.orc_grid_f64.argtypes = [_P, _I64, _I32, _P, _P, _P, _P, _P, _I32]
+        L.orc_degrid_f64.argtypes = [_P, _I32, _I32, _P, _P, _P, _P, _P, _I64]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.flags.c_contiguous
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+@dataclass
+class Config:
+    """One tConvolve problem (the constants of attic/tConvolveMPI/Benchmark.h:39-46)."""
+    n_samples: int
+    w_size: int
+    n_chan: int
+    g_size: int
+    cell_size: float
+    baseline: int = 2000
+    seed: int = 0  # LCG start state = seed + 1; seed 0 is the reference's next = 1
+
+
+ARCSEC_CELL_1024 = 1.0 / (1024 * 5.0 * math.pi / 648000.0)  # 5 arcsec cell on a 1024 grid, in wavelengths
+
+CONFIGS = {
+    "g1": Config(200, 5, 1, 128, 200.0),
+    "g2": Config(1000, 9, 4, 256, 100.0),
+    "c1": Config(16000, 9, 1, 1024, ARCSEC_CELL_1024),
+    "c2": Config(160000, 33, 1, 4096, 5.0),
+}
+
+
+def init_uvw(cfg: Config):
+    """u, v, w from the reference LCG (attic/tConvolveMPI/Benchmark.cc:46-80)."""
+    n = cfg.n_samples
+    u = np.empty(n, np.float64)
+    v = np.empty(n, np.float64)
+    w = np.empty(n, np.float64)
+    lib().orc_init_uvw(n, cfg.baseline, cfg.seed + 1, _p(u), _p(v), _p(w))
+    return u, v, w
+
+
+def init_freq(cfg: Config) -> np.ndarray:
+    """Inverse wavelengths per channel (attic/tConvolveMPI/Benchmark.cc:86-90)."""
+    f = np.empty(cfg.n_chan, np.float64)
+    lib().orc_init_freq(cfg.n_chan, _p(f))
+    return f
+
+
+def c_geometry(cfg: Config):
+    """(support, overSample, wCellSize) as attic/tConvolveMPI/Benchmark.cc:212-217 computes them."""
+    s = ctypes.c_int()
+    o = ctypes.c_int()
+    wc = ctypes.c_double()
+    freq = init_freq(cfg)
+    lib().orc_c_geometry(float(freq[0]), float(cfg.cell_size), cfg.baseline, cfg.w_size,
+                         ctypes.byref(s), ctypes.byref(o), ctypes.byref(wc))
+    return s.value, o.value, wc.value
+
+
+def init_c(cfg: Config, want_f64: bool = False):
+    """Normalised table C (attic/tConvolveMPI/Benchmark.cc:206-270).
+
+    Returns (C complex64 flat, C64 float64 flat or None, support, overSample, wCellSize, sumC).
+    """
+    support, os_, _ = c_geometry(cfg)
+    s = 2 * support + 1
+    n = s * s * os_ * os_ * cfg.w_size
+    c = np.empty(n, np.complex64)
+    c64 = np.empty(n, np.float64) if want_f64 else None
+    sup = ctypes.c_int()
+    o = ctypes.c_int()
+    wc = ctypes.c_double()
+    freq = init_freq(cfg)
+    sum_c = lib().orc_init_c(float(freq[0]), float(cfg.cell_size), cfg.baseline, cfg.w_size, _p(c),
+                             _p(c64) if want_f64 else None, ctypes.byref(sup), ctypes.byref(o),
+                             ctypes.byref(wc))
+    return c, c64, sup.value, o.value, wc.value, float(sum_c)
+
+
+def init_offsets(cfg: Config, u, v, w, w_cell_size: float, support: int, over_sample: int):
+    """iu, iv, cOffset per sample (attic/tConvolveMPI/Benchmark.cc:281-324)."""
+    n = cfg.n_samples * cfg.n_chan
+    iu = np.empty(n, np.int32)
+    iv = np.empty(n, np.int32)
+    co = np.empty(n, np.int32)
+    freq = init_freq(cfg)
+    lib().orc_init_offsets(cfg.n_samples, cfg.n_chan, _p(np.ascontiguousarray(u)),
+                           _p(np.ascontiguousarray(v)), _p(np.ascontiguousarray(w)), _p(freq),
+                           float(cfg.cell_size), float(w_cell_size), cfg.w_size, cfg.g_size,
+                           support, over_sample, _p(iu), _p(iv), _p(co))
+    return iu, iv, co
+
+
+def grid_f32(data, support, c, coff, iu, iv, grid, g_size, threads: int = 1):
+    """grid += gridding of data, reference arithmetic and order (Benchmark.cc:125-155). In place."""
+    data = np.ascontiguousarray(data, np.complex64)
+    assert grid.dtype == np.complex64 and grid.size == g_size * g_size
+    lib().orc_grid_f32(_p(data), data.size, support, _p(c), _p(coff), _p(iu), _p(iv), _p(grid),
+                       g_size, threads)
+    return grid
+
+
+def degrid_f32(grid, g_size, support, c, coff, iu, iv, threads: int = 1):
+    """Degridded samples, reference arithmetic and order (Benchmark.cc:158-195)."""
+    n = iu.size
+    out = np.empty(n, np.complex64)
+    lib().orc_degrid_f32(_p(grid), g_size, support, _p(c), _p(coff), _p(iu), _p(iv), _p(out), n,
+                         threads)
+    return out
+
+
+def grid_f64(data, support, c64, coff, iu, iv, grid64, g_size):
+    """FP64 gridding (complex128 data and grid, real float64 table). In place."""
+    data = np.ascontiguousarray(data, np.complex128)
+    assert grid64.dtype == np.complex128
+    lib().orc_grid_f64(_p(data), data.size, support, _p(c64), _p(coff), _p(iu), _p(iv),
+                       _p(grid64), g_size)
+    return grid64
+
+
+def degrid_f64(grid64, g_size, support, c64, coff, iu, iv):
+    n = iu.size
+    out = np.empty(n, np.complex128)
+    lib().orc_degrid_f64(_p(grid64), g_size, support, _p(c64), _p(coff), _p(iu), _p(iv), _p(out), n)
+    return out
+
+
+def run_plain(cfg: Config, vis: np.ndarray | None = None, threads: int = 1, want_f64: bool = False):
+    """The whole reference pipeline: init, one gridding pass into a zero grid, one degridding pass.
+
+    vis None means the reference's data = 1+0i (Benchmark.cc:76-79).
+    """
+    u, v, w = init_uvw(cfg)
+    c, c64, support, os_, wcs, sum_c = init_c(cfg, want_f64)
+    iu, iv, co = init_offsets(cfg, u, v, w, wcs, support, os_)
+    n = cfg.n_samples * cfg.n_chan
+    data = np.ones(n, np.complex64) if vis is None else np.ascontiguousarray(vis, np.complex64)
+    grid = np.zeros(cfg.g_size * cfg.g_size, np.complex64)
+    grid_f32(data, support, c, co, iu, iv, grid, cfg.g_size, threads)
+    out = degrid_f32(grid, cfg.g_size, support, c, co, iu, iv, threads)
+    res = dict(u=u, v=v, w=w, C=c, support=support, over_sample=os_, w_cell_size=wcs,
+               sum_c=sum_c, iu=iu, iv=iv, coff=co, data=data, grid=grid, outdata=out)
+    if want_f64:
+        g64 = np.zeros(cfg.g_size * cfg.g_size, np.complex128)
+        grid_f64(data.astype(np.complex128), support, c64, co, iu, iv, g64, cfg.g_size)
+        res["C64"] = c64
+        res["grid64"] = g64
+        res["outdata64"] = degrid_f64(g64, cfg.g_size, support, c64, co, iu, iv)
+    return res
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    """||a - b|| / ||b|| in float64."""
+    a = np.asarray(a).astype(np.complex128).ravel()
+    b = np.asarray(b).astype(np.complex128).ravel()
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))

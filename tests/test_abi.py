@@ -1,0 +1,108 @@
+"""The C ABI boundary, checked without a GPU: the library loads, exports every function that
+include/tconvolve.h declares, the binding's table matches the header, host-only functions give
+the reference's known answers, and calls that need a device fail loudly when there is none."""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import REPO
+from tconvolve.workload import PROBLEMS
+
+HEADER = os.path.join(REPO, "include", "tconvolve.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(tcv_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(tcv):
+    from tconvolve._lib import LIB_PATH
+
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB_PATH], check=True, capture_output=True,
+                         text=True).stdout
+    exported = set(re.findall(r" T (tcv_\w+)", out))
+    declared = header_functions()
+    assert len(declared) >= 50
+    missing = [f for f in declared if f not in exported]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_binding_covers_header(tcv):
+    from tconvolve._lib import SIGNATURES
+
+    assert sorted(SIGNATURES) == header_functions()
+
+
+def test_cuda_gridder_shim_exports_reference_symbols(tcv):
+    lib = os.path.join(tcv.BUILD_DIR, "libCudaGridder.so")
+    out = subprocess.run(["nm", "-DC", "--defined-only", lib], check=True, capture_output=True,
+                         text=True).stdout
+    assert "gridKernelCuda(std::vector<std::complex<float>" in out
+    assert "degridKernelCuda(std::vector<std::complex<float>" in out
+
+
+@pytest.mark.parametrize("cfg", ["g1", "g2", "c1", "c2"])
+def test_c_geometry_matches_reference(tcv, golden, cfg):
+    prob = PROBLEMS[cfg]
+    sup, os_, wcs, clen = ctypes.c_int(), ctypes.c_int(), ctypes.c_double(), ctypes.c_int64()
+    st = tcv.lib().tcv_c_geometry(prob.freq0, prob.cell_size, prob.baseline, prob.w_size,
+                                  ctypes.byref(sup), ctypes.byref(os_), ctypes.byref(wcs),
+                                  ctypes.byref(clen))
+    assert st == 0
+    meta = golden["runs"][f"{cfg}_ones"]["meta"]
+    assert sup.value == meta["support"] == prob.support()
+    assert os_.value == meta["overSample"]
+    assert wcs.value == meta["wCellSize"]
+    assert clen.value == golden["runs"][f"{cfg}_ones"]["shape"]["C"][0]
+
+
+def test_status_strings_and_type_sizes(tcv):
+    L = tcv.lib()
+    assert L.tcv_status_string(0) == b"ok"
+    assert L.tcv_status_string(2) == b"sample outside grid or table"
+    assert [L.tcv_ctype_bytes(t) for t in range(6)] == [8, 4, 4, 2, 4, 2]
+    assert L.tcv_ctype_bytes(17) == 0
+    assert b"sm_100a" in L.tcv_version()
+
+
+def test_argument_validation_before_device_use(tcv):
+    from tconvolve._lib import TcvConfig
+
+    L = tcv.lib()
+    bad = TcvConfig(n_samples=0, w_size=33, n_chan=1, g_size=4096, baseline=2000, cell_size=5.0)
+    ctx = ctypes.c_void_p()
+    assert L.tcv_create(ctypes.byref(bad), ctypes.byref(ctx)) == 1  # TCV_ERR_ARG
+    assert L.tcv_plan_build(None, None, None, None, 10, 3, 64, 100, None, 0, None) == 1
+    assert L.tcv_plan_workspace_bytes(-1, 3, 64, 100) == 0
+    assert L.tcv_plan_workspace_bytes(1000, 22, 1024, 1166400) > 0
+    assert L.tcv_run_grid(None) == 1
+    assert L.tcv_convert_c(None, 10, 1, None, None, None, None) == 1
+
+
+def test_no_silent_cpu_path(tcv):
+    """Without a usable GPU the context cannot be created: the library has no CPU fallback."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible; the loud-failure path is for GPU-less hosts")
+    from tconvolve import Benchmark, TcvError
+
+    with pytest.raises(TcvError) as e:
+        Benchmark(**PROBLEMS["g1"].kwargs())
+    assert e.value.status == 4  # TCV_ERR_CUDA
+
+
+def test_workspace_grows_with_samples(tcv):
+    L = tcv.lib()
+    a = L.tcv_plan_workspace_bytes(1000, 64, 4096, 35145792)
+    b = L.tcv_plan_workspace_bytes(160000, 64, 4096, 35145792)
+    assert b > a
+    # 160 k samples x 9 tiles: keys + values, double-buffered, plus the anchor sort; < 64 MiB
+    assert b < 64 << 20
