@@ -17,10 +17,14 @@ struct tcv_ctx {
     cudaStream_t own_stream = nullptr, stream = nullptr;
     double *u = nullptr, *v = nullptr, *w = nullptr, *freq = nullptr;
     float2 *data = nullptr, *outdata = nullptr, *grid = nullptr, *c64 = nullptr;
-    void* c_alt = nullptr;
+    void* c_alt = nullptr;      // active form, reference layout (when not complex64)
     int c_alt_type = -1;
-    int c_type = TCV_C_C64;
-    float c_scale = 1.f;
+    float c_alt_scale = 1.f;
+    void* c_pad = nullptr;      // active form, prepared (padded) layout for the TMA kernels
+    int c_pad_type = -1;
+    float c_pad_scale = 1.f;
+    int c_type = TCV_C_C64;     // active storage form
+    int path = TCV_PATH_TMA;
     int32_t *iu = nullptr, *iv = nullptr, *coff = nullptr;
     void* work = nullptr;
     size_t work_bytes = 0;
@@ -68,7 +72,58 @@ cudaError_t dalloc(T** p, size_t count)
     return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T) + 16);
 }
 
-const void* active_table(const tcv_ctx* c) { return c->c_type == TCV_C_C64 ? c->c64 : c->c_alt; }
+// table, type code (with the layout flag) and scale the kernels are given
+const void* active_table(const tcv_ctx* c)
+{
+    if (c->path == TCV_PATH_TMA) return c->c_pad;
+    return c->c_type == TCV_C_C64 ? static_cast<const void*>(c->c64) : c->c_alt;
+}
+int active_code(const tcv_ctx* c) { return c->path == TCV_PATH_TMA ? (c->c_type | TCV_C_PADDED) : c->c_type; }
+float active_scale(const tcv_ctx* c)
+{
+    if (c->path == TCV_PATH_TMA) return c->c_pad_scale;
+    return c->c_type == TCV_C_C64 ? 1.f : c->c_alt_scale;
+}
+
+// make sure the table of the active form exists in the layout the active path needs
+tcv_status ensure_tables(tcv_ctx* c)
+{
+    const int t = c->c_type;
+    if (c->path == TCV_PATH_TMA) {
+        if (c->c_pad_type == t) return TCV_OK;
+        if (c->c_pad) {
+            CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+            cudaFree(c->c_pad);
+            c->c_pad = nullptr;
+            c->c_pad_type = -1;
+        }
+        const size_t bytes = tcv_table_bytes(c->c_len, c->support, t | TCV_C_PADDED);
+        if (!bytes) return fail(c, TCV_ERR_UNSUPPORTED, "table shape has no prepared layout");
+        CTX_CUDA(c, cudaMalloc(&c->c_pad, bytes));
+        int64_t nz = 0;
+        CTX_TRY(c, tcv_prepare_table(reinterpret_cast<const float*>(c->c64), c->c_len, c->support, t, c->c_pad,
+                                     &c->c_pad_scale, &nz, c->stream));
+        const bool real_form = t == TCV_C_R32 || t == TCV_C_RBF16 || t == TCV_C_RF16;
+        if (real_form && nz > 0) return fail(c, TCV_ERR_ARG, "real table form requested for a table with imaginary parts");
+        c->c_pad_type = t;
+        return TCV_OK;
+    }
+    if (t == TCV_C_C64 || c->c_alt_type == t) return TCV_OK;
+    if (c->c_alt) {
+        CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->c_alt);
+        c->c_alt = nullptr;
+        c->c_alt_type = -1;
+    }
+    CTX_CUDA(c, cudaMalloc(&c->c_alt, size_t(c->c_len) * tcv_ctype_bytes(t) + 16));
+    int64_t nz = 0;
+    CTX_TRY(c, tcv_convert_c(reinterpret_cast<const float*>(c->c64), c->c_len, t, c->c_alt, &c->c_alt_scale, &nz,
+                             c->stream));
+    const bool real_form = t == TCV_C_R32 || t == TCV_C_RBF16 || t == TCV_C_RF16;
+    if (real_form && nz > 0) return fail(c, TCV_ERR_ARG, "real table form requested for a table with imaginary parts");
+    c->c_alt_type = t;
+    return TCV_OK;
+}
 
 tcv_status rebuild_plan(tcv_ctx* c)
 {
@@ -133,7 +188,7 @@ void tcv_destroy(tcv_ctx* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->plan) tcv_plan_destroy(c->plan);
     void* bufs[] = {c->u, c->v, c->w, c->freq, c->data, c->outdata, c->grid, c->c64, c->c_alt,
-                    c->iu, c->iv, c->coff, c->work, c->c_scratch};
+                    c->c_pad, c->iu, c->iv, c->coff, c->work, c->c_scratch};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -227,50 +282,42 @@ tcv_status tcv_init(tcv_ctx* c)
                                     c->iu, c->iv, c->coff, c->stream));
     c->initialized = true;
     c->c_alt_type = -1;
-    const int want = cfg.c_type;
-    c->c_type = TCV_C_C64;
-    if (want != TCV_C_C64) CTX_TRY(c, tcv_set_ctype(c, want));
+    c->c_pad_type = -1;
+    c->c_type = cfg.c_type & 0xff;
+    CTX_TRY(c, ensure_tables(c));
     return rebuild_plan(c);
 }
 
 tcv_status tcv_set_ctype(tcv_ctx* c, int c_type)
 {
-    if (!c || tcv_ctype_bytes(c_type) == 0) return TCV_ERR_ARG;
+    if (!c || tcv_ctype_bytes(c_type) == 0 || (c_type & TCV_C_PADDED)) return TCV_ERR_ARG;
     if (!c->initialized) return fail(c, TCV_ERR_STATE, "set_ctype before init");
-    if (c_type == TCV_C_C64) {
-        c->c_type = c_type;
-        c->c_scale = 1.f;
-        return TCV_OK;
-    }
-    if (c->c_alt_type != c_type) {
-        if (c->c_alt) {
-            CTX_CUDA(c, cudaStreamSynchronize(c->stream));
-            cudaFree(c->c_alt);
-            c->c_alt = nullptr;
-        }
-        CTX_CUDA(c, cudaMalloc(&c->c_alt, size_t(c->c_len) * tcv_ctype_bytes(c_type) + 16));
-        int64_t nz = 0;
-        CTX_TRY(c, tcv_convert_c(reinterpret_cast<const float*>(c->c64), c->c_len, c_type, c->c_alt,
-                                 &c->c_scale, &nz, c->stream));
-        const bool real_form = c_type == TCV_C_R32 || c_type == TCV_C_RBF16 || c_type == TCV_C_RF16;
-        if (real_form && nz > 0) {
-            cudaFree(c->c_alt);
-            c->c_alt = nullptr;
-            c->c_alt_type = -1;
-            return fail(c, TCV_ERR_ARG, "real table form requested for a table with imaginary parts");
-        }
-        c->c_alt_type = c_type;
-    }
+    const int prev = c->c_type;
     c->c_type = c_type;
-    return TCV_OK;
+    const tcv_status s = ensure_tables(c);
+    if (s != TCV_OK) c->c_type = prev;
+    return s;
 }
+
+tcv_status tcv_set_path(tcv_ctx* c, int path)
+{
+    if (!c || (path != TCV_PATH_TMA && path != TCV_PATH_DIRECT)) return TCV_ERR_ARG;
+    const int prev = c->path;
+    c->path = path;
+    if (!c->initialized) return TCV_OK;
+    const tcv_status s = ensure_tables(c);
+    if (s != TCV_OK) c->path = prev;
+    return s;
+}
+
+int tcv_get_path(const tcv_ctx* c) { return c ? c->path : -1; }
 
 tcv_status tcv_run_grid(tcv_ctx* c)
 {
     if (!c) return TCV_ERR_ARG;
     if (!c->initialized || !c->plan) return fail(c, TCV_ERR_STATE, "run_grid before init");
-    CTX_TRY(c, tcv_plan_grid(c->plan, reinterpret_cast<const float*>(c->data), active_table(c), c->c_type,
-                             c->c_scale, reinterpret_cast<float*>(c->grid), c->stream));
+    CTX_TRY(c, tcv_plan_grid(c->plan, reinterpret_cast<const float*>(c->data), active_table(c), active_code(c),
+                             active_scale(c), reinterpret_cast<float*>(c->grid), c->stream));
     return TCV_OK;
 }
 
@@ -278,8 +325,8 @@ tcv_status tcv_run_degrid(tcv_ctx* c)
 {
     if (!c) return TCV_ERR_ARG;
     if (!c->initialized || !c->plan) return fail(c, TCV_ERR_STATE, "run_degrid before init");
-    CTX_TRY(c, tcv_plan_degrid(c->plan, reinterpret_cast<const float*>(c->grid), active_table(c), c->c_type,
-                               c->c_scale, reinterpret_cast<float*>(c->outdata), c->stream));
+    CTX_TRY(c, tcv_plan_degrid(c->plan, reinterpret_cast<const float*>(c->grid), active_table(c), active_code(c),
+                               active_scale(c), reinterpret_cast<float*>(c->outdata), c->stream));
     return TCV_OK;
 }
 
@@ -390,8 +437,8 @@ tcv_status tcv_get_device_buffers(tcv_ctx* c, tcv_device_buffers* o)
     o->v = c->v;
     o->w = c->w;
     o->plan = c->plan;
-    o->c_scale = c->c_scale;
-    o->c_type = c->c_type;
+    o->c_scale = active_scale(c);
+    o->c_type = active_code(c);
     return TCV_OK;
 }
 

@@ -33,7 +33,7 @@ constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s: a tile load takes
 
 struct DegridArgs {
     int support, s, g_size;
-    int ta, natx, box_w, box_h, parts;
+    int ta, natx, natiles, box_w, box_h, parts;
     float c_scale;
 };
 
@@ -148,69 +148,82 @@ degrid_staged_kernel(const __grid_constant__ CUtensorMap tmap,
                      const typename Tab::elem* __restrict__ ctab, const int32_t* __restrict__ iu,
                      const int32_t* __restrict__ iv, const int32_t* __restrict__ coff,
                      const uint32_t* __restrict__ order, const uint32_t* __restrict__ atile_start,
-                     const uint32_t* __restrict__ atile_count, float2* __restrict__ out,
+                     const uint32_t* __restrict__ atile_count, const uint32_t* __restrict__ aitems,
+                     const uint32_t* __restrict__ n_aitems, float2* __restrict__ out,
                      unsigned int* status, DegridArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    const int at = blockIdx.x;
-    const uint32_t cnt = atile_count[at];
-    if (cnt == 0) return;
-    const uint32_t start = atile_start[at];
-    const int x0 = (at % a.natx) * a.ta;
-    const int y0 = (at / a.natx) * a.ta;
     const uint32_t box_bytes = uint32_t(a.box_w) * a.box_h * 8u;
     float2* box = reinterpret_cast<float2*>(smem);
     float2* part = reinterpret_cast<float2*>(smem + box_bytes);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + box_bytes + kChunk * kMaxParts * 8);
+    volatile int& give_up = *reinterpret_cast<volatile int*>(bar + 1);  // inside the dynamic region
 
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        give_up = 0;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(box_bytes)
-                     : "memory");
-        asm volatile(
-            "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-            " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(box)),
-            "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(x0), "r"(y0), "r"(smem_u32(bar))
-            : "memory");
-    }
-    if (!mbar_wait_bounded(bar, 0)) {
-        if (threadIdx.x == 0) atomicOr(status, 1u);
-        mbar_wait_bounded(bar, 0);  // let the copy land before the CTA's shared memory is released
-        return;
-    }
-
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = a.s, s2 = s * s, P = a.parts;
     const int per = (s2 + P - 1) / P;
     const SmemRegion region{box};
-    for (uint32_t c0 = 0; c0 < cnt; c0 += kChunk) {
-        const int m = int(cnt - c0 < uint32_t(kChunk) ? cnt - c0 : uint32_t(kChunk));
-        const int items = m * P;
-        for (int it = warp; it < items; it += kWarps) {
-            const int j = it / P, p = it - j * P;
-            const uint32_t k = order[start + c0 + j];
-            const int fx = iu[k] - a.support - x0;
-            const int fy = iv[k] - y0;
-            const int f_lo = p * per;
-            const int f_hi = min(s2, f_lo + per);
-            float2 v = walk<Tab>(ctab + coff[k], region, f_lo, f_hi, s, a.box_w, fx, fy, lane);
-            v = warp_sum(v);
-            if (lane == 0) part[j * kMaxParts + p] = v;
+    const uint32_t n_items = *n_aitems;
+    uint32_t phase = 0;
+    // persistent: cells in group-major order, so all SMs work on one slice of the table at a time
+    for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x, phase ^= 1u) {
+        const uint32_t cell = aitems[it];
+        const uint32_t cnt = atile_count[cell];
+        const uint32_t start = atile_start[cell];
+        const int at = int(cell % uint32_t(a.natiles));
+        const int x0 = (at % a.natx) * a.ta;
+        const int y0 = (at / a.natx) * a.ta;
+        if (threadIdx.x == 0) {
+            // the box was last read through the generic proxy; order that before the TMA write
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(box_bytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(box)),
+                "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(x0), "r"(y0), "r"(smem_u32(bar))
+                : "memory");
         }
+        if (!mbar_wait_bounded(bar, phase)) give_up = 1;
         __syncthreads();
-        for (int j = threadIdx.x; j < m; j += kThreads) {
-            float2 v = part[j * kMaxParts];
-            for (int p = 1; p < P; ++p) {
-                v.x += part[j * kMaxParts + p].x;
-                v.y += part[j * kMaxParts + p].y;
+        if (give_up) {
+            if (threadIdx.x == 0) {
+                atomicOr(status, 1u);
+                mbar_wait_bounded(bar, phase);  // let the copy land before shared memory is released
             }
-            out[order[start + c0 + j]] = make_float2(v.x * a.c_scale, v.y * a.c_scale);
+            return;
         }
-        __syncthreads();
+        for (uint32_t c0 = 0; c0 < cnt; c0 += kChunk) {
+            const int m = int(cnt - c0 < uint32_t(kChunk) ? cnt - c0 : uint32_t(kChunk));
+            const int items = m * P;
+            for (int w = warp; w < items; w += kWarps) {
+                const int j = w / P, p = w - j * P;
+                const uint32_t k = order[start + c0 + j];
+                const int fx = iu[k] - a.support - x0;
+                const int fy = iv[k] - y0;
+                const int f_lo = p * per;
+                const int f_hi = min(s2, f_lo + per);
+                float2 v = walk<Tab>(ctab + coff[k], region, f_lo, f_hi, s, a.box_w, fx, fy, lane);
+                v = warp_sum(v);
+                if (lane == 0) part[j * kMaxParts + p] = v;
+            }
+            __syncthreads();
+            for (int j = threadIdx.x; j < m; j += kThreads) {
+                float2 v = part[j * kMaxParts];
+                for (int p = 1; p < P; ++p) {
+                    v.x += part[j * kMaxParts + p].x;
+                    v.y += part[j * kMaxParts + p].y;
+                }
+                out[order[start + c0 + j]] = make_float2(v.x * a.c_scale, v.y * a.c_scale);
+            }
+            __syncthreads();  // the box and the partial sums are free again
+        }
     }
 }
 
@@ -285,10 +298,13 @@ tcv_status launch_staged(const tcv_plan* p, const float2* grid, const void* c, f
     });
     TCV_CUDA(attr_err);
     const int parts = g.degrid_parts < 1 ? 1 : (g.degrid_parts > kMaxParts ? kMaxParts : g.degrid_parts);
-    DegridArgs a{g.support, g.s, g.g_size, g.ta, g.natx, g.box_w, g.box_h, parts, c_scale};
-    degrid_staged_kernel<Tab><<<g.natx * g.naty, kThreads, smem, st>>>(
+    DegridArgs a{g.support, g.s, g.g_size, g.ta, g.natx, g.natx * g.naty, g.box_w, g.box_h, parts, c_scale};
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    degrid_staged_kernel<Tab><<<sms, kThreads, smem, st>>>(
         map, static_cast<const typename Tab::elem*>(c), p->iu, p->iv, p->coff, p->avals[p->asel],
-        p->atile_start, p->atile_count, out, p->status, a);
+        p->atile_start, p->atile_count, p->aitems, p->n_aitems, out, p->status, a);
     TCV_CUDA(cudaGetLastError());
     return TCV_OK;
 }
@@ -299,11 +315,11 @@ tcv_status launch_direct(const tcv_plan* p, const float2* grid, const void* c, f
 {
     const PlanGeom& g = p->g;
     if (int64_t(g.g_size) * g.g_size >= (int64_t(1) << 31)) return TCV_ERR_UNSUPPORTED;
-    DegridArgs a{g.support, g.s, g.g_size, g.ta, g.natx, g.box_w, g.box_h, 1, c_scale};
+    DegridArgs a{g.support, g.s, g.g_size, g.ta, g.natx, g.natx * g.naty, g.box_w, g.box_h, 1, c_scale};
     const uint64_t threads = uint64_t(g.n) * 32;
     degrid_direct_kernel<Tab><<<unsigned((threads + 255) / 256), 256, 0, st>>>(
         grid, static_cast<const typename Tab::elem*>(c), p->iu, p->iv, p->coff, p->avals[p->asel],
-        (unsigned long long)g.n, p->atile_start, p->atile_count, g.natx * g.naty, out, a);
+        (unsigned long long)g.n, p->atile_start, p->atile_count, g.n_groups * g.natx * g.naty, out, a);
     TCV_CUDA(cudaGetLastError());
     return TCV_OK;
 }

@@ -268,7 +268,7 @@ tcv_status tcv_init_c_raw(double freq0, double cell_size, int baseline, int w_si
 
 size_t tcv_ctype_bytes(int c_type)
 {
-    switch (c_type) {
+    switch (c_type & 0xff) {
         case TCV_C_C64: return 8;
         case TCV_C_R32: return 4;
         case TCV_C_CBF16: return 4;
@@ -282,7 +282,7 @@ size_t tcv_ctype_bytes(int c_type)
 tcv_status tcv_convert_c(const float* d_c64, int64_t c_len, int c_type, void* d_out,
                          float* c_scale_out, int64_t* imag_nonzero_out, void* stream)
 {
-    if (!d_c64 || c_len <= 0 || tcv_ctype_bytes(c_type) == 0) return TCV_ERR_ARG;
+    if (!d_c64 || c_len <= 0 || tcv_ctype_bytes(c_type) == 0 || (c_type & TCV_C_PADDED)) return TCV_ERR_ARG;
     if (c_type == TCV_C_C64) {
         if (!d_out) return TCV_ERR_ARG;
         if (d_out != d_c64)

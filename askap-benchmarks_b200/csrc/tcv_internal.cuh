@@ -78,7 +78,10 @@ struct PlanGeom {
     int g_size;
     int64_t c_len;      // table entries
     int kid_bits;       // bits of the kernel index cOffset / sSize^2
-    // gridding: output-stationary tiles
+    // kernels are processed in groups of kid_group consecutive indices (whole w-planes), sized
+    // so that one group's slice of the table stays resident in L2 while every SM works on it
+    int kid_group, n_groups, group_bits;
+    // gridding: output-stationary tiles; work cells are (group, tile)
     int tw, th, ntx, nty, max_tiles;   // max_tiles = tiles one footprint can touch
     int tile_bits, key_bits;
     // degridding: anchor tiles (footprint top-left corner), tile + halo staged in shared memory
@@ -99,16 +102,23 @@ struct tcv_plan {
     uint32_t* vals[2];             // grid pair sample indices
     void* akeys[2];                // anchor keys, n
     uint32_t* avals[2];            // anchor sample indices
-    uint32_t* tile_count;          // ntx*nty
-    uint32_t* tile_start;
-    uint32_t* atile_count;         // natx*naty
+    uint32_t* tile_count;          // samples per cell (group, tile): n_groups * ntx * nty
+    uint32_t* tile_start;          // first sorted pair of each cell
+    uint32_t* items;               // non-empty gridding cells, group-major
+    uint32_t* n_items;             // [0] = number of non-empty gridding cells
+    uint32_t* group_start;         // n_groups + 1: items of group g are [group_start[g], group_start[g+1])
+    uint32_t* atile_count;         // samples per anchor cell (group, anchor tile)
     uint32_t* atile_start;
+    uint32_t* aitems;              // non-empty anchor cells, group-major
+    uint32_t* n_aitems;
     unsigned long long* rejected;  // samples left out as out of bounds
     unsigned int* status;          // device status word: bit 0 = a bounded wait timed out
+    float2* slots;                 // degridding partial sums, n * max_tiles (pipeline kernels)
     void* cub_temp;
     size_t cub_bytes;
     int sel;                       // which buffer holds the sorted grid pairs
     int asel;                      // which buffer holds the sorted anchor pairs
+    int degrid_variant;            // TCV_DEGRID_TILES or TCV_DEGRID_ANCHOR (reference-layout tables)
 };
 
 namespace tcv {
@@ -122,6 +132,19 @@ tcv_status launch_grid(const tcv_plan* p, const float2* data, const void* c, int
                        float c_scale, float2* grid, cudaStream_t st);
 tcv_status launch_degrid(const tcv_plan* p, const float2* grid, const void* c, int c_type,
                          float c_scale, float2* out, cudaStream_t st);
+
+// degridding on the gridding plan (tcv_grid.cu), and the per-sample slot sum it ends with
+tcv_status launch_degrid_tiles(const tcv_plan* p, const float2* grid, const void* c, int c_type,
+                               float c_scale, float2* out, cudaStream_t st);
+tcv_status slot_reduce(const tcv_plan* p, float c_scale, float2* out, cudaStream_t st);
+
+// TMA pipeline kernels on prepared (padded) tables, tcv_pipe.cu
+tcv_status launch_grid_pipe(const tcv_plan* p, const float2* data, const void* table, int c_type,
+                            float c_scale, float2* grid, cudaStream_t st);
+tcv_status launch_degrid_pipe(const tcv_plan* p, const float2* grid, const void* table, int c_type,
+                              float c_scale, float2* out, cudaStream_t st);
+size_t padded_table_bytes(int64_t c_len, int s, int c_type);
+tcv_status pad_table(const void* in, int64_t c_len, int s, int c_type, void* out, cudaStream_t st);
 
 inline tcv_status cuda_status(cudaError_t e)
 {

@@ -7,15 +7,21 @@
 //               overlaps it (a footprint of sSize^2 touches up to max_tiles tiles);
 //   degridding: every anchor tile of ta x ta gets the samples whose footprint's top-left corner
 //               lies in it (each sample exactly once).
-// Within a tile, samples are ordered by kernel index cOffset / sSize^2 (w-plane major, then the
-// oversampling offsets), so that tiles progress through the table in the same order and the
-// slice of C in use stays resident in L2.  The sort is stable, so equal keys keep index order.
+// Kernel indices kid = cOffset / sSize^2 (w-plane major, then the oversampling offsets) are
+// grouped into runs of whole w-planes whose slice of the table fits in L2 with room to spare.
+// The sort key is (group, tile, kid): work cells are (group, tile), ordered group-major, so all
+// SMs work through the table one group at a time and the slice in use stays resident in L2.
+// The sort is stable, so equal keys keep index order.  The non-empty cells are compacted into
+// work lists (with per-group ranges) that persistent kernels walk.
 // Samples whose footprint or table range falls outside the grid or the table are counted and
 // left out (sentinel key, sorted past the end).
 #include "tcv_internal.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
 
 #include <algorithm>
 #include <new>
@@ -62,25 +68,49 @@ __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* 
         return;
     }
     const K kid = K(co / (s * s));
+    const uint32_t grp = uint32_t(co / (s * s) / g.kid_group);
+    const uint32_t cell0 = grp * uint32_t(g.ntx * g.nty);
     const int tx0 = int(fx / g.tw), tx1 = int((fx + s - 1) / g.tw);
     const int ty0 = int(fy / g.th), ty1 = int((fy + s - 1) / g.th);
     int t = 0;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
-            const uint32_t tile = uint32_t(ty) * g.ntx + tx;
-            kp[t] = (K(tile) << g.kid_bits) | kid;
+            const uint32_t cell = cell0 + uint32_t(ty) * g.ntx + tx;
+            kp[t] = (K(cell) << g.kid_bits) | kid;
             vp[t] = uint32_t(d);
-            atomicAdd(&tile_count[tile], 1u);
+            atomicAdd(&tile_count[cell], 1u);
             ++t;
         }
     for (; t < g.max_tiles; ++t) {
         kp[t] = sentinel;
         vp[t] = uint32_t(d);
     }
-    const uint32_t at = uint32_t(fy / g.ta) * g.natx + uint32_t(fx / g.ta);
+    const uint32_t at = grp * uint32_t(g.natx * g.naty) + uint32_t(fy / g.ta) * g.natx + uint32_t(fx / g.ta);
     akeys[d] = (K(at) << g.kid_bits) | kid;
     avals[d] = uint32_t(d);
     atomicAdd(&atile_count[at], 1u);
+}
+
+struct NonZero {
+    __host__ __device__ __forceinline__ bool operator()(const uint32_t& v) const { return v != 0; }
+};
+
+// group_start[g] = first item whose cell belongs to group g or later (items are sorted)
+__global__ void group_ranges_kernel(const uint32_t* items, const uint32_t* n_items, int n_groups,
+                                    uint32_t cells_per_group, uint32_t* group_start)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g > n_groups) return;
+    const uint32_t key = uint32_t(g) * cells_per_group;
+    uint32_t lo = 0, hi = *n_items;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (items[mid] < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    group_start[g] = lo;
 }
 
 inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
@@ -88,15 +118,20 @@ inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 template <typename K>
 size_t cub_temp_bytes(const PlanGeom& g)
 {
-    size_t a = 0, b = 0, c = 0, d = 0;
+    size_t a = 0, b = 0, c = 0, d = 0, e = 0, f = 0;
     const int64_t np = g.n * g.max_tiles;
+    const int cells = g.n_groups * g.ntx * g.nty, acells = g.n_groups * g.natx * g.naty;
     cub::DoubleBuffer<K> kb(nullptr, nullptr);
     cub::DoubleBuffer<uint32_t> vb(nullptr, nullptr);
     cub::DeviceRadixSort::SortPairs(nullptr, a, kb, vb, np, 0, g.key_bits);
     cub::DeviceRadixSort::SortPairs(nullptr, b, kb, vb, g.n, 0, g.akey_bits);
-    cub::DeviceScan::ExclusiveSum(nullptr, c, (uint32_t*)nullptr, (uint32_t*)nullptr, g.ntx * g.nty);
-    cub::DeviceScan::ExclusiveSum(nullptr, d, (uint32_t*)nullptr, (uint32_t*)nullptr, g.natx * g.naty);
-    return std::max(std::max(a, b), std::max(c, d));
+    cub::DeviceScan::ExclusiveSum(nullptr, c, (uint32_t*)nullptr, (uint32_t*)nullptr, cells);
+    cub::DeviceScan::ExclusiveSum(nullptr, d, (uint32_t*)nullptr, (uint32_t*)nullptr, acells);
+    thrust::counting_iterator<uint32_t> it(0);
+    thrust::transform_iterator<NonZero, const uint32_t*> fl((const uint32_t*)nullptr, NonZero());
+    cub::DeviceSelect::Flagged(nullptr, e, it, fl, (uint32_t*)nullptr, (uint32_t*)nullptr, cells);
+    cub::DeviceSelect::Flagged(nullptr, f, it, fl, (uint32_t*)nullptr, (uint32_t*)nullptr, acells);
+    return std::max(std::max(std::max(a, b), std::max(c, d)), std::max(e, f));
 }
 
 template <typename K>
@@ -105,8 +140,9 @@ tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_
 {
     const PlanGeom& g = p->g;
     const int64_t np = g.n * g.max_tiles;
-    TCV_CUDA(cudaMemsetAsync(p->tile_count, 0, sizeof(uint32_t) * size_t(g.ntx) * g.nty, st));
-    TCV_CUDA(cudaMemsetAsync(p->atile_count, 0, sizeof(uint32_t) * size_t(g.natx) * g.naty, st));
+    const int cells = g.n_groups * g.ntx * g.nty, acells = g.n_groups * g.natx * g.naty;
+    TCV_CUDA(cudaMemsetAsync(p->tile_count, 0, sizeof(uint32_t) * size_t(cells), st));
+    TCV_CUDA(cudaMemsetAsync(p->atile_count, 0, sizeof(uint32_t) * size_t(acells), st));
     TCV_CUDA(cudaMemsetAsync(p->rejected, 0, sizeof(unsigned long long), st));
     TCV_CUDA(cudaMemsetAsync(p->status, 0, sizeof(unsigned int), st));
     if (g.n > 0) {
@@ -129,9 +165,19 @@ tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_
         p->asel = 0;
     }
     size_t tb = p->cub_bytes;
-    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->tile_count, p->tile_start, g.ntx * g.nty, st));
+    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->tile_count, p->tile_start, cells, st));
     tb = p->cub_bytes;
-    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->atile_count, p->atile_start, g.natx * g.naty, st));
+    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->atile_count, p->atile_start, acells, st));
+    thrust::counting_iterator<uint32_t> it(0);
+    thrust::transform_iterator<NonZero, const uint32_t*> fl(p->tile_count, NonZero());
+    tb = p->cub_bytes;
+    TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, fl, p->items, p->n_items, cells, st));
+    thrust::transform_iterator<NonZero, const uint32_t*> afl(p->atile_count, NonZero());
+    tb = p->cub_bytes;
+    TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, afl, p->aitems, p->n_aitems, acells, st));
+    group_ranges_kernel<<<(g.n_groups + 1 + 127) / 128, 128, 0, st>>>(p->items, p->n_items, g.n_groups,
+                                                                       uint32_t(g.ntx * g.nty), p->group_start);
+    TCV_CUDA(cudaGetLastError());
     return TCV_OK;
 }
 
@@ -150,13 +196,24 @@ PlanGeom make_geom(int64_t n, int support, int g_size, int64_t c_len)
     g.g_size = g_size;
     g.c_len = c_len;
     const int64_t s2 = int64_t(g.s) * g.s;
-    g.kid_bits = bits_for(uint64_t(c_len / s2));
+    const int64_t nk = (c_len + s2 - 1) / s2;
+    g.kid_bits = bits_for(uint64_t(nk));
+    // kernels per group: whole planes of 64 (8 x 8 oversampling) whose complex64 slice is about
+    // 32 MiB, a quarter of the 126 MB L2
+    const int64_t per_kernel = s2 * 8;
+    int64_t kg = ((int64_t(32) << 20) / per_kernel) / 64 * 64;
+    if (kg < 64) kg = 64;
+    if (kg > nk) kg = nk < 1 ? 1 : nk;
+    g.kid_group = int(kg);
+    g.n_groups = int((nk + kg - 1) / kg);
+    if (g.n_groups < 1) g.n_groups = 1;
+    g.group_bits = bits_for(uint64_t(g.n_groups - 1));
     g.tw = 64;
     g.th = 64;
     g.ntx = (g_size + g.tw - 1) / g.tw;
     g.nty = (g_size + g.th - 1) / g.th;
     g.max_tiles = ((g.s + g.tw - 2) / g.tw + 1) * ((g.s + g.th - 2) / g.th + 1);
-    g.tile_bits = bits_for(uint64_t(g.ntx) * g.nty - 1);
+    g.tile_bits = bits_for(uint64_t(g.n_groups) * g.ntx * g.nty - 1);
     g.key_bits = g.tile_bits + g.kid_bits + 1;
 
     constexpr size_t kSmemBudget = 220 * 1024;  // of 227 KB per CTA; the rest holds partial sums
@@ -176,7 +233,7 @@ PlanGeom make_geom(int64_t n, int support, int g_size, int64_t c_len)
     }
     g.natx = (g_size + g.ta - 1) / g.ta;
     g.naty = (g_size + g.ta - 1) / g.ta;
-    g.atile_bits = bits_for(uint64_t(g.natx) * g.naty - 1);
+    g.atile_bits = bits_for(uint64_t(g.n_groups) * g.natx * g.naty - 1);
     g.akey_bits = g.atile_bits + g.kid_bits + 1;
     g.key64 = g.key_bits > 32 || g.akey_bits > 32;
     g.degrid_parts = 4;
@@ -192,9 +249,11 @@ size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out)
     size_t b = 0;
     b += 2 * align_up(np * ks) + 2 * align_up(np * 4);
     b += 2 * align_up(size_t(g.n) * ks) + 2 * align_up(size_t(g.n) * 4);
-    b += 2 * align_up(size_t(g.ntx) * g.nty * 4);
-    b += 2 * align_up(size_t(g.natx) * g.naty * 4);
+    const size_t cells = size_t(g.n_groups) * g.ntx * g.nty, acells = size_t(g.n_groups) * g.natx * g.naty;
+    b += 3 * align_up(cells * 4) + align_up(4) + align_up(size_t(g.n_groups + 1) * 4);
+    b += 3 * align_up(acells * 4) + align_up(4);
     b += align_up(sizeof(unsigned long long)) + align_up(sizeof(unsigned int));
+    b += align_up(np * sizeof(float2));
     b += align_up(cb);
     return b;
 }
@@ -246,16 +305,24 @@ tcv_status tcv_plan_build(tcv_plan** plan_out, const int32_t* d_iu, const int32_
     p->akeys[1] = take(size_t(g.n) * ks);
     p->avals[0] = static_cast<uint32_t*>(take(size_t(g.n) * 4));
     p->avals[1] = static_cast<uint32_t*>(take(size_t(g.n) * 4));
-    p->tile_count = static_cast<uint32_t*>(take(size_t(g.ntx) * g.nty * 4));
-    p->tile_start = static_cast<uint32_t*>(take(size_t(g.ntx) * g.nty * 4));
-    p->atile_count = static_cast<uint32_t*>(take(size_t(g.natx) * g.naty * 4));
-    p->atile_start = static_cast<uint32_t*>(take(size_t(g.natx) * g.naty * 4));
+    const size_t cells = size_t(g.n_groups) * g.ntx * g.nty, acells = size_t(g.n_groups) * g.natx * g.naty;
+    p->tile_count = static_cast<uint32_t*>(take(cells * 4));
+    p->tile_start = static_cast<uint32_t*>(take(cells * 4));
+    p->items = static_cast<uint32_t*>(take(cells * 4));
+    p->n_items = static_cast<uint32_t*>(take(4));
+    p->group_start = static_cast<uint32_t*>(take(size_t(g.n_groups + 1) * 4));
+    p->atile_count = static_cast<uint32_t*>(take(acells * 4));
+    p->atile_start = static_cast<uint32_t*>(take(acells * 4));
+    p->aitems = static_cast<uint32_t*>(take(acells * 4));
+    p->n_aitems = static_cast<uint32_t*>(take(4));
     p->rejected = static_cast<unsigned long long*>(take(sizeof(unsigned long long)));
     p->status = static_cast<unsigned int*>(take(sizeof(unsigned int)));
+    p->slots = static_cast<float2*>(take(np * sizeof(float2)));
     p->cub_temp = take(cb);
     p->iu = d_iu;
     p->iv = d_iv;
     p->coff = d_coff;
+    p->degrid_variant = TCV_DEGRID_TILES;
     p->cub_bytes = cb;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const tcv_status s = g.key64 ? build<uint64_t>(p, d_iu, d_iv, d_coff, st)
@@ -297,7 +364,7 @@ tcv_status tcv_plan_info(const tcv_plan* plan, int* tile_w, int* tile_h, int* an
     if (tile_h) *tile_h = plan->g.th;
     if (anchor) *anchor = plan->g.ta;
     if (degrid_mode) *degrid_mode = plan->g.degrid_mode;
-    if (n_tiles) *n_tiles = plan->g.ntx * plan->g.nty;
+    if (n_tiles) *n_tiles = plan->g.ntx * plan->g.nty * plan->g.n_groups;
     return TCV_OK;
 }
 
@@ -308,6 +375,9 @@ tcv_status tcv_plan_grid(const tcv_plan* plan, const float* d_data, const void* 
 {
     if (!plan || !d_c || !d_grid || (plan->g.n > 0 && !d_data)) return TCV_ERR_ARG;
     if (tcv_ctype_bytes(c_type) == 0) return TCV_ERR_ARG;
+    if (c_type & TCV_C_PADDED)
+        return launch_grid_pipe(plan, reinterpret_cast<const float2*>(d_data), d_c, c_type & 0xff, c_scale,
+                                reinterpret_cast<float2*>(d_grid), static_cast<cudaStream_t>(stream));
     return launch_grid(plan, reinterpret_cast<const float2*>(d_data), d_c, c_type, c_scale,
                        reinterpret_cast<float2*>(d_grid), static_cast<cudaStream_t>(stream));
 }
@@ -317,8 +387,25 @@ tcv_status tcv_plan_degrid(const tcv_plan* plan, const float* d_grid, const void
 {
     if (!plan || !d_c || !d_grid || (plan->g.n > 0 && !d_data)) return TCV_ERR_ARG;
     if (tcv_ctype_bytes(c_type) == 0) return TCV_ERR_ARG;
+    if (c_type & TCV_C_PADDED) {
+        if (plan->g.n == 0) return TCV_OK;
+        return launch_degrid_pipe(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type & 0xff, c_scale,
+                                  reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
+    }
+    if (plan->degrid_variant == TCV_DEGRID_TILES) {
+        if (plan->g.n == 0) return TCV_OK;
+        return launch_degrid_tiles(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type, c_scale,
+                                   reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
+    }
     return launch_degrid(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type, c_scale,
                          reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
+}
+
+tcv_status tcv_plan_set_degrid_variant(tcv_plan* plan, int variant)
+{
+    if (!plan || (variant != TCV_DEGRID_TILES && variant != TCV_DEGRID_ANCHOR)) return TCV_ERR_ARG;
+    plan->degrid_variant = variant;
+    return TCV_OK;
 }
 
 tcv_status tcv_grid_raw(const float* d_data, int64_t n, int support, const void* d_c, int c_type,

@@ -24,6 +24,9 @@ STATUS_NAMES = {
 C64, R32, CBF16, RBF16, CF16, RF16 = range(6)
 CTYPE_NAMES = {C64: "c64", R32: "r32", CBF16: "cbf16", RBF16: "rbf16", CF16: "cf16", RF16: "rf16"}
 CTYPE_BY_NAME = {v: k for k, v in CTYPE_NAMES.items()}
+PADDED = 0x100          # TCV_C_PADDED: prepared (TMA) table layout
+PATH_TMA, PATH_DIRECT = 0, 1
+DEGRID_TILES, DEGRID_ANCHOR = 0, 1
 
 
 class TcvError(RuntimeError):
@@ -73,6 +76,8 @@ SIGNATURES = {
     "tcv_init_c_scratch_bytes": (_S, []),
     "tcv_init_c_raw": (_I, [_D, _D, _I, _I, _P, _P, _P, _P]),
     "tcv_convert_c": (_I, [_P, _I64, _I, _P, _P, _P, _P]),
+    "tcv_table_bytes": (_S, [_I64, _I, _I]),
+    "tcv_prepare_table": (_I, [_P, _I64, _I, _I, _P, _P, _P, _P]),
     "tcv_init_uvw_raw": (_I, [_I64, _I, ctypes.c_uint64, _P, _P, _P, _P]),
     "tcv_init_offsets_raw": (_I, [_P, _P, _P, _I64, _P, _I, _D, _D, _I, _I, _I, _I, _P, _P, _P, _P]),
     "tcv_plan_workspace_bytes": (_S, [_I64, _I, _I, _I64]),
@@ -81,6 +86,7 @@ SIGNATURES = {
     "tcv_plan_degrid": (_I, [_P, _P, _P, _I, _F, _P, _P]),
     "tcv_plan_rejected": (_I, [_P, _P, _P]),
     "tcv_plan_status": (_I, [_P, _P]),
+    "tcv_plan_set_degrid_variant": (_I, [_P, _I]),
     "tcv_plan_info": (_I, [_P, _P, _P, _P, _P, _P]),
     "tcv_plan_destroy": (None, [_P]),
     "tcv_grid_raw": (_I, [_P, _I64, _I, _P, _I, _F, _I64, _P, _P, _P, _P, _I, _P, _S, _P]),
@@ -106,6 +112,8 @@ SIGNATURES = {
     "tcv_n_data": (_I64, [_P]),
     "tcv_updates_per_pass": (_D, [_P]),
     "tcv_set_ctype": (_I, [_P, _I]),
+    "tcv_set_path": (_I, [_P, _I]),
+    "tcv_get_path": (_I, [_P]),
     "tcv_set_data": (_I, [_P, _P, _I64]),
     "tcv_get_data": (_I, [_P, _P, _I64]),
     "tcv_get_outdata": (_I, [_P, _P, _I64]),

@@ -95,6 +95,23 @@ class Benchmark:
             c_type = _lib.CTYPE_BY_NAME[c_type]
         check(lib().tcv_set_ctype(self._ctx, int(c_type)), "tcv_set_ctype", self._ctx)
 
+    def set_path(self, path: int | str):
+        """Kernel family: "tma" (prepared table, default) or "direct" (reference-layout table)."""
+        if isinstance(path, str):
+            path = {"tma": _lib.PATH_TMA, "direct": _lib.PATH_DIRECT}[path]
+        check(lib().tcv_set_path(self._ctx, int(path)), "tcv_set_path", self._ctx)
+
+    def set_degrid_variant(self, variant: int | str):
+        """Degridding kernel on the direct path: "tiles" (default) or "anchor"."""
+        if isinstance(variant, str):
+            variant = {"tiles": _lib.DEGRID_TILES, "anchor": _lib.DEGRID_ANCHOR}[variant]
+        plan = ctypes.c_void_p(self.device_buffers().plan)
+        check(lib().tcv_plan_set_degrid_variant(plan, int(variant)), "tcv_plan_set_degrid_variant")
+
+    @property
+    def path(self) -> int:
+        return lib().tcv_get_path(self._ctx)
+
     @property
     def overSample(self) -> int:
         return lib().tcv_over_sample(self._ctx)

@@ -104,6 +104,9 @@ class Plan:
         check(lib().tcv_plan_degrid(self.handle, _ptr(grid), _ptr(c), c_type, c_scale, _ptr(out),
                                     _stream(stream)), "tcv_plan_degrid")
 
+    def set_degrid_variant(self, variant: int):
+        check(lib().tcv_plan_set_degrid_variant(self.handle, variant), "tcv_plan_set_degrid_variant")
+
     def rejected(self, stream=None) -> int:
         r = ctypes.c_int64()
         check(lib().tcv_plan_rejected(self.handle, ctypes.byref(r), _stream(stream)),

@@ -49,6 +49,9 @@ def parse_args():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="c2", choices=sorted(PROBLEMS))
     p.add_argument("--form", default="c64", help="table storage form (c64 = plain FP32)")
+    p.add_argument("--path", default="direct", choices=["tma", "direct"], help="kernel family")
+    p.add_argument("--degrid", default="tiles", choices=["tiles", "anchor"],
+                   help="degridding kernel on the direct path")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=4.0, help="target wall time of the CPU sample")
     return p.parse_args()
@@ -209,6 +212,7 @@ def b200_arm(args):
 
     b = tconvolve.Benchmark(**prob.kwargs(), device=local)
     b.set_stream(stream.cuda_stream)
+    b.set_path(args.path)
     b.init()
     if form != tconvolve.C64:
         b.set_ctype(form)
@@ -226,6 +230,8 @@ def b200_arm(args):
     sp = ctypes.c_void_p(stream.cuda_stream)
     P = ctypes.c_void_p
 
+    dvariant = {"tiles": tconvolve._lib.DEGRID_TILES, "anchor": tconvolve._lib.DEGRID_ANCHOR}[args.degrid]
+
     def step(evs=None):
         sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)  # the capture stream too
         plan = ctypes.c_void_p()
@@ -233,6 +239,7 @@ def b200_arm(args):
             evs[0].record(stream)
         check(L.tcv_plan_build(ctypes.byref(plan), P(bufs.iu), P(bufs.iv), P(bufs.coff), n, support,
                                prob.g_size, c_len, P(work.data_ptr()), wbytes, sp), "plan")
+        L.tcv_plan_set_degrid_variant(plan, dvariant)
         if evs:
             evs[1].record(stream)
         check(L.tcv_plan_grid(plan, P(bufs.data), P(bufs.c_active), bufs.c_type, bufs.c_scale,
@@ -298,6 +305,7 @@ def b200_arm(args):
         check(L.tcv_plan_build(ctypes.byref(plan), P(d_iu.data_ptr()), P(d_iv.data_ptr()),
                                P(d_co.data_ptr()), n, support, prob.g_size, c_len,
                                P(work.data_ptr()), wbytes, sp), "plan")
+        L.tcv_plan_set_degrid_variant(plan, dvariant)
         check(L.tcv_plan_grid(plan, P(d_vis.data_ptr()), P(bufs.c_active), bufs.c_type, bufs.c_scale,
                               P(bufs.grid), sp), "grid")
         check(L.tcv_plan_degrid(plan, P(bufs.grid), P(bufs.c_active), bufs.c_type, bufs.c_scale,
@@ -339,7 +347,12 @@ def b200_arm(args):
     peak, peak_kind = measured_hbm_peak()
     achieved = ALG_BYTES[dom] * updates / (dom_ms * 1e-3) / 1e9
     traffic = ncu_traffic(dom)
-    kname = {"grid": "grid_tile_kernel", "degrid": "degrid_staged_kernel"}[dom]
+    tma = bool(bufs.c_type & tconvolve._lib.PADDED)
+    kname = {("grid", True): "pipe_kernel<gridding> (TMA pipeline)",
+             ("degrid", True): "pipe_kernel<degridding> + slot_reduce_kernel (TMA pipeline)",
+             ("grid", False): "grid_tile_kernel",
+             ("degrid", False): ("degrid_tile_kernel + slot_reduce_kernel" if args.degrid == "tiles"
+                                 else "degrid_staged_kernel")}[(dom, tma)]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -355,7 +368,8 @@ def b200_arm(args):
             "config": {"workload": f"{args.workload}: {prob.n_samples} samples x {prob.n_chan} chan, "
                                    f"gSize {prob.g_size}, wSize {prob.w_size}, support {support} "
                                    f"({2 * support + 1}^2 footprint), cellSize {prob.cell_size}",
-                       "form": args.form, "parallelism": f"replicas x{world}",
+                       "form": args.form, "path": args.path, "degrid": args.degrid,
+                       "parallelism": f"replicas x{world}",
                        "l2": f"{L2_FLUSH_BYTES >> 20} MiB buffer written between timed steps",
                        "step": "binning plan + gridding pass + degridding pass"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -56,11 +56,14 @@ typedef enum tcv_ctype {
     TCV_C_CBF16 = 2,/* complex bfloat16 (4 B/entry) */
     TCV_C_RBF16 = 3,/* real bfloat16 (2 B/entry) */
     TCV_C_CF16 = 4, /* complex float16 x 2^e (4 B/entry), power-of-two scale passed as c_scale */
-    TCV_C_RF16 = 5  /* real float16 x 2^e (2 B/entry) */
+    TCV_C_RF16 = 5, /* real float16 x 2^e (2 B/entry) */
+    /* Flag: the table is in the prepared (padded) layout made by tcv_prepare_table, rows of
+     * sSize entries padded to a 16-byte pitch; the kernels then stream it with TMA. */
+    TCV_C_PADDED = 0x100
 } tcv_ctype;
 
 const char *tcv_status_string(tcv_status s);
-/* Bytes per table entry of a tcv_ctype, 0 for an unknown code. */
+/* Bytes per table entry of a tcv_ctype (the TCV_C_PADDED flag is ignored), 0 for an unknown code. */
 size_t tcv_ctype_bytes(int c_type);
 /* Library version string and the compute capability it was built for ("sm_100a"). */
 const char *tcv_version(void);
@@ -89,6 +92,18 @@ tcv_status tcv_init_c_raw(double freq0, double cell_size, int baseline, int w_si
  * (may be NULL) receives the number of entries that were not (synchronises the stream). */
 tcv_status tcv_convert_c(const float *d_c64, int64_t c_len, int c_type, void *d_out,
                          float *c_scale_out, int64_t *imag_nonzero_out, void *stream);
+
+/* Bytes of a table of c_len entries in storage type c_type; with TCV_C_PADDED set, in the
+ * prepared layout for footprints of sSize = 2*support+1 (0 if c_len is not a multiple of sSize^2). */
+size_t tcv_table_bytes(int64_t c_len, int support, int c_type);
+/* Prepare a table for the TMA pipeline kernels: convert the complex64 reference-layout table to
+ * storage type c_type (as tcv_convert_c) and write it in the padded layout to d_out
+ * (tcv_table_bytes(c_len, support, c_type | TCV_C_PADDED) bytes).  Set-up path: allocates a
+ * temporary for the reduced forms and synchronises the stream.  Pass the result to the kernels
+ * with c_type | TCV_C_PADDED. */
+tcv_status tcv_prepare_table(const float *d_c64, int64_t c_len, int support, int c_type,
+                             void *d_out, float *c_scale_out, int64_t *imag_nonzero_out,
+                             void *stream);
 
 /* u, v, w for n_samples samples from the reference's K&R generator (Benchmark.cc:46-80), state0 =
  * generator state before the first draw (1 in the reference), computed in parallel by jump-ahead. */
@@ -130,6 +145,12 @@ tcv_status tcv_plan_rejected(const tcv_plan *plan, int64_t *rejected_out, void *
 /* TCV_ERR_TIMEOUT if a kernel run with this plan gave up a bounded wait, else TCV_OK
  * (synchronises the stream). */
 tcv_status tcv_plan_status(const tcv_plan *plan, void *stream);
+/* Degridding kernel for reference-layout tables: TCV_DEGRID_TILES (default; the adjoint of the
+ * gridding tiles, grid values in registers) or TCV_DEGRID_ANCHOR (anchor tiles with the grid
+ * region staged in shared memory by TMA).  Prepared (TCV_C_PADDED) tables always use the TMA
+ * pipeline kernels. */
+enum { TCV_DEGRID_TILES = 0, TCV_DEGRID_ANCHOR = 1 };
+tcv_status tcv_plan_set_degrid_variant(tcv_plan *plan, int variant);
 /* Tile geometry chosen for the plan: grid tile width/height, anchor tile, degrid mode
  * (0 = TMA-staged tiles, 1 = direct), number of grid tiles, max samples in one grid tile. */
 tcv_status tcv_plan_info(const tcv_plan *plan, int *tile_w, int *tile_h, int *anchor,
@@ -211,6 +232,11 @@ int64_t tcv_n_data(const tcv_ctx *ctx);        /* nSamples * nChan */
 double tcv_updates_per_pass(const tcv_ctx *ctx); /* nSamples * nChan * sSize^2 */
 /* Switch the table storage type used by run_grid / run_degrid (converts once, keeps the C64 table). */
 tcv_status tcv_set_ctype(tcv_ctx *ctx, int c_type);
+/* Kernel family used by run_grid / run_degrid: the TMA pipeline kernels on the prepared table
+ * (default) or the kernels that read the reference-layout table directly. */
+enum { TCV_PATH_TMA = 0, TCV_PATH_DIRECT = 1 };
+tcv_status tcv_set_path(tcv_ctx *ctx, int path);
+int tcv_get_path(const tcv_ctx *ctx);
 
 /* Host <-> device transfers of the context's buffers (synchronous; host pointers). */
 tcv_status tcv_set_data(tcv_ctx *ctx, const float *vis, int64_t n);          /* n complex */
@@ -235,8 +261,8 @@ typedef struct tcv_device_buffers {
     int32_t *iu, *iv, *coff;
     double *u, *v, *w;
     const tcv_plan *plan;
-    float c_scale;
-    int32_t c_type;
+    float c_scale;    /* c_scale to pass with c_active */
+    int32_t c_type;   /* type code of c_active, TCV_C_PADDED set on the TMA path */
 } tcv_device_buffers;
 tcv_status tcv_get_device_buffers(tcv_ctx *ctx, tcv_device_buffers *out);
 

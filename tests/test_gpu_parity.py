@@ -18,6 +18,21 @@ from tconvolve.workload import PROBLEMS, normal_vis
 pytestmark = pytest.mark.gpu
 
 
+KERNELS = ["tma", "direct-tiles", "direct-anchor"]
+
+
+def _use(b, kernels):
+    """Select the kernel family: TMA pipeline, or direct with the tiles/anchor degridding kernel."""
+    path, _, variant = kernels.partition("-")
+    b.set_path(path)
+    return variant
+
+
+def _after_init(b, variant):
+    if variant:
+        b.set_degrid_variant(variant)
+
+
 def _table_close(gpu_c, ref_c):
     a = gpu_c.view(np.float32)
     b = ref_c.view(np.float32)
@@ -29,13 +44,16 @@ def _table_close(gpu_c, ref_c):
     return diff.size
 
 
+@pytest.mark.parametrize("kernels", KERNELS)
 @pytest.mark.parametrize("cfg", ["g1", "g2", "c1"])
 @pytest.mark.parametrize("vis_kind", ["ones", "normal"])
-def test_benchmark_parity(tcv, orc, golden, cuda_ok, cfg, vis_kind):
+def test_benchmark_parity(tcv, orc, golden, cuda_ok, cfg, vis_kind, kernels):
     prob = PROBLEMS[cfg]
     ref = golden["runs"][f"{cfg}_{vis_kind}"]
     b = tcv.Benchmark(**prob.kwargs())
+    variant = _use(b, kernels)
     b.init()
+    _after_init(b, variant)
     if vis_kind == "normal":
         b.set_data(normal_vis(prob.n_data(), VIS_SEED))
     b.runGrid()
@@ -63,12 +81,15 @@ def test_benchmark_parity(tcv, orc, golden, cuda_ok, cfg, vis_kind):
     b.close()
 
 
-def test_default_config_full_size(tcv, orc, golden, cuda_ok):
+@pytest.mark.parametrize("kernels", KERNELS)
+def test_default_config_full_size(tcv, orc, golden, cuda_ok, kernels):
     """The reference default (160 k samples, 4096^2 grid, 129^2 footprints) at full size."""
     prob = PROBLEMS["c2"]
     ref = golden["runs"]["c2_normal"]
     b = tcv.Benchmark(**prob.kwargs())
+    variant = _use(b, kernels)
     b.init()
+    _after_init(b, variant)
     vis = normal_vis(prob.n_data(), VIS_SEED)
     b.set_data(vis)
     b.runGrid()
@@ -134,15 +155,18 @@ def test_full_size_properties(tcv, cuda_ok):
     assert np.array_equal(b.outdata(), dg.astype(np.complex64))
 
 
+@pytest.mark.parametrize("kernels", KERNELS)
 @pytest.mark.parametrize("form,bound", [("r32", 0.0), ("cbf16", 6e-3), ("rbf16", 6e-3),
                                          ("cf16", 8e-4), ("rf16", 8e-4)])
-def test_reduced_table_forms(tcv, orc, cuda_ok, form, bound):
+def test_reduced_table_forms(tcv, orc, cuda_ok, form, bound, kernels):
     """Table storage forms against the FP64 oracle.  r32 must equal the complex64 form bit for
     bit (the attic table is real); the 16-bit forms stay within the stated relative L2."""
     prob = PROBLEMS["c1"]
     vis = normal_vis(prob.n_data(), VIS_SEED)
     b = tcv.Benchmark(**prob.kwargs())
+    variant = _use(b, kernels)
     b.init()
+    _after_init(b, variant)
     b.set_data(vis)
     b.runGrid()
     b.runDegrid()
@@ -231,8 +255,13 @@ def test_raw_out_of_bounds_samples_are_rejected(tcv, orc, cuda_ok):
     plan.grid(dvis, dc, tcv.C64, grid)
     out = torch.full((n,), 7 + 7j, dtype=torch.complex64, device="cuda")
     plan.degrid(grid, dc, tcv.C64, out)
+    out_anchor = torch.full((n,), 7 + 7j, dtype=torch.complex64, device="cuda")
+    plan.set_degrid_variant(1)
+    plan.degrid(grid, dc, tcv.C64, out_anchor)
     torch.cuda.synchronize()
     assert plan.rejected() == bad.size
+    assert np.all(out_anchor.cpu().numpy()[bad] == 0)
+    assert orc.rel_l2(out_anchor.cpu().numpy(), out.cpu().numpy()) <= 1e-6
     keep = np.ones(n, bool)
     keep[bad] = False
     ref = np.zeros(prob.g_size ** 2, np.complex64)
@@ -285,7 +314,9 @@ def test_direct_degrid_path(tcv, orc, cuda_ok, g_size, cell, w_size):
 
     prob = Problem("direct", 3000, w_size, 1, g_size, cell)
     b = tcv.Benchmark(**prob.kwargs())
+    b.set_path("direct")
     b.init()
+    b.set_degrid_variant("anchor")
     vis = normal_vis(prob.n_data(), 4)
     b.set_data(vis)
     b.runGrid()
@@ -295,6 +326,55 @@ def test_direct_degrid_path(tcv, orc, cuda_ok, g_size, cell, w_size):
     r = orc.run_plain(oracle_config(orc, prob), vis=vis, threads=8)
     assert orc.rel_l2(b.grid(), r["grid"]) <= REL_L2_FP32
     assert orc.rel_l2(b.outdata(), r["outdata"]) <= REL_L2_FP32
+
+
+@pytest.mark.parametrize("form", ["c64", "r32", "rbf16"])
+def test_raw_prepared_table(tcv, orc, cuda_ok, form):
+    """The TMA kernels through the raw entry points: a table prepared by tcv_prepare_table, passed
+    with the TCV_C_PADDED flag, gives the same grid and samples as the reference-layout kernels."""
+    import ctypes
+
+    import torch
+
+    from tconvolve import raw
+    from tconvolve._lib import PADDED, check, lib
+
+    prob = PROBLEMS["c1"]
+    c, support, iu, iv, co = _setup(orc, prob)
+    vis = normal_vis(iu.size, 31)
+    dvis, dc, diu, div, dco = _dev(vis, c, iu, iv, co)
+    t = tcv.CTYPE_BY_NAME[form]
+    nbytes = lib().tcv_table_bytes(c.size, support, t | PADDED)
+    assert nbytes > 0
+    padded = torch.zeros(nbytes, dtype=torch.uint8, device="cuda")
+    scale, nz = ctypes.c_float(), ctypes.c_int64()
+    check(lib().tcv_prepare_table(ctypes.c_void_p(dc.data_ptr()), c.size, support, t,
+                                  ctypes.c_void_p(padded.data_ptr()), ctypes.byref(scale),
+                                  ctypes.byref(nz), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+          "prepare")
+    assert nz.value == 0
+    if form == "c64":
+        flat, fscale = dc, 1.0
+    else:
+        flat, fscale, _ = raw.convert_c(dc, t)
+    plan = raw.Plan(diu, div, dco, support, prob.g_size, c.size)
+    g_tma = torch.zeros(prob.g_size ** 2, dtype=torch.complex64, device="cuda")
+    g_dir = torch.zeros_like(g_tma)
+    plan.grid(dvis, padded, t | PADDED, g_tma, c_scale=scale.value)
+    plan.grid(dvis, flat, t, g_dir, c_scale=fscale)
+    o_tma = torch.empty_like(dvis)
+    o_dir = torch.empty_like(dvis)
+    plan.degrid(g_dir, padded, t | PADDED, o_tma, c_scale=scale.value)
+    plan.degrid(g_dir, flat, t, o_dir, c_scale=fscale)
+    torch.cuda.synchronize()
+    assert plan.status() == 0
+    a, b = g_tma.cpu().numpy(), g_dir.cpu().numpy()
+    assert orc.rel_l2(a, b) <= 1e-6
+    assert orc.rel_l2(o_tma.cpu().numpy(), o_dir.cpu().numpy()) <= 1e-6
+    if form == "c64":
+        ref = np.zeros(prob.g_size ** 2, np.complex64)
+        orc.grid_f32(vis, support, c, co, iu, iv, ref, prob.g_size)
+        assert orc.rel_l2(a, ref) <= REL_L2_FP32
 
 
 def test_plan_reuse_and_streams(tcv, orc, cuda_ok):
