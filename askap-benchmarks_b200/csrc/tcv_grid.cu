@@ -78,11 +78,19 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
                 const bool colok = unsigned(dx) < unsigned(s);
                 const float2 dv = make_float2(q.x, q.y);
                 const typename Tab::elem* cp = ctab + (sm_coff[j] + dy0 * s + dx);
+                if (dy0 >= 0 && dy0 + kRowsPerWarp <= s) {
+                    // every row of the block is inside the footprint: only the column test remains
+                    if (colok) {
 #pragma unroll
-                for (int r = 0; r < kRowsPerWarp; ++r) {
-                    if (colok && unsigned(dy0 + r) < unsigned(s)) {
-                        const float2 c = Tab::load(cp + r * s);
-                        cmac<Tab::kReal>(acc[r], dv, c);
+                        for (int r = 0; r < kRowsPerWarp; ++r) cmac<Tab::kReal>(acc[r], dv, Tab::load(cp + r * s));
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < kRowsPerWarp; ++r) {
+                        if (colok && unsigned(dy0 + r) < unsigned(s)) {
+                            const float2 c = Tab::load(cp + r * s);
+                            cmac<Tab::kReal>(acc[r], dv, c);
+                        }
                     }
                 }
             }
@@ -153,13 +161,24 @@ degrid_tile_kernel(const float2* __restrict__ grid, const typename Tab::elem* __
                     const int dx = gx - fx;
                     const bool colok = unsigned(dx) < unsigned(s);
                     const typename Tab::elem* cp = ctab + (q.w + dy0 * s + dx);
+                    // four independent partial sums keep the FMA chains short
+                    float2 pv[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
+                                    make_float2(0.f, 0.f)};
+                    if (dy0 >= 0 && dy0 + kRowsPerWarp <= s) {
+                        if (colok) {
 #pragma unroll
-                    for (int r = 0; r < kRowsPerWarp; ++r) {
-                        if (colok && unsigned(dy0 + r) < unsigned(s)) {
-                            const float2 c = Tab::load(cp + r * s);
-                            cmac<Tab::kReal>(v, gv[r], c);
+                            for (int r = 0; r < kRowsPerWarp; ++r) cmac<Tab::kReal>(pv[r & 3], gv[r], Tab::load(cp + r * s));
+                        }
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < kRowsPerWarp; ++r) {
+                            if (colok && unsigned(dy0 + r) < unsigned(s)) {
+                                const float2 c = Tab::load(cp + r * s);
+                                cmac<Tab::kReal>(pv[r & 3], gv[r], c);
+                            }
                         }
                     }
+                    v = make_float2((pv[0].x + pv[1].x) + (pv[2].x + pv[3].x), (pv[0].y + pv[1].y) + (pv[2].y + pv[3].y));
 #pragma unroll
                     for (int o = 16; o; o >>= 1) {
                         v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
