@@ -194,7 +194,7 @@ def b200_arm(args):
     import torch.distributed as dist
 
     import tconvolve
-    from tconvolve import raw
+    from tconvolve import replicas
     from tconvolve._lib import check, lib
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -331,13 +331,13 @@ def b200_arm(args):
     if int(torch.count_nonzero(torch.isnan(torch.view_as_real(h_out)))) != 0:
         raise RuntimeError("non-finite degridded output")
 
-    # max over ranks of the device time
+    # max over ranks of the device time; replicas of one problem must agree bit for bit
     mean_step = statistics.mean(step_ms)
     e2e_mean = statistics.mean(e2e_ms)
+    replicas_agree = True
     if world > 1:
-        t = torch.tensor([mean_step, e2e_mean, t_wall], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        mean_step, e2e_mean, t_wall = (float(x) for x in t.tolist())
+        mean_step, e2e_mean, t_wall = replicas.max_over_ranks([mean_step, e2e_mean, t_wall], device="cuda")
+        replicas_agree = replicas.cross_check(replicas.checksum(h_out.numpy()), device="cuda")
     value = world * 2 * updates / (mean_step * 1e-3)
     e2e_value = world * 2 * updates / (e2e_mean * 1e-3)
 
@@ -386,6 +386,7 @@ def b200_arm(args):
             "gpu_launches": launches_per_step * args.steps if launches_per_step else None,
             "launches_per_step": launches_per_step,
             "wall_s_timed_loop": t_wall,
+            "replicas_agree": replicas_agree,
             "clocks": clk,
         }
         if cpu:
