@@ -126,6 +126,8 @@ namespace tcv {
 // Host helpers implemented in tcv_plan.cu / tcv_api.cu
 PlanGeom make_geom(int64_t n, int support, int g_size, int64_t c_len);
 size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out);
+tcv_status plan_init(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff, int64_t n,
+                     int support, int g_size, int64_t c_len, void* d_work, size_t work_bytes, cudaStream_t st);
 
 // Launchers implemented in tcv_grid.cu / tcv_degrid.cu
 tcv_status launch_grid(const tcv_plan* p, const float2* data, const void* c, int c_type,

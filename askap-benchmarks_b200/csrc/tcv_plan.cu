@@ -271,23 +271,23 @@ size_t tcv_plan_workspace_bytes(int64_t n, int support, int g_size, int64_t c_le
     return plan_bytes(g, nullptr);
 }
 
-tcv_status tcv_plan_build(tcv_plan** plan_out, const int32_t* d_iu, const int32_t* d_iv,
-                          const int32_t* d_coff, int64_t n, int support, int g_size,
-                          int64_t c_len, void* d_work, size_t work_bytes, void* stream)
+}  // extern "C"
+
+namespace tcv {
+
+// Fill *p (a caller-owned object) with a plan built in d_work.
+tcv_status plan_init(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff, int64_t n,
+                     int support, int g_size, int64_t c_len, void* d_work, size_t work_bytes, cudaStream_t st)
 {
-    if (!plan_out || n < 0 || support < 0 || g_size < 1 || c_len < 1) return TCV_ERR_ARG;
+    if (!p || n < 0 || support < 0 || g_size < 1 || c_len < 1) return TCV_ERR_ARG;
     if (n > 0 && (!d_iu || !d_iv || !d_coff)) return TCV_ERR_ARG;
     if (n >= (int64_t(1) << 32) / 16) return TCV_ERR_UNSUPPORTED;  // 32-bit sample indices
     if (!d_work) return TCV_ERR_ARG;
-    tcv_plan* p = new (std::nothrow) tcv_plan{};
-    if (!p) return TCV_ERR_OOM;
+    *p = tcv_plan{};
     p->g = make_geom(n, support, g_size, c_len);
     size_t cb = 0;
     const size_t need = plan_bytes(p->g, &cb);
-    if (work_bytes < need) {
-        delete p;
-        return TCV_ERR_WORKSPACE;
-    }
+    if (work_bytes < need) return TCV_ERR_WORKSPACE;
     const PlanGeom& g = p->g;
     const size_t ks = g.key64 ? 8 : 4;
     const size_t np = size_t(g.n) * g.max_tiles;
@@ -319,14 +319,27 @@ tcv_status tcv_plan_build(tcv_plan** plan_out, const int32_t* d_iu, const int32_
     p->status = static_cast<unsigned int*>(take(sizeof(unsigned int)));
     p->slots = static_cast<float2*>(take(np * sizeof(float2)));
     p->cub_temp = take(cb);
+    p->cub_bytes = cb;
     p->iu = d_iu;
     p->iv = d_iv;
     p->coff = d_coff;
     p->degrid_variant = TCV_DEGRID_TILES;
-    p->cub_bytes = cb;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const tcv_status s = g.key64 ? build<uint64_t>(p, d_iu, d_iv, d_coff, st)
-                                 : build<uint32_t>(p, d_iu, d_iv, d_coff, st);
+    return g.key64 ? build<uint64_t>(p, d_iu, d_iv, d_coff, st) : build<uint32_t>(p, d_iu, d_iv, d_coff, st);
+}
+
+}  // namespace tcv
+
+extern "C" {
+
+tcv_status tcv_plan_build(tcv_plan** plan_out, const int32_t* d_iu, const int32_t* d_iv,
+                          const int32_t* d_coff, int64_t n, int support, int g_size,
+                          int64_t c_len, void* d_work, size_t work_bytes, void* stream)
+{
+    if (!plan_out) return TCV_ERR_ARG;
+    tcv_plan* p = new (std::nothrow) tcv_plan{};
+    if (!p) return TCV_ERR_OOM;
+    const tcv_status s = plan_init(p, d_iu, d_iv, d_coff, n, support, g_size, c_len, d_work, work_bytes,
+                                   static_cast<cudaStream_t>(stream));
     if (s != TCV_OK) {
         delete p;
         return s;

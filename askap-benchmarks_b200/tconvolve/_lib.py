@@ -91,6 +91,8 @@ SIGNATURES = {
     "tcv_plan_destroy": (None, [_P]),
     "tcv_grid_raw": (_I, [_P, _I64, _I, _P, _I, _F, _I64, _P, _P, _P, _P, _I, _P, _S, _P]),
     "tcv_degrid_raw": (_I, [_P, _I, _I, _P, _I, _F, _I64, _P, _P, _P, _P, _I64, _P, _S, _P]),
+    "tcv_static_scratch_bytes": (_S, []),
+    "tcv_grid_raw_static": (_I, [_P, _I64, _I, _P, _I, _F, _I64, _P, _P, _P, _P, _I, _P]),
     "tcv_grid_host_raw": (_I, [_P, _I64, _I, _P, _I64, _P, _P, _P, _P, _I, _I, _P]),
     "tcv_degrid_host_raw": (_I, [_P, _I, _I, _P, _I64, _P, _P, _P, _P, _I64, _I, _P]),
     "tcv_init_c_host": (_I, [_D, _D, _I, _I, _P, _I64, _I, _P, _P, _P, _P]),

@@ -167,6 +167,24 @@ tcv_status tcv_degrid_raw(const float *d_grid, int g_size, int support, const vo
                           const int32_t *d_iu, const int32_t *d_iv, float *d_data, int64_t n,
                           void *d_work, size_t work_bytes, void *stream);
 
+/* Gridding with no device allocation and no caller workspace, for callers that cannot
+ * allocate: a pipeline running latency-critical work on other streams cannot accept the
+ * device-wide synchronisation of cudaMalloc/cudaFree, and a host framework that manages all
+ * device memory in its own pool forbids allocations it does not make.  No counterpart in the
+ * reference (its gridders allocate per call, attic/tConvolveCuda/CudaGridder.cc:80-95).
+ * Same arguments and result as tcv_grid_raw (grid += gridding of d_data), with the plan's
+ * scratch in a fixed device array of tcv_static_scratch_bytes() (64 MiB) that every GPU loading
+ * the library holds until exit.  Problems whose plan needs more (tcv_plan_workspace_bytes > that
+ * size; about 277 k samples of a 129 x 129 footprint on a 4096 grid) return TCV_ERR_WORKSPACE
+ * before any device work.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the caller. */
+size_t tcv_static_scratch_bytes(void);
+tcv_status tcv_grid_raw_static(const float *d_data, int64_t n, int support, const void *d_c,
+                               int c_type, float c_scale, int64_t c_len, const int32_t *d_coff,
+                               const int32_t *d_iu, const int32_t *d_iv, float *d_grid,
+                               int g_size, void *stream);
+
 /* ------------------------------------------------------------------------------------------
  * Host-buffer one-call forms (the reference's libCudaGridder seam,
  * attic/tConvolveCuda/CudaGridder.cc:54-207 behind CudaGridder.h:32-50): allocate, upload,
