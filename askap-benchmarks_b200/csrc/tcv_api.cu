@@ -20,11 +20,11 @@ struct tcv_ctx {
     void* c_alt = nullptr;      // active form, reference layout (when not complex64)
     int c_alt_type = -1;
     float c_alt_scale = 1.f;
-    void* c_pad = nullptr;      // active form, prepared (padded) layout for the TMA kernels
-    int c_pad_type = -1;
+    void* c_pad = nullptr;      // active form, prepared layout (padded or paired) for the active path
+    int c_pad_type = -1;        // storage type | layout flag of c_pad
     float c_pad_scale = 1.f;
     int c_type = TCV_C_C64;     // active storage form
-    int path = TCV_PATH_TMA;
+    int path = TCV_PATH_DIRECT;
     int32_t *iu = nullptr, *iv = nullptr, *coff = nullptr;
     void* work = nullptr;
     size_t work_bytes = 0;
@@ -73,15 +73,16 @@ cudaError_t dalloc(T** p, size_t count)
 }
 
 // table, type code (with the layout flag) and scale the kernels are given
+int layout_flag(int path) { return path == TCV_PATH_TMA ? TCV_C_PADDED : (path == TCV_PATH_PAIRED ? TCV_C_PAIRED : 0); }
 const void* active_table(const tcv_ctx* c)
 {
-    if (c->path == TCV_PATH_TMA) return c->c_pad;
+    if (c->path != TCV_PATH_DIRECT) return c->c_pad;
     return c->c_type == TCV_C_C64 ? static_cast<const void*>(c->c64) : c->c_alt;
 }
-int active_code(const tcv_ctx* c) { return c->path == TCV_PATH_TMA ? (c->c_type | TCV_C_PADDED) : c->c_type; }
+int active_code(const tcv_ctx* c) { return c->c_type | layout_flag(c->path); }
 float active_scale(const tcv_ctx* c)
 {
-    if (c->path == TCV_PATH_TMA) return c->c_pad_scale;
+    if (c->path != TCV_PATH_DIRECT) return c->c_pad_scale;
     return c->c_type == TCV_C_C64 ? 1.f : c->c_alt_scale;
 }
 
@@ -89,23 +90,24 @@ float active_scale(const tcv_ctx* c)
 tcv_status ensure_tables(tcv_ctx* c)
 {
     const int t = c->c_type;
-    if (c->path == TCV_PATH_TMA) {
-        if (c->c_pad_type == t) return TCV_OK;
+    if (c->path != TCV_PATH_DIRECT) {
+        const int want = t | layout_flag(c->path);
+        if (c->c_pad_type == want) return TCV_OK;
         if (c->c_pad) {
             CTX_CUDA(c, cudaStreamSynchronize(c->stream));
             cudaFree(c->c_pad);
             c->c_pad = nullptr;
             c->c_pad_type = -1;
         }
-        const size_t bytes = tcv_table_bytes(c->c_len, c->support, t | TCV_C_PADDED);
+        const size_t bytes = tcv_table_bytes(c->c_len, c->support, want);
         if (!bytes) return fail(c, TCV_ERR_UNSUPPORTED, "table shape has no prepared layout");
         CTX_CUDA(c, cudaMalloc(&c->c_pad, bytes));
         int64_t nz = 0;
-        CTX_TRY(c, tcv_prepare_table(reinterpret_cast<const float*>(c->c64), c->c_len, c->support, t, c->c_pad,
+        CTX_TRY(c, tcv_prepare_table(reinterpret_cast<const float*>(c->c64), c->c_len, c->support, want, c->c_pad,
                                      &c->c_pad_scale, &nz, c->stream));
         const bool real_form = t == TCV_C_R32 || t == TCV_C_RBF16 || t == TCV_C_RF16;
         if (real_form && nz > 0) return fail(c, TCV_ERR_ARG, "real table form requested for a table with imaginary parts");
-        c->c_pad_type = t;
+        c->c_pad_type = want;
         return TCV_OK;
     }
     if (t == TCV_C_C64 || c->c_alt_type == t) return TCV_OK;
@@ -301,7 +303,7 @@ tcv_status tcv_set_ctype(tcv_ctx* c, int c_type)
 
 tcv_status tcv_set_path(tcv_ctx* c, int path)
 {
-    if (!c || (path != TCV_PATH_TMA && path != TCV_PATH_DIRECT)) return TCV_ERR_ARG;
+    if (!c || (path != TCV_PATH_TMA && path != TCV_PATH_DIRECT && path != TCV_PATH_PAIRED)) return TCV_ERR_ARG;
     const int prev = c->path;
     c->path = path;
     if (!c->initialized) return TCV_OK;

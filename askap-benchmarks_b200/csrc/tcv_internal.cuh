@@ -146,6 +146,16 @@ tcv_status launch_grid_pipe(const tcv_plan* p, const float2* data, const void* t
 tcv_status launch_degrid_pipe(const tcv_plan* p, const float2* grid, const void* table, int c_type,
                               float c_scale, float2* out, cudaStream_t st);
 size_t padded_table_bytes(int64_t c_len, int s, int c_type);
+
+// two-columns-per-lane tile kernels on paired tables, tcv_pair.cu
+tcv_status launch_grid_pair(const tcv_plan* p, const float2* data, const void* table, int c_type,
+                            float c_scale, float2* grid, cudaStream_t st);
+tcv_status launch_degrid_pair(const tcv_plan* p, const float2* grid, const void* table, int c_type,
+                              float c_scale, float2* out, cudaStream_t st);
+int paired_pitch(int s);
+int64_t paired_copy_stride(int64_t c_len, int s);
+size_t paired_table_bytes(int64_t c_len, int s, int c_type);
+tcv_status pair_table(const void* in, int64_t c_len, int s, int c_type, void* out, cudaStream_t st);
 tcv_status pad_table(const void* in, int64_t c_len, int s, int c_type, void* out, cudaStream_t st);
 
 inline tcv_status cuda_status(cudaError_t e)

@@ -609,8 +609,9 @@ extern "C" {
 size_t tcv_table_bytes(int64_t c_len, int support, int c_type)
 {
     const size_t es = tcv_ctype_bytes(c_type);
-    if (!es || c_len < 0 || support < 0) return 0;
+    if (!es || c_len < 0 || support < 0 || (c_type & TCV_C_PADDED && c_type & TCV_C_PAIRED)) return 0;
     if (c_type & TCV_C_PADDED) return padded_table_bytes(c_len, 2 * support + 1, c_type & 0xff);
+    if (c_type & TCV_C_PAIRED) return paired_table_bytes(c_len, 2 * support + 1, c_type & 0xff);
     return size_t(c_len) * es;
 }
 
@@ -618,20 +619,25 @@ tcv_status tcv_prepare_table(const float* d_c64, int64_t c_len, int support, int
                              float* c_scale_out, int64_t* imag_nonzero_out, void* stream)
 {
     const int base = c_type & 0xff;
+    const bool paired = (c_type & TCV_C_PAIRED) != 0;
     if (!d_c64 || !d_out || c_len <= 0 || support < 0 || tcv_ctype_bytes(base) == 0) return TCV_ERR_ARG;
+    if (paired == ((c_type & TCV_C_PADDED) != 0) && (c_type & (TCV_C_PADDED | TCV_C_PAIRED))) return TCV_ERR_ARG;
     const int s = 2 * support + 1;
-    if (padded_table_bytes(c_len, s, base) == 0) return TCV_ERR_ARG;
+    if ((paired ? paired_table_bytes(c_len, s, base) : padded_table_bytes(c_len, s, base)) == 0) return TCV_ERR_ARG;
     if ((reinterpret_cast<uintptr_t>(d_out) & 15)) return TCV_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    auto layout = [&](const void* in) {
+        return paired ? pair_table(in, c_len, s, base, d_out, st) : pad_table(in, c_len, s, base, d_out, st);
+    };
     if (base == TCV_C_C64) {
         if (c_scale_out) *c_scale_out = 1.0f;
         if (imag_nonzero_out) *imag_nonzero_out = 0;
-        return pad_table(d_c64, c_len, s, base, d_out, st);
+        return layout(d_c64);
     }
     void* tmp = nullptr;
     TCV_CUDA(cudaMalloc(&tmp, size_t(c_len) * tcv_ctype_bytes(base) + 16));
     tcv_status r = tcv_convert_c(d_c64, c_len, base, tmp, c_scale_out, imag_nonzero_out, stream);
-    if (r == TCV_OK) r = pad_table(tmp, c_len, s, base, d_out, st);
+    if (r == TCV_OK) r = layout(tmp);
     const cudaError_t e = cudaStreamSynchronize(st);
     cudaFree(tmp);
     if (r != TCV_OK) return r;

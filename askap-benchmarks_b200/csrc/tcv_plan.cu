@@ -9,10 +9,10 @@
 //               lies in it (each sample exactly once).
 // Kernel indices kid = cOffset / sSize^2 (w-plane major, then the oversampling offsets) are
 // grouped into runs of whole w-planes whose slice of the table fits in L2 with room to spare.
-// The sort key is (group, tile, kid): work cells are (group, tile), ordered group-major, so all
-// SMs work through the table one group at a time and the slice in use stays resident in L2.
-// The sort is stable, so equal keys keep index order.  The non-empty cells are compacted into
-// work lists (with per-group ranges) that persistent kernels walk.
+// The sort key is the work cell (group, tile), ordered group-major, so all SMs work through the
+// table one group at a time and the slice in use stays resident in L2; within a cell the stable
+// sort keeps samples in index order (the reference's order).  The non-empty cells are compacted
+// into work lists (with per-group ranges) that persistent kernels walk.
 // Samples whose footprint or table range falls outside the grid or the table are counted and
 // left out (sentinel key, sorted past the end).
 #include "tcv_internal.cuh"
@@ -67,7 +67,6 @@ __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* 
         avals[d] = uint32_t(d);
         return;
     }
-    const K kid = K(co / (s * s));
     const uint32_t grp = uint32_t(co / (s * s) / g.kid_group);
     const uint32_t cell0 = grp * uint32_t(g.ntx * g.nty);
     const int tx0 = int(fx / g.tw), tx1 = int((fx + s - 1) / g.tw);
@@ -76,7 +75,7 @@ __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* 
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
             const uint32_t cell = cell0 + uint32_t(ty) * g.ntx + tx;
-            kp[t] = (K(cell) << g.kid_bits) | kid;
+            kp[t] = K(cell);
             vp[t] = uint32_t(d);
             atomicAdd(&tile_count[cell], 1u);
             ++t;
@@ -86,7 +85,7 @@ __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* 
         vp[t] = uint32_t(d);
     }
     const uint32_t at = grp * uint32_t(g.natx * g.naty) + uint32_t(fy / g.ta) * g.natx + uint32_t(fx / g.ta);
-    akeys[d] = (K(at) << g.kid_bits) | kid;
+    akeys[d] = K(at);
     avals[d] = uint32_t(d);
     atomicAdd(&atile_count[at], 1u);
 }
@@ -214,7 +213,7 @@ PlanGeom make_geom(int64_t n, int support, int g_size, int64_t c_len)
     g.nty = (g_size + g.th - 1) / g.th;
     g.max_tiles = ((g.s + g.tw - 2) / g.tw + 1) * ((g.s + g.th - 2) / g.th + 1);
     g.tile_bits = bits_for(uint64_t(g.n_groups) * g.ntx * g.nty - 1);
-    g.key_bits = g.tile_bits + g.kid_bits + 1;
+    g.key_bits = g.tile_bits + 1;  // cell, plus the sentinel bit
 
     constexpr size_t kSmemBudget = 220 * 1024;  // of 227 KB per CTA; the rest holds partial sums
     const int cand[] = {128, 96, 64, 48, 32, 16, 8};
@@ -234,7 +233,7 @@ PlanGeom make_geom(int64_t n, int support, int g_size, int64_t c_len)
     g.natx = (g_size + g.ta - 1) / g.ta;
     g.naty = (g_size + g.ta - 1) / g.ta;
     g.atile_bits = bits_for(uint64_t(g.n_groups) * g.natx * g.naty - 1);
-    g.akey_bits = g.atile_bits + g.kid_bits + 1;
+    g.akey_bits = g.atile_bits + 1;
     g.key64 = g.key_bits > 32 || g.akey_bits > 32;
     g.degrid_parts = 4;
     return g;
@@ -391,6 +390,9 @@ tcv_status tcv_plan_grid(const tcv_plan* plan, const float* d_data, const void* 
     if (c_type & TCV_C_PADDED)
         return launch_grid_pipe(plan, reinterpret_cast<const float2*>(d_data), d_c, c_type & 0xff, c_scale,
                                 reinterpret_cast<float2*>(d_grid), static_cast<cudaStream_t>(stream));
+    if (c_type & TCV_C_PAIRED)
+        return launch_grid_pair(plan, reinterpret_cast<const float2*>(d_data), d_c, c_type & 0xff, c_scale,
+                                reinterpret_cast<float2*>(d_grid), static_cast<cudaStream_t>(stream));
     return launch_grid(plan, reinterpret_cast<const float2*>(d_data), d_c, c_type, c_scale,
                        reinterpret_cast<float2*>(d_grid), static_cast<cudaStream_t>(stream));
 }
@@ -403,6 +405,11 @@ tcv_status tcv_plan_degrid(const tcv_plan* plan, const float* d_grid, const void
     if (c_type & TCV_C_PADDED) {
         if (plan->g.n == 0) return TCV_OK;
         return launch_degrid_pipe(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type & 0xff, c_scale,
+                                  reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
+    }
+    if (c_type & TCV_C_PAIRED) {
+        if (plan->g.n == 0) return TCV_OK;
+        return launch_degrid_pair(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type & 0xff, c_scale,
                                   reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
     }
     if (plan->degrid_variant == TCV_DEGRID_TILES) {

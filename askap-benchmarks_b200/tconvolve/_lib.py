@@ -25,7 +25,8 @@ C64, R32, CBF16, RBF16, CF16, RF16 = range(6)
 CTYPE_NAMES = {C64: "c64", R32: "r32", CBF16: "cbf16", RBF16: "rbf16", CF16: "cf16", RF16: "rf16"}
 CTYPE_BY_NAME = {v: k for k, v in CTYPE_NAMES.items()}
 PADDED = 0x100          # TCV_C_PADDED: prepared (TMA) table layout
-PATH_TMA, PATH_DIRECT = 0, 1
+PAIRED = 0x200          # TCV_C_PAIRED: paired table layout (two columns per lane)
+PATH_TMA, PATH_DIRECT, PATH_PAIRED = 0, 1, 2
 DEGRID_TILES, DEGRID_ANCHOR = 0, 1
 
 

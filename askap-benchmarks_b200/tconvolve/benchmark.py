@@ -96,9 +96,10 @@ class Benchmark:
         check(lib().tcv_set_ctype(self._ctx, int(c_type)), "tcv_set_ctype", self._ctx)
 
     def set_path(self, path: int | str):
-        """Kernel family: "tma" (prepared table, default) or "direct" (reference-layout table)."""
+        """Kernel family: "direct" (default: tile kernels on the reference-layout table), "paired"
+        (two columns per lane on the paired table) or "tma" (TMA pipeline on the padded table)."""
         if isinstance(path, str):
-            path = {"tma": _lib.PATH_TMA, "direct": _lib.PATH_DIRECT}[path]
+            path = {"tma": _lib.PATH_TMA, "direct": _lib.PATH_DIRECT, "paired": _lib.PATH_PAIRED}[path]
         check(lib().tcv_set_path(self._ctx, int(path)), "tcv_set_path", self._ctx)
 
     def set_degrid_variant(self, variant: int | str):

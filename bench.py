@@ -48,8 +48,11 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="c2", choices=sorted(PROBLEMS))
-    p.add_argument("--form", default="c64", help="table storage form (c64 = plain FP32)")
-    p.add_argument("--path", default="direct", choices=["tma", "direct"], help="kernel family")
+    p.add_argument("--form", default="r32",
+                   help="table storage form of the headline: r32 (default; the attic table is real, "
+                        "so this is the plain FP32 result bit for bit) or c64 (the plain complex64 "
+                        "table), or a reduced form for study; c64 is always measured beside it")
+    p.add_argument("--path", default="direct", choices=["direct", "paired", "tma"], help="kernel family")
     p.add_argument("--degrid", default="tiles", choices=["tiles", "anchor"],
                    help="degridding kernel on the direct path")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -232,55 +235,66 @@ def b200_arm(args):
 
     dvariant = {"tiles": tconvolve._lib.DEGRID_TILES, "anchor": tconvolve._lib.DEGRID_ANCHOR}[args.degrid]
 
-    def step(evs=None):
+    def step(tab, evs=None):
+        """One step with table `tab` (a tcv_device_buffers): plan, gridding pass, degridding pass."""
         sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)  # the capture stream too
         plan = ctypes.c_void_p()
         if evs:
             evs[0].record(stream)
-        check(L.tcv_plan_build(ctypes.byref(plan), P(bufs.iu), P(bufs.iv), P(bufs.coff), n, support,
+        check(L.tcv_plan_build(ctypes.byref(plan), P(tab.iu), P(tab.iv), P(tab.coff), n, support,
                                prob.g_size, c_len, P(work.data_ptr()), wbytes, sp), "plan")
         L.tcv_plan_set_degrid_variant(plan, dvariant)
         if evs:
             evs[1].record(stream)
-        check(L.tcv_plan_grid(plan, P(bufs.data), P(bufs.c_active), bufs.c_type, bufs.c_scale,
-                              P(bufs.grid), sp), "grid")
+        check(L.tcv_plan_grid(plan, P(tab.data), P(tab.c_active), tab.c_type, tab.c_scale,
+                              P(tab.grid), sp), "grid")
         if evs:
             evs[2].record(stream)
-        check(L.tcv_plan_degrid(plan, P(bufs.grid), P(bufs.c_active), bufs.c_type, bufs.c_scale,
-                                P(bufs.outdata), sp), "degrid")
+        check(L.tcv_plan_degrid(plan, P(tab.grid), P(tab.c_active), tab.c_type, tab.c_scale,
+                                P(tab.outdata), sp), "degrid")
         if evs:
             evs[3].record(stream)
         L.tcv_plan_destroy(plan)
 
-    # kernels launched by one step, counted from a CUDA-graph capture of it
-    step()
-    torch.cuda.synchronize()
-    launches_per_step = count_step_kernels(torch, step)
+    def timed(tab, steps):
+        for _ in range(args.warmup):
+            step(tab)
+            flush.zero_()
+        torch.cuda.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(steps):
+            step(tab, evs[k])
+            flush.zero_()  # L2 flush between timed steps (outside the events)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        wall = time.perf_counter() - t0
+        return ([e[0].elapsed_time(e[1]) for e in evs], [e[1].elapsed_time(e[2]) for e in evs],
+                [e[2].elapsed_time(e[3]) for e in evs], [e[0].elapsed_time(e[3]) for e in evs], wall)
 
-    for _ in range(args.warmup):
-        step()
-        flush.zero_()
+    # kernels launched by one step, counted from a CUDA-graph capture of it
+    step(bufs)
     torch.cuda.synchronize()
+    launches_per_step = count_step_kernels(torch, lambda: step(bufs))
 
     gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     clocks = ClockSampler(gpu_uuid)
     clocks.start()
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t_wall0 = time.perf_counter()
-    for k in range(args.steps):
-        step(evs[k])
-        flush.zero_()  # L2 flush between timed steps (outside the events)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t_wall = time.perf_counter() - t_wall0
-    plan_ms = [e[0].elapsed_time(e[1]) for e in evs]
-    grid_ms = [e[1].elapsed_time(e[2]) for e in evs]
-    degrid_ms = [e[2].elapsed_time(e[3]) for e in evs]
-    step_ms = [e[0].elapsed_time(e[3]) for e in evs]
+    plan_ms, grid_ms, degrid_ms, step_ms, t_wall = timed(bufs, args.steps)
+    plain = None
+    if args.form != "c64":
+        # the plain form (complex64 table, the reference's storage) measured beside the chosen one
+        b.set_ctype("c64")
+        p_plan, p_grid, p_degrid, p_step, _ = timed(b.device_buffers(), args.steps)
+        b.set_ctype(form)
+        bufs = b.device_buffers()
+        plain = {"form": "c64", "value": world * 2 * updates / (statistics.mean(p_step) * 1e-3),
+                 "grid_ms": statistics.mean(p_grid), "degrid_ms": statistics.mean(p_degrid),
+                 "plan_ms": statistics.mean(p_plan)}
 
     # e2e: the same step through the C ABI with host buffers: H2D of the batch's samples from
     # pinned memory, plan, grid, degrid, D2H of the degridded visibilities, every step
@@ -302,6 +316,7 @@ def b200_arm(args):
         d_iv.copy_(h_iv, non_blocking=True)
         d_co.copy_(h_co, non_blocking=True)
         plan = ctypes.c_void_p()
+        sp = ctypes.c_void_p(stream.cuda_stream)
         check(L.tcv_plan_build(ctypes.byref(plan), P(d_iu.data_ptr()), P(d_iv.data_ptr()),
                                P(d_co.data_ptr()), n, support, prob.g_size, c_len,
                                P(work.data_ptr()), wbytes, sp), "plan")
@@ -347,12 +362,13 @@ def b200_arm(args):
     peak, peak_kind = measured_hbm_peak()
     achieved = ALG_BYTES[dom] * updates / (dom_ms * 1e-3) / 1e9
     traffic = ncu_traffic(dom)
-    tma = bool(bufs.c_type & tconvolve._lib.PADDED)
-    kname = {("grid", True): "pipe_kernel<gridding> (TMA pipeline)",
-             ("degrid", True): "pipe_kernel<degridding> + slot_reduce_kernel (TMA pipeline)",
-             ("grid", False): "grid_tile_kernel",
-             ("degrid", False): ("degrid_tile_kernel + slot_reduce_kernel" if args.degrid == "tiles"
-                                 else "degrid_staged_kernel")}[(dom, tma)]
+    kname = {("grid", "tma"): "pipe_kernel<gridding> (TMA pipeline)",
+             ("degrid", "tma"): "pipe_kernel<degridding> + slot_reduce_kernel (TMA pipeline)",
+             ("grid", "paired"): "pair_tile_kernel<gridding>",
+             ("degrid", "paired"): "pair_tile_kernel<degridding> + slot_reduce_kernel",
+             ("grid", "direct"): "grid_tile_kernel",
+             ("degrid", "direct"): ("degrid_tile_kernel + slot_reduce_kernel" if args.degrid == "tiles"
+                                    else "degrid_staged_kernel")}[(dom, args.path)]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -368,7 +384,10 @@ def b200_arm(args):
             "config": {"workload": f"{args.workload}: {prob.n_samples} samples x {prob.n_chan} chan, "
                                    f"gSize {prob.g_size}, wSize {prob.w_size}, support {support} "
                                    f"({2 * support + 1}^2 footprint), cellSize {prob.cell_size}",
-                       "form": args.form, "path": args.path, "degrid": args.degrid,
+                       "form": (f"{args.form} (chosen form: real parts of the reference's table, whose "
+                                "imaginary parts are zero; bit-identical to the plain c64 result)"
+                                if args.form == "r32" else args.form),
+                       "path": args.path, "degrid": args.degrid,
                        "parallelism": f"replicas x{world}",
                        "l2": f"{L2_FLUSH_BYTES >> 20} MiB buffer written between timed steps",
                        "step": "binning plan + gridding pass + degridding pass"},
@@ -381,6 +400,7 @@ def b200_arm(args):
                         "degrid_alg_GBps": ALG_BYTES["degrid"] * updates / (d_ms * 1e-3) / 1e9,
                         "grid_updates_per_s": updates / (g_ms * 1e-3),
                         "degrid_updates_per_s": updates / (d_ms * 1e-3)},
+            "plain_form": plain,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * (8 + 4 * 3),
                     "d2h_bytes_per_step": n * 8, "ms_per_step": e2e_mean},
             "gpu_launches": launches_per_step * args.steps if launches_per_step else None,

@@ -59,7 +59,11 @@ typedef enum tcv_ctype {
     TCV_C_RF16 = 5, /* real float16 x 2^e (2 B/entry) */
     /* Flag: the table is in the prepared (padded) layout made by tcv_prepare_table, rows of
      * sSize entries padded to a 16-byte pitch; the kernels then stream it with TMA. */
-    TCV_C_PADDED = 0x100
+    TCV_C_PADDED = 0x100,
+    /* Flag: the table is in the paired layout made by tcv_prepare_table: every kernel row stored
+     * twice (as is, and shifted right by one column) with an even pitch, so that the tile
+     * kernels read two columns per lane with one aligned load. */
+    TCV_C_PAIRED = 0x200
 } tcv_ctype;
 
 const char *tcv_status_string(tcv_status s);
@@ -93,14 +97,16 @@ tcv_status tcv_init_c_raw(double freq0, double cell_size, int baseline, int w_si
 tcv_status tcv_convert_c(const float *d_c64, int64_t c_len, int c_type, void *d_out,
                          float *c_scale_out, int64_t *imag_nonzero_out, void *stream);
 
-/* Bytes of a table of c_len entries in storage type c_type; with TCV_C_PADDED set, in the
- * prepared layout for footprints of sSize = 2*support+1 (0 if c_len is not a multiple of sSize^2). */
+/* Bytes of a table of c_len entries in storage type c_type; with TCV_C_PADDED or TCV_C_PAIRED
+ * set, in that prepared layout for footprints of sSize = 2*support+1 (0 if c_len is not a
+ * multiple of sSize^2). */
 size_t tcv_table_bytes(int64_t c_len, int support, int c_type);
-/* Prepare a table for the TMA pipeline kernels: convert the complex64 reference-layout table to
- * storage type c_type (as tcv_convert_c) and write it in the padded layout to d_out
- * (tcv_table_bytes(c_len, support, c_type | TCV_C_PADDED) bytes).  Set-up path: allocates a
- * temporary for the reduced forms and synchronises the stream.  Pass the result to the kernels
- * with c_type | TCV_C_PADDED. */
+/* Prepare a table for the faster kernels: convert the complex64 reference-layout table to storage
+ * type c_type & 0xff (as tcv_convert_c) and write it to d_out in the layout the flag selects,
+ * TCV_C_PADDED (TMA pipeline kernels) or TCV_C_PAIRED (two-columns-per-lane tile kernels);
+ * tcv_table_bytes(c_len, support, c_type) bytes.  Set-up path: allocates a temporary for the
+ * reduced forms and synchronises the stream.  Pass the result to the kernels with the same
+ * c_type (flag included). */
 tcv_status tcv_prepare_table(const float *d_c64, int64_t c_len, int support, int c_type,
                              void *d_out, float *c_scale_out, int64_t *imag_nonzero_out,
                              void *stream);
@@ -250,9 +256,10 @@ int64_t tcv_n_data(const tcv_ctx *ctx);        /* nSamples * nChan */
 double tcv_updates_per_pass(const tcv_ctx *ctx); /* nSamples * nChan * sSize^2 */
 /* Switch the table storage type used by run_grid / run_degrid (converts once, keeps the C64 table). */
 tcv_status tcv_set_ctype(tcv_ctx *ctx, int c_type);
-/* Kernel family used by run_grid / run_degrid: the TMA pipeline kernels on the prepared table
- * (default) or the kernels that read the reference-layout table directly. */
-enum { TCV_PATH_TMA = 0, TCV_PATH_DIRECT = 1 };
+/* Kernel family used by run_grid / run_degrid: the TMA pipeline kernels on the padded table,
+ * the tile kernels that read the reference-layout table directly (default), or the
+ * two-columns-per-lane tile kernels on the paired table. */
+enum { TCV_PATH_TMA = 0, TCV_PATH_DIRECT = 1, TCV_PATH_PAIRED = 2 };
 tcv_status tcv_set_path(tcv_ctx *ctx, int path);
 int tcv_get_path(const tcv_ctx *ctx);
 

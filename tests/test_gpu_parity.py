@@ -18,7 +18,7 @@ from tconvolve.workload import PROBLEMS, normal_vis
 pytestmark = pytest.mark.gpu
 
 
-KERNELS = ["tma", "direct-tiles", "direct-anchor"]
+KERNELS = ["paired", "tma", "direct-tiles", "direct-anchor"]
 
 
 def _use(b, kernels):
@@ -328,27 +328,30 @@ def test_direct_degrid_path(tcv, orc, cuda_ok, g_size, cell, w_size):
     assert orc.rel_l2(b.outdata(), r["outdata"]) <= REL_L2_FP32
 
 
-@pytest.mark.parametrize("form", ["c64", "r32", "rbf16"])
-def test_raw_prepared_table(tcv, orc, cuda_ok, form):
-    """The TMA kernels through the raw entry points: a table prepared by tcv_prepare_table, passed
-    with the TCV_C_PADDED flag, gives the same grid and samples as the reference-layout kernels."""
+@pytest.mark.parametrize("layout", ["padded", "paired"])
+@pytest.mark.parametrize("form", ["c64", "r32", "rbf16", "cf16"])
+def test_raw_prepared_table(tcv, orc, cuda_ok, form, layout):
+    """Prepared tables through the raw entry points: a table prepared by tcv_prepare_table, passed
+    with its layout flag (TMA pipeline or paired tile kernels), gives the same grid and samples
+    as the reference-layout kernels."""
     import ctypes
 
     import torch
 
     from tconvolve import raw
-    from tconvolve._lib import PADDED, check, lib
+    from tconvolve._lib import PADDED, PAIRED, check, lib
 
+    FLAG = PADDED if layout == "padded" else PAIRED
     prob = PROBLEMS["c1"]
     c, support, iu, iv, co = _setup(orc, prob)
     vis = normal_vis(iu.size, 31)
     dvis, dc, diu, div, dco = _dev(vis, c, iu, iv, co)
     t = tcv.CTYPE_BY_NAME[form]
-    nbytes = lib().tcv_table_bytes(c.size, support, t | PADDED)
+    nbytes = lib().tcv_table_bytes(c.size, support, t | FLAG)
     assert nbytes > 0
     padded = torch.zeros(nbytes, dtype=torch.uint8, device="cuda")
     scale, nz = ctypes.c_float(), ctypes.c_int64()
-    check(lib().tcv_prepare_table(ctypes.c_void_p(dc.data_ptr()), c.size, support, t,
+    check(lib().tcv_prepare_table(ctypes.c_void_p(dc.data_ptr()), c.size, support, t | FLAG,
                                   ctypes.c_void_p(padded.data_ptr()), ctypes.byref(scale),
                                   ctypes.byref(nz), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
           "prepare")
@@ -360,11 +363,11 @@ def test_raw_prepared_table(tcv, orc, cuda_ok, form):
     plan = raw.Plan(diu, div, dco, support, prob.g_size, c.size)
     g_tma = torch.zeros(prob.g_size ** 2, dtype=torch.complex64, device="cuda")
     g_dir = torch.zeros_like(g_tma)
-    plan.grid(dvis, padded, t | PADDED, g_tma, c_scale=scale.value)
+    plan.grid(dvis, padded, t | FLAG, g_tma, c_scale=scale.value)
     plan.grid(dvis, flat, t, g_dir, c_scale=fscale)
     o_tma = torch.empty_like(dvis)
     o_dir = torch.empty_like(dvis)
-    plan.degrid(g_dir, padded, t | PADDED, o_tma, c_scale=scale.value)
+    plan.degrid(g_dir, padded, t | FLAG, o_tma, c_scale=scale.value)
     plan.degrid(g_dir, flat, t, o_dir, c_scale=fscale)
     torch.cuda.synchronize()
     assert plan.status() == 0
