@@ -110,6 +110,7 @@ tcv_status ensure_tables(tcv_ctx* c)
         c->c_pad_type = want;
         return TCV_OK;
     }
+    tcv_jit_prepare(t, c->support);  // the direct path's tile kernels, specialised on sSize
     if (t == TCV_C_C64 || c->c_alt_type == t) return TCV_OK;
     if (c->c_alt) {
         CTX_CUDA(c, cudaStreamSynchronize(c->stream));

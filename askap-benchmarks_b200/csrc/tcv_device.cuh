@@ -1,0 +1,265 @@
+// tcv_device.cuh -- device code of the output-stationary tile kernels (gridding and its adjoint).
+//
+// Self-contained device code: compiled into libtconvolve for every table form with the footprint
+// width sSize as a runtime value (kS = 0), and handed to NVRTC at plan time to build copies with
+// sSize a compile-time constant (kS = sSize), where row offsets become load immediates and loop
+// bounds constants.  Nothing here includes a host header, so both compilers accept it.
+//
+// Output-stationary tiles.  One CTA owns a 64 x 64 tile of the grid; each of its 8 warps owns a
+// 32-column x 16-row block with one accumulator per point held in registers (lane = column).
+// The CTA walks the tile's sample list (from the plan), staging sample records in shared memory;
+// for each sample a warp whose block meets the footprint reads the table rows it needs (32
+// consecutive entries per row: one coalesced load per row) and accumulates data * C into its
+// registers.  When the list is done the tile is added into the grid with coalesced
+// read-modify-writes.  Every grid point has exactly one owner thread: no atomics, and the result
+// is the same on every run.  Gridding follows attic/tConvolveMPI/Benchmark.cc:125-155.
+//
+// Degridding (Benchmark.cc:158-195) is the adjoint on the same plan: a lane holds its 16 grid
+// points in registers; for each sample a warp whose block meets the footprint forms the partial
+// dot product of its block with the table, reduces it with shuffles, and the CTA adds its 8 warp
+// partials in warp order into the sample's slot for this tile; a final pass adds each sample's
+// tile slots in tile order.
+#pragma once
+
+namespace tcv {
+
+using u32 = unsigned int;
+
+constexpr int kTileW = 64;
+constexpr int kTileH = 64;
+constexpr int kRowsPerWarp = 16;
+constexpr int kTileWarps = (kTileW / 32) * (kTileH / kRowsPerWarp);
+constexpr int kTileThreads = kTileWarps * 32;
+constexpr int kTileChunk = kTileThreads;  // samples staged per round
+
+struct GridArgs {
+    int support, s, g_size, ntx, ntiles, group;
+    float c_scale;
+};
+
+// ------------------------------------------------------------------------------------------
+// Table loaders.  Every storage form returns the entry as (re, im) floats; the real forms
+// return im = 0 and tell the multiply-accumulate to skip the imaginary products, which gives
+// exactly the same result as the complex form on a table whose imaginary parts are zero
+// (fma(-d.im, 0, acc) == acc).
+// ------------------------------------------------------------------------------------------
+struct TabC64 {
+    static constexpr bool kReal = false;
+    using elem = float2;
+    __device__ __forceinline__ static float2 load(const elem* p) { return __ldg(p); }
+};
+struct TabR32 {
+    static constexpr bool kReal = true;
+    using elem = float;
+    __device__ __forceinline__ static float2 load(const elem* p) { return make_float2(__ldg(p), 0.f); }
+};
+struct TabCBF16 {
+    static constexpr bool kReal = false;
+    using elem = u32;  // (re, im) bfloat16 pair, re in the low half
+    __device__ __forceinline__ static float2 load(const elem* p)
+    {
+        const u32 u = __ldg(p);
+        return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
+    }
+};
+struct TabRBF16 {
+    static constexpr bool kReal = true;
+    using elem = unsigned short;
+    __device__ __forceinline__ static float2 load(const elem* p)
+    {
+        const u32 u = __ldg(p);
+        return make_float2(__uint_as_float(u << 16), 0.f);
+    }
+};
+
+// acc += a * b (complex), FP32 fused multiply-adds.  With a real table (b.y == 0 by construction)
+// only the two real-by-complex products are issued.
+template <bool kReal>
+__device__ __forceinline__ void cmac(float2& acc, const float2 a, const float2 b)
+{
+    acc.x = fmaf(a.x, b.x, acc.x);
+    acc.y = fmaf(a.y, b.x, acc.y);
+    if (!kReal) {
+        acc.x = fmaf(-a.y, b.y, acc.x);
+        acc.y = fmaf(a.x, b.y, acc.y);
+    }
+}
+
+template <class Tab, int kS>
+__global__ void __launch_bounds__(kTileThreads, 3)
+grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
+                 const int* __restrict__ iu, const int* __restrict__ iv,
+                 const int* __restrict__ coff, const u32* __restrict__ order,
+                 const u32* __restrict__ tile_start, const u32* __restrict__ tile_count,
+                 const u32* __restrict__ items, const u32* __restrict__ group_start,
+                 float2* __restrict__ grid, GridArgs a)
+{
+    __shared__ float4 sm_rec[kTileChunk];  // (data.re, data.im, first column, first row)
+    __shared__ int sm_coff[kTileChunk];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
+    // persistent: this CTA takes every gridDim.x-th non-empty cell of the group
+    const u32 i1 = group_start[a.group + 1];
+    for (u32 it = group_start[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
+        const u32 cell = items[it];
+        const u32 cnt = tile_count[cell];
+        const u32 start = tile_start[cell];
+        const int tile = int(cell % u32(a.ntiles));
+        const int tx = tile % a.ntx, ty = tile / a.ntx;
+        const int bx0 = tx * kTileW + (warp % (kTileW / 32)) * 32;  // first column of this warp
+        const int gx = bx0 + lane;
+        const int gy0 = ty * kTileH + (warp / (kTileW / 32)) * kRowsPerWarp;
+
+        float2 acc[kRowsPerWarp];
+#pragma unroll
+        for (int r = 0; r < kRowsPerWarp; ++r) acc[r] = make_float2(0.f, 0.f);
+
+        for (u32 base = 0; base < cnt; base += kTileChunk) {
+            const int m = int(cnt - base < u32(kTileChunk) ? cnt - base : u32(kTileChunk));
+            __syncthreads();
+            if (threadIdx.x < m) {
+                const u32 k = order[start + base + threadIdx.x];
+                const float2 d = data[k];
+                sm_rec[threadIdx.x] = make_float4(d.x * a.c_scale, d.y * a.c_scale,
+                                                  __int_as_float(iu[k] - a.support), __int_as_float(iv[k]));
+                sm_coff[threadIdx.x] = coff[k];
+            }
+            __syncthreads();
+            for (int j = 0; j < m; ++j) {
+                const float4 q = sm_rec[j];
+                const int fx = __float_as_int(q.z), fy = __float_as_int(q.w);
+                const int dy0 = gy0 - fy;  // footprint row of this warp's first row
+                if (dy0 >= s || dy0 + kRowsPerWarp <= 0) continue;   // warp-uniform
+                if (fx > bx0 + 31 || fx + s <= bx0) continue;          // warp-uniform
+                const int dx = gx - fx;
+                const bool colok = unsigned(dx) < unsigned(s);
+                const float2 dv = make_float2(q.x, q.y);
+                // 32-bit element index off the kernel-wide table base (tables hold < 2^31 entries)
+                const int ci = sm_coff[j] + dy0 * s + dx;
+                if (dy0 >= 0 && dy0 + kRowsPerWarp <= s) {
+                    // every row of the block is inside the footprint: only the column test remains
+                    if (colok) {
+#pragma unroll
+                        for (int r = 0; r < kRowsPerWarp; ++r) cmac<Tab::kReal>(acc[r], dv, Tab::load(ctab + (ci + r * s)));
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < kRowsPerWarp; ++r) {
+                        if (colok && unsigned(dy0 + r) < unsigned(s)) {
+                            const float2 c = Tab::load(ctab + (ci + r * s));
+                            cmac<Tab::kReal>(acc[r], dv, c);
+                        }
+                    }
+                }
+            }
+        }
+        if (gx < a.g_size) {
+#pragma unroll
+            for (int r = 0; r < kRowsPerWarp; ++r) {
+                const int gy = gy0 + r;
+                if (gy < a.g_size) {
+                    float2* gp = grid + ((unsigned long long)(gy) * a.g_size + gx);
+                    float2 v = *gp;
+                    v.x += acc[r].x;
+                    v.y += acc[r].y;
+                    *gp = v;
+                }
+            }
+        }
+    }
+}
+
+// Degridding on the gridding plan (the adjoint of grid_tile_kernel).  A lane holds its 16 grid
+// points in registers; for each sample of the cell a warp whose block meets the footprint forms
+// the partial dot product of its block with the table, reduces it with shuffles, and the CTA
+// adds its 8 warp partials in warp order into the sample's slot for this tile.  A final pass
+// (slot_reduce_kernel) adds each sample's tile slots in tile order: no atomics, deterministic.
+template <class Tab, int kS>
+__global__ void __launch_bounds__(kTileThreads, 3)
+degrid_tile_kernel(const float2* __restrict__ grid, const typename Tab::elem* __restrict__ ctab,
+                   const int* __restrict__ iu, const int* __restrict__ iv,
+                   const int* __restrict__ coff, const u32* __restrict__ order,
+                   const u32* __restrict__ tile_start, const u32* __restrict__ tile_count,
+                   const u32* __restrict__ items, const u32* __restrict__ group_start,
+                   float2* __restrict__ slots, int max_tiles, GridArgs a)
+{
+    __shared__ int4 sm_rec[kTileChunk];              // (sample, first column, first row, cOffset)
+    __shared__ float2 sm_part[kTileChunk][kTileWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
+    const u32 i1 = group_start[a.group + 1];
+    for (u32 it = group_start[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
+        const u32 cell = items[it];
+        const u32 cnt = tile_count[cell];
+        const u32 start = tile_start[cell];
+        const int tile = int(cell % u32(a.ntiles));
+        const int tx = tile % a.ntx, ty = tile / a.ntx;
+        const int bx0 = tx * kTileW + (warp % (kTileW / 32)) * 32;
+        const int gx = bx0 + lane;
+        const int gy0 = ty * kTileH + (warp / (kTileW / 32)) * kRowsPerWarp;
+        float2 gv[kRowsPerWarp];
+#pragma unroll
+        for (int r = 0; r < kRowsPerWarp; ++r)
+            gv[r] = (gx < a.g_size && gy0 + r < a.g_size) ? grid[(unsigned long long)(gy0 + r) * a.g_size + gx] : make_float2(0.f, 0.f);
+
+        for (u32 base = 0; base < cnt; base += kTileChunk) {
+            const int m = int(cnt - base < u32(kTileChunk) ? cnt - base : u32(kTileChunk));
+            __syncthreads();
+            if (threadIdx.x < m) {
+                const u32 k = order[start + base + threadIdx.x];
+                sm_rec[threadIdx.x] = make_int4(int(k), iu[k] - a.support, iv[k], coff[k]);
+            }
+            __syncthreads();
+            for (int j = 0; j < m; ++j) {
+                const int4 q = sm_rec[j];
+                const int fx = q.y, fy = q.z;
+                const int dy0 = gy0 - fy;
+                float2 v = make_float2(0.f, 0.f);
+                if (!(dy0 >= s || dy0 + kRowsPerWarp <= 0) && !(fx > bx0 + 31 || fx + s <= bx0)) {  // warp-uniform
+                    const int dx = gx - fx;
+                    const bool colok = unsigned(dx) < unsigned(s);
+                    const int ci = q.w + dy0 * s + dx;
+                    // four independent partial sums keep the FMA chains short
+                    float2 pv[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
+                                    make_float2(0.f, 0.f)};
+                    if (dy0 >= 0 && dy0 + kRowsPerWarp <= s) {
+                        if (colok) {
+#pragma unroll
+                            for (int r = 0; r < kRowsPerWarp; ++r) cmac<Tab::kReal>(pv[r & 3], gv[r], Tab::load(ctab + (ci + r * s)));
+                        }
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < kRowsPerWarp; ++r) {
+                            if (colok && unsigned(dy0 + r) < unsigned(s)) {
+                                const float2 c = Tab::load(ctab + (ci + r * s));
+                                cmac<Tab::kReal>(pv[r & 3], gv[r], c);
+                            }
+                        }
+                    }
+                    v = make_float2((pv[0].x + pv[1].x) + (pv[2].x + pv[3].x), (pv[0].y + pv[1].y) + (pv[2].y + pv[3].y));
+#pragma unroll
+                    for (int o = 16; o; o >>= 1) {
+                        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+                        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+                    }
+                }
+                if (lane == 0) sm_part[j][warp] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x < m) {
+                const int4 q = sm_rec[threadIdx.x];
+                float2 v = sm_part[threadIdx.x][0];
+#pragma unroll
+                for (int w = 1; w < kTileWarps; ++w) {
+                    v.x += sm_part[threadIdx.x][w].x;
+                    v.y += sm_part[threadIdx.x][w].y;
+                }
+                const int sx0 = q.y / kTileW, sx1 = (q.y + s - 1) / kTileW, sy0 = q.z / kTileH;
+                const int slot = (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0);
+                slots[(unsigned long long)(u32(q.x)) * max_tiles + slot] = v;
+            }
+        }
+    }
+}
+
+}  // namespace tcv

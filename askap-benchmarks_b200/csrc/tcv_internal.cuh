@@ -8,43 +8,11 @@
 #include <cstddef>
 
 #include "tconvolve.h"
+#include "tcv_device.cuh"
 
 namespace tcv {
 
-// ------------------------------------------------------------------------------------------
-// Table loaders.  Every storage form returns the entry as (re, im) floats; the real forms
-// return im = 0 and tell the multiply-accumulate to skip the imaginary products, which gives
-// exactly the same result as the complex form on a table whose imaginary parts are zero
-// (fma(-d.im, 0, acc) == acc).
-// ------------------------------------------------------------------------------------------
-struct TabC64 {
-    static constexpr bool kReal = false;
-    using elem = float2;
-    __device__ __forceinline__ static float2 load(const elem* p) { return __ldg(p); }
-};
-struct TabR32 {
-    static constexpr bool kReal = true;
-    using elem = float;
-    __device__ __forceinline__ static float2 load(const elem* p) { return make_float2(__ldg(p), 0.f); }
-};
-struct TabCBF16 {
-    static constexpr bool kReal = false;
-    using elem = uint32_t;  // (re, im) bfloat16 pair, re in the low half
-    __device__ __forceinline__ static float2 load(const elem* p)
-    {
-        const uint32_t u = __ldg(p);
-        return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
-    }
-};
-struct TabRBF16 {
-    static constexpr bool kReal = true;
-    using elem = uint16_t;
-    __device__ __forceinline__ static float2 load(const elem* p)
-    {
-        const uint32_t u = __ldg(p);
-        return make_float2(__uint_as_float(u << 16), 0.f);
-    }
-};
+// float16 table forms (need cuda_fp16.h, so they live outside the NVRTC-compiled device header)
 struct TabCF16 {
     static constexpr bool kReal = false;
     using elem = __half2;
@@ -55,19 +23,6 @@ struct TabRF16 {
     using elem = __half;
     __device__ __forceinline__ static float2 load(const elem* p) { return make_float2(__half2float(__ldg(p)), 0.f); }
 };
-
-// acc += a * b (complex), FP32 fused multiply-adds.  With a real table (b.y == 0 by construction)
-// only the two real-by-complex products are issued.
-template <bool kReal>
-__device__ __forceinline__ void cmac(float2& acc, const float2 a, const float2 b)
-{
-    acc.x = fmaf(a.x, b.x, acc.x);
-    acc.y = fmaf(a.y, b.x, acc.y);
-    if (!kReal) {
-        acc.x = fmaf(-a.y, b.y, acc.x);
-        acc.y = fmaf(a.x, b.y, acc.y);
-    }
-}
 
 // ------------------------------------------------------------------------------------------
 // Plan: binning of samples into grid tiles (gridding) and anchor tiles (degridding).
@@ -134,6 +89,10 @@ tcv_status launch_grid(const tcv_plan* p, const float2* data, const void* c, int
                        float c_scale, float2* grid, cudaStream_t st);
 tcv_status launch_degrid(const tcv_plan* p, const float2* grid, const void* c, int c_type,
                          float c_scale, float2* out, cudaStream_t st);
+
+// tile kernels specialised on the footprint width (tcv_jit.cu): kind 0 gridding, 1 degridding;
+// nullptr when no specialised copy is available (the generic copy is used)
+const void* jit_tile_kernel(int kind, int c_type, int s);
 
 // degridding on the gridding plan (tcv_grid.cu), and the per-sample slot sum it ends with
 tcv_status launch_degrid_tiles(const tcv_plan* p, const float2* grid, const void* c, int c_type,

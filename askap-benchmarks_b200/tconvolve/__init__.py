@@ -8,5 +8,14 @@ from ._lib import (C64, R32, CBF16, RBF16, CF16, RF16, CTYPE_BY_NAME, CTYPE_NAME
                    build, lib, LIB_PATH, BUILD_DIR)
 from .benchmark import Benchmark
 
-__all__ = ["Benchmark", "TcvError", "build", "lib", "C64", "R32", "CBF16", "RBF16", "CF16", "RF16",
+
+def jit_info() -> str:
+    """State of the footprint-width specialisation of the tile kernels (tcv_jit_info)."""
+    return lib().tcv_jit_info().decode()
+
+
+def jit_enable(enabled: bool) -> None:
+    lib().tcv_jit_enable(1 if enabled else 0)
+
+__all__ = ["Benchmark", "jit_info", "jit_enable", "TcvError", "build", "lib", "C64", "R32", "CBF16", "RBF16", "CF16", "RF16",
            "CTYPE_BY_NAME", "CTYPE_NAMES", "LIB_PATH", "BUILD_DIR"]

@@ -90,6 +90,9 @@ SIGNATURES = {
     "tcv_plan_set_degrid_variant": (_I, [_P, _I]),
     "tcv_plan_info": (_I, [_P, _P, _P, _P, _P, _P]),
     "tcv_plan_destroy": (None, [_P]),
+    "tcv_jit_prepare": (_I, [_I, _I]),
+    "tcv_jit_enable": (None, [_I]),
+    "tcv_jit_info": (ctypes.c_char_p, []),
     "tcv_grid_raw": (_I, [_P, _I64, _I, _P, _I, _F, _I64, _P, _P, _P, _P, _I, _P, _S, _P]),
     "tcv_degrid_raw": (_I, [_P, _I, _I, _P, _I, _F, _I64, _P, _P, _P, _P, _I64, _P, _S, _P]),
     "tcv_static_scratch_bytes": (_S, []),

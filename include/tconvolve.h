@@ -163,6 +163,16 @@ tcv_status tcv_plan_info(const tcv_plan *plan, int *tile_w, int *tile_h, int *an
                          int *degrid_mode, int *n_tiles);
 void tcv_plan_destroy(tcv_plan *plan);
 
+/* Tile kernels specialised on the footprint width.  The first launch of the tile kernels for a
+ * (table form, support) builds copies with sSize = 2*support+1 a compile-time constant (NVRTC,
+ * about a second, cached for the process); tcv_jit_prepare builds them ahead of time (set-up;
+ * call it before any stream capture).  If NVRTC is unavailable or a build fails, the generic
+ * copies compiled into the library run instead.  tcv_jit_enable(0) forces the generic copies;
+ * tcv_jit_info describes the current state. */
+tcv_status tcv_jit_prepare(int c_type, int support);
+void tcv_jit_enable(int enabled);
+const char *tcv_jit_info(void);
+
 /* One-call forms: plan_build + grid (or degrid) in the given workspace. */
 tcv_status tcv_grid_raw(const float *d_data, int64_t n, int support, const void *d_c, int c_type,
                         float c_scale, int64_t c_len, const int32_t *d_coff, const int32_t *d_iu,

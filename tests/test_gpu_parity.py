@@ -428,3 +428,34 @@ def test_device_setup_functions(tcv, orc, cuda_ok):
     assert np.array_equal(iu.cpu().numpy(), iu_r)
     assert np.array_equal(iv.cpu().numpy(), iv_r)
     assert np.array_equal(co.cpu().numpy(), co_r)
+
+
+@pytest.mark.parametrize("form", ["c64", "r32"])
+def test_specialised_tile_kernels_match_generic(tcv, orc, cuda_ok, form):
+    """The tile kernels compiled at run time with the footprint width as a constant give the same
+    results as the generic copies (and are really in use on the device)."""
+    prob = PROBLEMS["c1"]
+    vis = normal_vis(prob.n_data(), VIS_SEED)
+    out = {}
+    try:
+        for jit in (True, False):
+            tcv.jit_enable(jit)
+            b = tcv.Benchmark(**prob.kwargs())
+            b.set_path("direct")
+            b.init()
+            b.set_ctype(form)
+            b.set_data(vis)
+            b.runGrid()
+            b.runDegrid()
+            b.sync()
+            out[jit] = (b.grid(), b.outdata())
+            if jit:
+                assert "specialised tile kernels in use" in tcv.jit_info(), tcv.jit_info()
+            b.close()
+    finally:
+        tcv.jit_enable(True)
+    assert orc.rel_l2(out[True][0], out[False][0]) <= 1e-6
+    assert orc.rel_l2(out[True][1], out[False][1]) <= 1e-6
+    r = orc.run_plain(oracle_config(orc, prob), vis=vis, threads=8)
+    assert orc.rel_l2(out[True][0], r["grid"]) <= REL_L2_FP32
+    assert orc.rel_l2(out[True][1], r["outdata"]) <= REL_L2_FP32
