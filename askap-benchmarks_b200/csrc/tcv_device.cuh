@@ -44,16 +44,19 @@ struct GridArgs {
 // (fma(-d.im, 0, acc) == acc).
 // ------------------------------------------------------------------------------------------
 struct TabC64 {
+    static constexpr int kMinBlocks = 3;  // CTAs per SM the register budget is sized for
     static constexpr bool kReal = false;
     using elem = float2;
     __device__ __forceinline__ static float2 load(const elem* p) { return __ldg(p); }
 };
 struct TabR32 {
+    static constexpr int kMinBlocks = 4;
     static constexpr bool kReal = true;
     using elem = float;
     __device__ __forceinline__ static float2 load(const elem* p) { return make_float2(__ldg(p), 0.f); }
 };
 struct TabCBF16 {
+    static constexpr int kMinBlocks = 3;
     static constexpr bool kReal = false;
     using elem = u32;  // (re, im) bfloat16 pair, re in the low half
     __device__ __forceinline__ static float2 load(const elem* p)
@@ -63,6 +66,7 @@ struct TabCBF16 {
     }
 };
 struct TabRBF16 {
+    static constexpr int kMinBlocks = 4;
     static constexpr bool kReal = true;
     using elem = unsigned short;
     __device__ __forceinline__ static float2 load(const elem* p)
@@ -85,8 +89,43 @@ __device__ __forceinline__ void cmac(float2& acc, const float2 a, const float2 b
     }
 }
 
+// The CTA's work is the sequence of chunks (up to kTileChunk samples) of the cells it owns (every
+// gridDim.x-th non-empty cell of the plane group).  Chunk i is staged in shared memory while chunk
+// i-1 is processed, so each chunk costs one barrier and the next cell's samples arrive early.
+struct ChunkCursor {
+    u32 it, base;  // cell list position, first sample of the chunk in that cell
+    u32 cell, cnt, start;
+    int m;         // samples in the chunk (0: no more work)
+};
+
+__device__ __forceinline__ void cursor_load(ChunkCursor& c, u32 it, u32 i1, const u32* __restrict__ items,
+                                            const u32* __restrict__ tile_start, const u32* __restrict__ tile_count)
+{
+    c.it = it;
+    c.base = 0;
+    c.m = 0;
+    if (it < i1) {
+        c.cell = items[it];
+        c.cnt = tile_count[c.cell];
+        c.start = tile_start[c.cell];
+        c.m = int(c.cnt < u32(kTileChunk) ? c.cnt : u32(kTileChunk));
+    }
+}
+
+__device__ __forceinline__ void cursor_next(ChunkCursor& c, u32 i1, const u32* __restrict__ items,
+                                            const u32* __restrict__ tile_start, const u32* __restrict__ tile_count)
+{
+    if (c.base + u32(kTileChunk) < c.cnt) {
+        c.base += u32(kTileChunk);
+        const u32 left = c.cnt - c.base;
+        c.m = int(left < u32(kTileChunk) ? left : u32(kTileChunk));
+    } else {
+        cursor_load(c, c.it + gridDim.x, i1, items, tile_start, tile_count);
+    }
+}
+
 template <class Tab, int kS>
-__global__ void __launch_bounds__(kTileThreads, 3)
+__global__ void __launch_bounds__(kTileThreads, Tab::kMinBlocks)
 grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
                  const int* __restrict__ iu, const int* __restrict__ iv,
                  const int* __restrict__ coff, const u32* __restrict__ order,
@@ -94,78 +133,86 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
                  const u32* __restrict__ items, const u32* __restrict__ group_start,
                  float2* __restrict__ grid, GridArgs a)
 {
-    __shared__ float4 sm_rec[kTileChunk];  // (data.re, data.im, first column, first row)
-    __shared__ int sm_coff[kTileChunk];
+    __shared__ float4 sm_rec[2][kTileChunk];  // (data.re, data.im, first column, first row)
+    __shared__ int sm_coff[2][kTileChunk];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
-    // persistent: this CTA takes every gridDim.x-th non-empty cell of the group
     const u32 i1 = group_start[a.group + 1];
-    for (u32 it = group_start[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
-        const u32 cell = items[it];
-        const u32 cnt = tile_count[cell];
-        const u32 start = tile_start[cell];
-        const int tile = int(cell % u32(a.ntiles));
+    auto stage = [&](const ChunkCursor& c, int buf) {
+        if (int(threadIdx.x) < c.m) {
+            const u32 k = order[c.start + c.base + threadIdx.x];
+            const float2 d = data[k];
+            sm_rec[buf][threadIdx.x] = make_float4(d.x * a.c_scale, d.y * a.c_scale,
+                                                   __int_as_float(iu[k] - a.support), __int_as_float(iv[k]));
+            sm_coff[buf][threadIdx.x] = coff[k];
+        }
+    };
+    ChunkCursor cur;
+    cursor_load(cur, group_start[a.group] + blockIdx.x, i1, items, tile_start, tile_count);
+    stage(cur, 0);
+    __syncthreads();
+    float2 acc[kRowsPerWarp];
+#pragma unroll
+    for (int r = 0; r < kRowsPerWarp; ++r) acc[r] = make_float2(0.f, 0.f);
+    int buf = 0;
+    while (cur.m > 0) {
+        ChunkCursor nxt = cur;
+        cursor_next(nxt, i1, items, tile_start, tile_count);
+        stage(nxt, buf ^ 1);  // overlaps with the work below
+
+        const int tile = int(cur.cell % u32(a.ntiles));
         const int tx = tile % a.ntx, ty = tile / a.ntx;
         const int bx0 = tx * kTileW + (warp % (kTileW / 32)) * 32;  // first column of this warp
         const int gx = bx0 + lane;
         const int gy0 = ty * kTileH + (warp / (kTileW / 32)) * kRowsPerWarp;
-
-        float2 acc[kRowsPerWarp];
+        for (int j = 0; j < cur.m; ++j) {
+            const float4 q = sm_rec[buf][j];
+            const int fx = __float_as_int(q.z), fy = __float_as_int(q.w);
+            const int dy0 = gy0 - fy;  // footprint row of this warp's first row
+            if (dy0 >= s || dy0 + kRowsPerWarp <= 0) continue;   // warp-uniform
+            if (fx > bx0 + 31 || fx + s <= bx0) continue;          // warp-uniform
+            const int dx = gx - fx;
+            const bool colok = unsigned(dx) < unsigned(s);
+            const float2 dv = make_float2(q.x, q.y);
+            // 32-bit element index off the kernel-wide table base (tables hold < 2^31 entries)
+            const int ci = sm_coff[buf][j] + dy0 * s + dx;
+            if (dy0 >= 0 && dy0 + kRowsPerWarp <= s) {
+                // every row of the block is inside the footprint: only the column test remains
+                if (colok) {
 #pragma unroll
-        for (int r = 0; r < kRowsPerWarp; ++r) acc[r] = make_float2(0.f, 0.f);
-
-        for (u32 base = 0; base < cnt; base += kTileChunk) {
-            const int m = int(cnt - base < u32(kTileChunk) ? cnt - base : u32(kTileChunk));
-            __syncthreads();
-            if (threadIdx.x < m) {
-                const u32 k = order[start + base + threadIdx.x];
-                const float2 d = data[k];
-                sm_rec[threadIdx.x] = make_float4(d.x * a.c_scale, d.y * a.c_scale,
-                                                  __int_as_float(iu[k] - a.support), __int_as_float(iv[k]));
-                sm_coff[threadIdx.x] = coff[k];
-            }
-            __syncthreads();
-            for (int j = 0; j < m; ++j) {
-                const float4 q = sm_rec[j];
-                const int fx = __float_as_int(q.z), fy = __float_as_int(q.w);
-                const int dy0 = gy0 - fy;  // footprint row of this warp's first row
-                if (dy0 >= s || dy0 + kRowsPerWarp <= 0) continue;   // warp-uniform
-                if (fx > bx0 + 31 || fx + s <= bx0) continue;          // warp-uniform
-                const int dx = gx - fx;
-                const bool colok = unsigned(dx) < unsigned(s);
-                const float2 dv = make_float2(q.x, q.y);
-                // 32-bit element index off the kernel-wide table base (tables hold < 2^31 entries)
-                const int ci = sm_coff[j] + dy0 * s + dx;
-                if (dy0 >= 0 && dy0 + kRowsPerWarp <= s) {
-                    // every row of the block is inside the footprint: only the column test remains
-                    if (colok) {
+                    for (int r = 0; r < kRowsPerWarp; ++r) cmac<Tab::kReal>(acc[r], dv, Tab::load(ctab + (ci + r * s)));
+                }
+            } else {
 #pragma unroll
-                        for (int r = 0; r < kRowsPerWarp; ++r) cmac<Tab::kReal>(acc[r], dv, Tab::load(ctab + (ci + r * s)));
-                    }
-                } else {
-#pragma unroll
-                    for (int r = 0; r < kRowsPerWarp; ++r) {
-                        if (colok && unsigned(dy0 + r) < unsigned(s)) {
-                            const float2 c = Tab::load(ctab + (ci + r * s));
-                            cmac<Tab::kReal>(acc[r], dv, c);
-                        }
+                for (int r = 0; r < kRowsPerWarp; ++r) {
+                    if (colok && unsigned(dy0 + r) < unsigned(s)) {
+                        const float2 c = Tab::load(ctab + (ci + r * s));
+                        cmac<Tab::kReal>(acc[r], dv, c);
                     }
                 }
             }
         }
-        if (gx < a.g_size) {
+        if (nxt.it != cur.it || nxt.m == 0) {
+            // the cell is complete: add its tile into the grid (each point has this one owner)
+            if (gx < a.g_size) {
 #pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) {
-                const int gy = gy0 + r;
-                if (gy < a.g_size) {
-                    float2* gp = grid + ((unsigned long long)(gy) * a.g_size + gx);
-                    float2 v = *gp;
-                    v.x += acc[r].x;
-                    v.y += acc[r].y;
-                    *gp = v;
+                for (int r = 0; r < kRowsPerWarp; ++r) {
+                    const int gy = gy0 + r;
+                    if (gy < a.g_size) {
+                        float2* gp = grid + ((unsigned long long)(gy) * a.g_size + gx);
+                        float2 v = *gp;
+                        v.x += acc[r].x;
+                        v.y += acc[r].y;
+                        *gp = v;
+                    }
                 }
             }
+#pragma unroll
+            for (int r = 0; r < kRowsPerWarp; ++r) acc[r] = make_float2(0.f, 0.f);
         }
+        __syncthreads();  // the next chunk is staged; this chunk's records are free
+        cur = nxt;
+        buf ^= 1;
     }
 }
 

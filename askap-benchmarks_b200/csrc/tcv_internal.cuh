@@ -14,11 +14,13 @@ namespace tcv {
 
 // float16 table forms (need cuda_fp16.h, so they live outside the NVRTC-compiled device header)
 struct TabCF16 {
+    static constexpr int kMinBlocks = 3;
     static constexpr bool kReal = false;
     using elem = __half2;
     __device__ __forceinline__ static float2 load(const elem* p) { return __half22float2(__ldg(p)); }
 };
 struct TabRF16 {
+    static constexpr int kMinBlocks = 4;
     static constexpr bool kReal = true;
     using elem = __half;
     __device__ __forceinline__ static float2 load(const elem* p) { return make_float2(__half2float(__ldg(p)), 0.f); }
