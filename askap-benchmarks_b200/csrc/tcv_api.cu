@@ -30,6 +30,7 @@ struct tcv_ctx {
     size_t work_bytes = 0;
     void* c_scratch = nullptr;
     tcv_plan* plan = nullptr;
+    tcv_tuning tuning{16, 32};
     bool initialized = false;
     std::string err;
 };
@@ -110,7 +111,7 @@ tcv_status ensure_tables(tcv_ctx* c)
         c->c_pad_type = want;
         return TCV_OK;
     }
-    tcv_jit_prepare(t, c->support);  // the direct path's tile kernels, specialised on sSize
+    tcv::jit_prepare(t, 2 * c->support + 1, c->tuning.tile_rows);  // the direct path's tile kernels, specialised on sSize
     if (t == TCV_C_C64 || c->c_alt_type == t) return TCV_OK;
     if (c->c_alt) {
         CTX_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -134,8 +135,17 @@ tcv_status rebuild_plan(tcv_ctx* c)
         tcv_plan_destroy(c->plan);
         c->plan = nullptr;
     }
-    CTX_TRY(c, tcv_plan_build(&c->plan, c->iu, c->iv, c->coff, c->n_data, c->support, c->cfg.g_size,
-                              c->c_len, c->work, c->work_bytes, c->stream));
+    const size_t need = tcv_plan_workspace_bytes_tuned(c->n_data, c->support, c->cfg.g_size, c->c_len, &c->tuning);
+    if (need > c->work_bytes) {
+        CTX_CUDA(c, cudaStreamSynchronize(c->stream));
+        cudaFree(c->work);
+        c->work = nullptr;
+        c->work_bytes = 0;
+        CTX_CUDA(c, cudaMalloc(&c->work, need));
+        c->work_bytes = need;
+    }
+    CTX_TRY(c, tcv_plan_build_tuned(&c->plan, c->iu, c->iv, c->coff, c->n_data, c->support, c->cfg.g_size,
+                                    c->c_len, &c->tuning, c->work, c->work_bytes, c->stream));
     int64_t rej = 0;
     CTX_TRY(c, tcv_plan_rejected(c->plan, &rej, c->stream));
     if (rej > 0) {
@@ -314,6 +324,47 @@ tcv_status tcv_set_path(tcv_ctx* c, int path)
 }
 
 int tcv_get_path(const tcv_ctx* c) { return c ? c->path : -1; }
+
+tcv_status tcv_set_tuning(tcv_ctx* c, const tcv_tuning* t)
+{
+    if (!c || !t) return TCV_ERR_ARG;
+    const tcv_tuning nt{t->tile_rows ? t->tile_rows : 16, t->group_mib ? t->group_mib : 32};
+    if ((nt.tile_rows != 8 && nt.tile_rows != 16 && nt.tile_rows != 32) || nt.group_mib < -1) return TCV_ERR_ARG;
+    const tcv_tuning prev = c->tuning;
+    c->tuning = nt;
+    if (!c->initialized) return TCV_OK;
+    tcv_status s = ensure_tables(c);
+    if (s == TCV_OK) s = rebuild_plan(c);
+    if (s != TCV_OK && s != TCV_ERR_BOUNDS) {
+        c->tuning = prev;
+        rebuild_plan(c);
+    }
+    return s;
+}
+
+tcv_status tcv_get_tuning(const tcv_ctx* c, tcv_tuning* out)
+{
+    if (!c || !out) return TCV_ERR_ARG;
+    *out = c->tuning;
+    return TCV_OK;
+}
+
+tcv_status tcv_tune(tcv_ctx* c, int reps, tcv_tuning* best_out, float* best_ms_out)
+{
+    if (!c || reps < 1) return TCV_ERR_ARG;
+    if (!c->initialized) return fail(c, TCV_ERR_STATE, "tune before init");
+    if (c->path != TCV_PATH_DIRECT) return fail(c, TCV_ERR_UNSUPPORTED, "tuning needs the direct path");
+    const tcv_job job{c->n_data, c->cfg.g_size, reinterpret_cast<float*>(c->grid)};
+    tcv_tuning best{16, 32};
+    float ms = 0.f;
+    CTX_TRY(c, tcv_autotune(&job, 1, c->iu, c->iv, c->coff, reinterpret_cast<const float*>(c->data), active_table(c),
+                            active_code(c), active_scale(c), c->c_len, c->support, reps, &best, &ms, c->stream));
+    const tcv_status s = tcv_set_tuning(c, &best);
+    if (s != TCV_OK) return s;
+    if (best_out) *best_out = best;
+    if (best_ms_out) *best_ms_out = ms;
+    return TCV_OK;
+}
 
 tcv_status tcv_run_grid(tcv_ctx* c)
 {

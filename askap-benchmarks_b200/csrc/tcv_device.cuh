@@ -5,8 +5,9 @@
 // sSize a compile-time constant (kS = sSize), where row offsets become load immediates and loop
 // bounds constants.  Nothing here includes a host header, so both compilers accept it.
 //
-// Output-stationary tiles.  One CTA owns a 64 x 64 tile of the grid; each of its 8 warps owns a
-// 32-column x 16-row block with one accumulator per point held in registers (lane = column).
+// Output-stationary tiles.  One CTA owns a tile of 64 x 4*kR grid points (kR = rows per warp, 8,
+// 16 or 32: the tile shape an autotuner chooses between); each of its 8 warps owns a 32-column x
+// kR-row block with one accumulator per point held in registers (lane = column).
 // The CTA walks the tile's sample list (from the plan), staging sample records in shared memory;
 // for each sample a warp whose block meets the footprint reads the table rows it needs (32
 // consecutive entries per row: one coalesced load per row) and accumulates data * C into its
@@ -14,28 +15,50 @@
 // read-modify-writes.  Every grid point has exactly one owner thread: no atomics, and the result
 // is the same on every run.  Gridding follows attic/tConvolveMPI/Benchmark.cc:125-155.
 //
-// Degridding (Benchmark.cc:158-195) is the adjoint on the same plan: a lane holds its 16 grid
+// Degridding (Benchmark.cc:158-195) is the adjoint on the same plan: a lane holds its kR grid
 // points in registers; for each sample a warp whose block meets the footprint forms the partial
 // dot product of its block with the table, reduces it with shuffles, and the CTA adds its 8 warp
 // partials in warp order into the sample's slot for this tile; a final pass adds each sample's
 // tile slots in tile order.
+//
+// A plan may hold several jobs (channels, Taylor terms) that share the table but have their own
+// samples, grid and grid size.  Tiles of all jobs are numbered in one space; a 32-bit per-tile
+// record gives the job and the tile's column and row, and the job table gives the job's grid.
 #pragma once
 
 namespace tcv {
 
 using u32 = unsigned int;
 
-constexpr int kTileW = 64;
-constexpr int kTileH = 64;
-constexpr int kRowsPerWarp = 16;
-constexpr int kTileWarps = (kTileW / 32) * (kTileH / kRowsPerWarp);
+constexpr int kTileW = 64;         // tile width: two warps of 32 columns
+constexpr int kTileWarps = 8;      // four rows of two warps
 constexpr int kTileThreads = kTileWarps * 32;
 constexpr int kTileChunk = kTileThreads;  // samples staged per round
+__host__ __device__ constexpr int tile_height(int rows_per_warp) { return rows_per_warp * (kTileWarps * 32 / kTileW); }
+
+// One job of a plan: its grid (nullptr: the grid is passed at launch), side, tiles per row and
+// first tile number.
+struct JobDesc {
+    float2* grid;
+    int g_size, ntx;
+    u32 tile_base, n_tiles;
+};
 
 struct GridArgs {
-    int support, s, g_size, ntx, ntiles, group;
+    int support, s, ntiles, group;  // ntiles: tiles of all jobs (cells per plane group)
     float c_scale;
+    float2* grid;                   // grid of a one-job plan given at launch, else nullptr
+    const JobDesc* __restrict__ jobs;
+    const u32* __restrict__ tinfo;  // per tile: column | row << 11 | job << 22
 };
+
+// per-tile record: tile column (11 bits), tile row (11 bits), job (10 bits)
+__host__ __device__ constexpr u32 tile_record(u32 job, u32 tx, u32 ty) { return tx | (ty << 11) | (job << 22); }
+__host__ __device__ constexpr int rec_tx(u32 r) { return int(r & 0x7ffu); }
+__host__ __device__ constexpr int rec_ty(u32 r) { return int((r >> 11) & 0x7ffu); }
+__host__ __device__ constexpr int rec_job(u32 r) { return int(r >> 22); }
+constexpr int kMaxJobs = 1 << 10;
+constexpr int kMaxTilesPerSide = 1 << 11;
 
 // ------------------------------------------------------------------------------------------
 // Table loaders.  Every storage form returns the entry as (re, im) floats; the real forms
@@ -89,50 +112,61 @@ __device__ __forceinline__ void cmac(float2& acc, const float2 a, const float2 b
     }
 }
 
+// CTAs per SM the register budget of a tile kernel is sized for: kR accumulators (gridding) or
+// grid values (degridding) per lane, two floats each.
+template <class Tab, int kR>
+__host__ __device__ constexpr int grid_min_blocks() { return kR >= 32 ? 2 : Tab::kMinBlocks; }
+template <int kR>
+__host__ __device__ constexpr int degrid_min_blocks() { return kR >= 32 ? 2 : 3; }
+
 // The CTA's work is the sequence of chunks (up to kTileChunk samples) of the cells it owns (every
 // gridDim.x-th non-empty cell of the plane group).  Chunk i is staged in shared memory while chunk
 // i-1 is processed, so each chunk costs one barrier and the next cell's samples arrive early.
 struct ChunkCursor {
     u32 it, base;  // cell list position, first sample of the chunk in that cell
-    u32 cell, cnt, start;
+    u32 cnt, start;
+    u32 ti;        // the cell's tile record (tile_record)
     int m;         // samples in the chunk (0: no more work)
 };
 
 __device__ __forceinline__ void cursor_load(ChunkCursor& c, u32 it, u32 i1, const u32* __restrict__ items,
-                                            const u32* __restrict__ tile_start, const u32* __restrict__ tile_count)
+                                            const u32* __restrict__ tile_start, const u32* __restrict__ tile_count,
+                                            const GridArgs& a)
 {
     c.it = it;
     c.base = 0;
     c.m = 0;
     if (it < i1) {
-        c.cell = items[it];
-        c.cnt = tile_count[c.cell];
-        c.start = tile_start[c.cell];
+        const u32 cell = items[it];
+        c.cnt = tile_count[cell];
+        c.start = tile_start[cell];
+        c.ti = a.tinfo[cell - u32(a.group) * u32(a.ntiles)];
         c.m = int(c.cnt < u32(kTileChunk) ? c.cnt : u32(kTileChunk));
     }
 }
 
 __device__ __forceinline__ void cursor_next(ChunkCursor& c, u32 i1, const u32* __restrict__ items,
-                                            const u32* __restrict__ tile_start, const u32* __restrict__ tile_count)
+                                            const u32* __restrict__ tile_start, const u32* __restrict__ tile_count,
+                                            const GridArgs& a)
 {
     if (c.base + u32(kTileChunk) < c.cnt) {
         c.base += u32(kTileChunk);
         const u32 left = c.cnt - c.base;
         c.m = int(left < u32(kTileChunk) ? left : u32(kTileChunk));
     } else {
-        cursor_load(c, c.it + gridDim.x, i1, items, tile_start, tile_count);
+        cursor_load(c, c.it + gridDim.x, i1, items, tile_start, tile_count, a);
     }
 }
 
-template <class Tab, int kS>
-__global__ void __launch_bounds__(kTileThreads, Tab::kMinBlocks)
+template <class Tab, int kS, int kR>
+__global__ void __launch_bounds__(kTileThreads, grid_min_blocks<Tab, kR>())
 grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
                  const int* __restrict__ iu, const int* __restrict__ iv,
                  const int* __restrict__ coff, const u32* __restrict__ order,
                  const u32* __restrict__ tile_start, const u32* __restrict__ tile_count,
-                 const u32* __restrict__ items, const u32* __restrict__ group_start,
-                 float2* __restrict__ grid, GridArgs a)
+                 const u32* __restrict__ items, const u32* __restrict__ group_start, GridArgs a)
 {
+    constexpr int kTH = tile_height(kR);
     __shared__ float4 sm_rec[2][kTileChunk];  // (data.re, data.im, first column, first row)
     __shared__ int sm_coff[2][kTileChunk];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -148,43 +182,42 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
         }
     };
     ChunkCursor cur;
-    cursor_load(cur, group_start[a.group] + blockIdx.x, i1, items, tile_start, tile_count);
+    cursor_load(cur, group_start[a.group] + blockIdx.x, i1, items, tile_start, tile_count, a);
     stage(cur, 0);
     __syncthreads();
-    float2 acc[kRowsPerWarp];
+    float2 acc[kR];
 #pragma unroll
-    for (int r = 0; r < kRowsPerWarp; ++r) acc[r] = make_float2(0.f, 0.f);
+    for (int r = 0; r < kR; ++r) acc[r] = make_float2(0.f, 0.f);
     int buf = 0;
     while (cur.m > 0) {
         ChunkCursor nxt = cur;
-        cursor_next(nxt, i1, items, tile_start, tile_count);
+        cursor_next(nxt, i1, items, tile_start, tile_count, a);
         stage(nxt, buf ^ 1);  // overlaps with the work below
 
-        const int tile = int(cur.cell % u32(a.ntiles));
-        const int tx = tile % a.ntx, ty = tile / a.ntx;
+        const int tx = rec_tx(cur.ti), ty = rec_ty(cur.ti);
         const int bx0 = tx * kTileW + (warp % (kTileW / 32)) * 32;  // first column of this warp
         const int gx = bx0 + lane;
-        const int gy0 = ty * kTileH + (warp / (kTileW / 32)) * kRowsPerWarp;
+        const int gy0 = ty * kTH + (warp / (kTileW / 32)) * kR;
         for (int j = 0; j < cur.m; ++j) {
             const float4 q = sm_rec[buf][j];
             const int fx = __float_as_int(q.z), fy = __float_as_int(q.w);
             const int dy0 = gy0 - fy;  // footprint row of this warp's first row
-            if (dy0 >= s || dy0 + kRowsPerWarp <= 0) continue;   // warp-uniform
-            if (fx > bx0 + 31 || fx + s <= bx0) continue;          // warp-uniform
+            if (dy0 >= s || dy0 + kR <= 0) continue;      // warp-uniform
+            if (fx > bx0 + 31 || fx + s <= bx0) continue;  // warp-uniform
             const int dx = gx - fx;
             const bool colok = unsigned(dx) < unsigned(s);
             const float2 dv = make_float2(q.x, q.y);
             // 32-bit element index off the kernel-wide table base (tables hold < 2^31 entries)
             const int ci = sm_coff[buf][j] + dy0 * s + dx;
-            if (dy0 >= 0 && dy0 + kRowsPerWarp <= s) {
+            if (dy0 >= 0 && dy0 + kR <= s) {
                 // every row of the block is inside the footprint: only the column test remains
                 if (colok) {
 #pragma unroll
-                    for (int r = 0; r < kRowsPerWarp; ++r) cmac<Tab::kReal>(acc[r], dv, Tab::load(ctab + (ci + r * s)));
+                    for (int r = 0; r < kR; ++r) cmac<Tab::kReal>(acc[r], dv, Tab::load(ctab + (ci + r * s)));
                 }
             } else {
 #pragma unroll
-                for (int r = 0; r < kRowsPerWarp; ++r) {
+                for (int r = 0; r < kR; ++r) {
                     if (colok && unsigned(dy0 + r) < unsigned(s)) {
                         const float2 c = Tab::load(ctab + (ci + r * s));
                         cmac<Tab::kReal>(acc[r], dv, c);
@@ -193,13 +226,16 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
             }
         }
         if (nxt.it != cur.it || nxt.m == 0) {
-            // the cell is complete: add its tile into the grid (each point has this one owner)
-            if (gx < a.g_size) {
+            // the cell is complete: add its tile into the job's grid (each point has this one owner)
+            const JobDesc& jd = a.jobs[rec_job(cur.ti)];
+            const int gs = jd.g_size;
+            float2* grid = a.grid ? a.grid : jd.grid;
+            if (gx < gs) {
 #pragma unroll
-                for (int r = 0; r < kRowsPerWarp; ++r) {
+                for (int r = 0; r < kR; ++r) {
                     const int gy = gy0 + r;
-                    if (gy < a.g_size) {
-                        float2* gp = grid + ((unsigned long long)(gy) * a.g_size + gx);
+                    if (gy < gs) {
+                        float2* gp = grid + ((unsigned long long)(gy) * gs + gx);
                         float2 v = *gp;
                         v.x += acc[r].x;
                         v.y += acc[r].y;
@@ -208,7 +244,7 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
                 }
             }
 #pragma unroll
-            for (int r = 0; r < kRowsPerWarp; ++r) acc[r] = make_float2(0.f, 0.f);
+            for (int r = 0; r < kR; ++r) acc[r] = make_float2(0.f, 0.f);
         }
         __syncthreads();  // the next chunk is staged; this chunk's records are free
         cur = nxt;
@@ -216,20 +252,21 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
     }
 }
 
-// Degridding on the gridding plan (the adjoint of grid_tile_kernel).  A lane holds its 16 grid
+// Degridding on the gridding plan (the adjoint of grid_tile_kernel).  A lane holds its kR grid
 // points in registers; for each sample of the cell a warp whose block meets the footprint forms
 // the partial dot product of its block with the table, reduces it with shuffles, and the CTA
 // adds its 8 warp partials in warp order into the sample's slot for this tile.  A final pass
 // (slot_reduce_kernel) adds each sample's tile slots in tile order: no atomics, deterministic.
-template <class Tab, int kS>
-__global__ void __launch_bounds__(kTileThreads, 3)
-degrid_tile_kernel(const float2* __restrict__ grid, const typename Tab::elem* __restrict__ ctab,
+template <class Tab, int kS, int kR>
+__global__ void __launch_bounds__(kTileThreads, degrid_min_blocks<kR>())
+degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                    const int* __restrict__ iu, const int* __restrict__ iv,
                    const int* __restrict__ coff, const u32* __restrict__ order,
                    const u32* __restrict__ tile_start, const u32* __restrict__ tile_count,
                    const u32* __restrict__ items, const u32* __restrict__ group_start,
                    float2* __restrict__ slots, int max_tiles, GridArgs a)
 {
+    constexpr int kTH = tile_height(kR);
     __shared__ int4 sm_rec[kTileChunk];              // (sample, first column, first row, cOffset)
     __shared__ float2 sm_part[kTileChunk][kTileWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -239,15 +276,18 @@ degrid_tile_kernel(const float2* __restrict__ grid, const typename Tab::elem* __
         const u32 cell = items[it];
         const u32 cnt = tile_count[cell];
         const u32 start = tile_start[cell];
-        const int tile = int(cell % u32(a.ntiles));
-        const int tx = tile % a.ntx, ty = tile / a.ntx;
+        const u32 ti = a.tinfo[cell - u32(a.group) * u32(a.ntiles)];
+        const JobDesc& jd = a.jobs[rec_job(ti)];
+        const int gs = jd.g_size;
+        const float2* grid = a.grid ? a.grid : jd.grid;
+        const int tx = rec_tx(ti), ty = rec_ty(ti);
         const int bx0 = tx * kTileW + (warp % (kTileW / 32)) * 32;
         const int gx = bx0 + lane;
-        const int gy0 = ty * kTileH + (warp / (kTileW / 32)) * kRowsPerWarp;
-        float2 gv[kRowsPerWarp];
+        const int gy0 = ty * kTH + (warp / (kTileW / 32)) * kR;
+        float2 gv[kR];
 #pragma unroll
-        for (int r = 0; r < kRowsPerWarp; ++r)
-            gv[r] = (gx < a.g_size && gy0 + r < a.g_size) ? grid[(unsigned long long)(gy0 + r) * a.g_size + gx] : make_float2(0.f, 0.f);
+        for (int r = 0; r < kR; ++r)
+            gv[r] = (gx < gs && gy0 + r < gs) ? grid[(unsigned long long)(gy0 + r) * gs + gx] : make_float2(0.f, 0.f);
 
         for (u32 base = 0; base < cnt; base += kTileChunk) {
             const int m = int(cnt - base < u32(kTileChunk) ? cnt - base : u32(kTileChunk));
@@ -262,21 +302,21 @@ degrid_tile_kernel(const float2* __restrict__ grid, const typename Tab::elem* __
                 const int fx = q.y, fy = q.z;
                 const int dy0 = gy0 - fy;
                 float2 v = make_float2(0.f, 0.f);
-                if (!(dy0 >= s || dy0 + kRowsPerWarp <= 0) && !(fx > bx0 + 31 || fx + s <= bx0)) {  // warp-uniform
+                if (!(dy0 >= s || dy0 + kR <= 0) && !(fx > bx0 + 31 || fx + s <= bx0)) {  // warp-uniform
                     const int dx = gx - fx;
                     const bool colok = unsigned(dx) < unsigned(s);
                     const int ci = q.w + dy0 * s + dx;
                     // four independent partial sums keep the FMA chains short
                     float2 pv[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
                                     make_float2(0.f, 0.f)};
-                    if (dy0 >= 0 && dy0 + kRowsPerWarp <= s) {
+                    if (dy0 >= 0 && dy0 + kR <= s) {
                         if (colok) {
 #pragma unroll
-                            for (int r = 0; r < kRowsPerWarp; ++r) cmac<Tab::kReal>(pv[r & 3], gv[r], Tab::load(ctab + (ci + r * s)));
+                            for (int r = 0; r < kR; ++r) cmac<Tab::kReal>(pv[r & 3], gv[r], Tab::load(ctab + (ci + r * s)));
                         }
                     } else {
 #pragma unroll
-                        for (int r = 0; r < kRowsPerWarp; ++r) {
+                        for (int r = 0; r < kR; ++r) {
                             if (colok && unsigned(dy0 + r) < unsigned(s)) {
                                 const float2 c = Tab::load(ctab + (ci + r * s));
                                 cmac<Tab::kReal>(pv[r & 3], gv[r], c);
@@ -301,7 +341,7 @@ degrid_tile_kernel(const float2* __restrict__ grid, const typename Tab::elem* __
                     v.x += sm_part[threadIdx.x][w].x;
                     v.y += sm_part[threadIdx.x][w].y;
                 }
-                const int sx0 = q.y / kTileW, sx1 = (q.y + s - 1) / kTileW, sy0 = q.z / kTileH;
+                const int sx0 = q.y / kTileW, sx1 = (q.y + s - 1) / kTileW, sy0 = q.z / kTH;
                 const int slot = (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0);
                 slots[(unsigned long long)(u32(q.x)) * max_tiles + slot] = v;
             }

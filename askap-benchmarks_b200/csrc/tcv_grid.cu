@@ -8,23 +8,7 @@
 namespace tcv {
 namespace {
 
-template <class Tab>
-int resident_ctas()
-{
-    static int per_sm = 0;
-    static int sms = 0;
-    if (!per_sm) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_tile_kernel<Tab, 0>, kTileThreads, 0);
-        if (per_sm < 1) per_sm = 1;
-    }
-    return per_sm * sms;
-}
-
-// One persistent launch per plane group, in group order on the stream: launches of one stream
-// run one after another, so a tile's read-modify-write never races with another group's.
+// CTAs of a persistent launch: every SM filled to the kernel's occupancy
 int resident_of(const void* kernel)
 {
     int dev = 0, sms = 148, per_sm = 0;
@@ -35,79 +19,94 @@ int resident_of(const void* kernel)
     return per_sm * sms;
 }
 
-template <class Tab>
+GridArgs make_args(const tcv_plan* p, int grp, float c_scale, float2* grid)
+{
+    const PlanGeom& g = p->g;
+    GridArgs a{};
+    a.support = g.support;
+    a.s = g.s;
+    a.ntiles = int(g.ntiles);
+    a.group = grp;
+    a.c_scale = c_scale;
+    a.grid = grid;
+    a.jobs = p->jobs;
+    a.tinfo = p->tinfo;
+    return a;
+}
+
+// One persistent launch per plane group, in group order on the stream: launches of one stream
+// run one after another, so a tile's read-modify-write never races with another group's.
+template <class Tab, int kR>
 tcv_status launch(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
                   cudaStream_t st, int c_type)
 {
     const PlanGeom& g = p->g;
-    if (g.tw != kTileW || g.th != kTileH) return TCV_ERR_UNSUPPORTED;
     if (g.n == 0) return TCV_OK;
-    const void* spec = jit_tile_kernel(0, c_type, g.s);
-    const int ctas = spec ? resident_of(spec) : resident_ctas<Tab>();
+    const void* spec = jit_tile_kernel(0, c_type, g.s, kR);
+    const void* generic = reinterpret_cast<const void*>(&grid_tile_kernel<Tab, 0, kR>);
+    const void* kernel = spec ? spec : generic;
+    const int ctas = resident_of(kernel);
     const typename Tab::elem* tab = static_cast<const typename Tab::elem*>(c);
     const unsigned int* order = p->vals[p->sel];
     for (int grp = 0; grp < g.n_groups; ++grp) {
-        GridArgs a{g.support, g.s, g.g_size, g.ntx, g.ntx * g.nty, grp, c_scale};
-        if (spec) {
-            void* args[] = {&data, &tab, const_cast<const int32_t**>(&p->iu), const_cast<const int32_t**>(&p->iv),
-                            const_cast<const int32_t**>(&p->coff), &order,
-                            const_cast<uint32_t**>(&p->tile_start), const_cast<uint32_t**>(&p->tile_count),
-                            const_cast<uint32_t**>(&p->items), const_cast<uint32_t**>(&p->group_start), &grid, &a};
-            TCV_CUDA(cudaLaunchKernel(spec, dim3(ctas), dim3(kTileThreads), args, 0, st));
-        } else {
-            grid_tile_kernel<Tab, 0><<<ctas, kTileThreads, 0, st>>>(data, tab, p->iu, p->iv, p->coff, order,
-                                                                     p->tile_start, p->tile_count, p->items,
-                                                                     p->group_start, grid, a);
-            TCV_CUDA(cudaGetLastError());
-        }
+        GridArgs a = make_args(p, grp, c_scale, grid);
+        void* args[] = {&data, &tab, const_cast<const int32_t**>(&p->iu), const_cast<const int32_t**>(&p->iv),
+                        const_cast<const int32_t**>(&p->coff), &order,
+                        const_cast<uint32_t**>(&p->tile_start), const_cast<uint32_t**>(&p->tile_count),
+                        const_cast<uint32_t**>(&p->items), const_cast<uint32_t**>(&p->group_start), &a};
+        TCV_CUDA(cudaLaunchKernel(kernel, dim3(ctas), dim3(kTileThreads), args, 0, st));
     }
     return TCV_OK;
 }
 
-template <class Tab>
-int resident_degrid_ctas()
-{
-    static int per_sm = 0;
-    static int sms = 0;
-    if (!per_sm) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, degrid_tile_kernel<Tab, 0>, kTileThreads, 0);
-        if (per_sm < 1) per_sm = 1;
-    }
-    return per_sm * sms;
-}
-
-template <class Tab>
+template <class Tab, int kR>
 tcv_status launch_adjoint(const tcv_plan* p, const float2* grid, const void* c, float c_scale, float2* out,
                           cudaStream_t st, int c_type)
 {
     const PlanGeom& g = p->g;
-    if (g.tw != kTileW || g.th != kTileH) return TCV_ERR_UNSUPPORTED;
     if (g.n == 0) return TCV_OK;
-    const void* spec = jit_tile_kernel(1, c_type, g.s);
-    const int ctas = spec ? resident_of(spec) : resident_degrid_ctas<Tab>();
+    const void* spec = jit_tile_kernel(1, c_type, g.s, kR);
+    const void* generic = reinterpret_cast<const void*>(&degrid_tile_kernel<Tab, 0, kR>);
+    const void* kernel = spec ? spec : generic;
+    const int ctas = resident_of(kernel);
     const typename Tab::elem* tab = static_cast<const typename Tab::elem*>(c);
     const unsigned int* order = p->vals[p->sel];
     int max_tiles = g.max_tiles;
+    float2* gridp = const_cast<float2*>(grid);
     for (int grp = 0; grp < g.n_groups; ++grp) {
-        GridArgs a{g.support, g.s, g.g_size, g.ntx, g.ntx * g.nty, grp, c_scale};
-        if (spec) {
-            void* args[] = {&grid, &tab, const_cast<const int32_t**>(&p->iu), const_cast<const int32_t**>(&p->iv),
-                            const_cast<const int32_t**>(&p->coff), &order,
-                            const_cast<uint32_t**>(&p->tile_start), const_cast<uint32_t**>(&p->tile_count),
-                            const_cast<uint32_t**>(&p->items), const_cast<uint32_t**>(&p->group_start),
-                            const_cast<float2**>(&p->slots), &max_tiles, &a};
-            TCV_CUDA(cudaLaunchKernel(spec, dim3(ctas), dim3(kTileThreads), args, 0, st));
-        } else {
-            degrid_tile_kernel<Tab, 0><<<ctas, kTileThreads, 0, st>>>(grid, tab, p->iu, p->iv, p->coff, order,
-                                                                       p->tile_start, p->tile_count, p->items,
-                                                                       p->group_start, p->slots, max_tiles, a);
-            TCV_CUDA(cudaGetLastError());
-        }
+        GridArgs a = make_args(p, grp, c_scale, gridp);
+        void* args[] = {&tab, const_cast<const int32_t**>(&p->iu), const_cast<const int32_t**>(&p->iv),
+                        const_cast<const int32_t**>(&p->coff), &order,
+                        const_cast<uint32_t**>(&p->tile_start), const_cast<uint32_t**>(&p->tile_count),
+                        const_cast<uint32_t**>(&p->items), const_cast<uint32_t**>(&p->group_start),
+                        const_cast<float2**>(&p->slots), &max_tiles, &a};
+        TCV_CUDA(cudaLaunchKernel(kernel, dim3(ctas), dim3(kTileThreads), args, 0, st));
     }
     return slot_reduce(p, c_scale, out, st);
+}
+
+template <class Tab>
+tcv_status grid_rows(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
+                     cudaStream_t st, int c_type)
+{
+    switch (p->g.rows) {
+        case 8: return launch<Tab, 8>(p, data, c, c_scale, grid, st, c_type);
+        case 16: return launch<Tab, 16>(p, data, c, c_scale, grid, st, c_type);
+        case 32: return launch<Tab, 32>(p, data, c, c_scale, grid, st, c_type);
+        default: return TCV_ERR_UNSUPPORTED;
+    }
+}
+
+template <class Tab>
+tcv_status degrid_rows(const tcv_plan* p, const float2* grid, const void* c, float c_scale, float2* out,
+                       cudaStream_t st, int c_type)
+{
+    switch (p->g.rows) {
+        case 8: return launch_adjoint<Tab, 8>(p, grid, c, c_scale, out, st, c_type);
+        case 16: return launch_adjoint<Tab, 16>(p, grid, c, c_scale, out, st, c_type);
+        case 32: return launch_adjoint<Tab, 32>(p, grid, c, c_scale, out, st, c_type);
+        default: return TCV_ERR_UNSUPPORTED;
+    }
 }
 
 }  // namespace
@@ -116,12 +115,12 @@ tcv_status launch_degrid_tiles(const tcv_plan* p, const float2* grid, const void
                                float c_scale, float2* out, cudaStream_t st)
 {
     switch (c_type) {
-        case TCV_C_C64: return launch_adjoint<TabC64>(p, grid, c, c_scale, out, st, c_type);
-        case TCV_C_R32: return launch_adjoint<TabR32>(p, grid, c, c_scale, out, st, c_type);
-        case TCV_C_CBF16: return launch_adjoint<TabCBF16>(p, grid, c, c_scale, out, st, c_type);
-        case TCV_C_RBF16: return launch_adjoint<TabRBF16>(p, grid, c, c_scale, out, st, c_type);
-        case TCV_C_CF16: return launch_adjoint<TabCF16>(p, grid, c, c_scale, out, st, c_type);
-        case TCV_C_RF16: return launch_adjoint<TabRF16>(p, grid, c, c_scale, out, st, c_type);
+        case TCV_C_C64: return degrid_rows<TabC64>(p, grid, c, c_scale, out, st, c_type);
+        case TCV_C_R32: return degrid_rows<TabR32>(p, grid, c, c_scale, out, st, c_type);
+        case TCV_C_CBF16: return degrid_rows<TabCBF16>(p, grid, c, c_scale, out, st, c_type);
+        case TCV_C_RBF16: return degrid_rows<TabRBF16>(p, grid, c, c_scale, out, st, c_type);
+        case TCV_C_CF16: return degrid_rows<TabCF16>(p, grid, c, c_scale, out, st, c_type);
+        case TCV_C_RF16: return degrid_rows<TabRF16>(p, grid, c, c_scale, out, st, c_type);
         default: return TCV_ERR_ARG;
     }
 }
@@ -130,12 +129,12 @@ tcv_status launch_grid(const tcv_plan* p, const float2* data, const void* c, int
                        float c_scale, float2* grid, cudaStream_t st)
 {
     switch (c_type) {
-        case TCV_C_C64: return launch<TabC64>(p, data, c, c_scale, grid, st, c_type);
-        case TCV_C_R32: return launch<TabR32>(p, data, c, c_scale, grid, st, c_type);
-        case TCV_C_CBF16: return launch<TabCBF16>(p, data, c, c_scale, grid, st, c_type);
-        case TCV_C_RBF16: return launch<TabRBF16>(p, data, c, c_scale, grid, st, c_type);
-        case TCV_C_CF16: return launch<TabCF16>(p, data, c, c_scale, grid, st, c_type);
-        case TCV_C_RF16: return launch<TabRF16>(p, data, c, c_scale, grid, st, c_type);
+        case TCV_C_C64: return grid_rows<TabC64>(p, data, c, c_scale, grid, st, c_type);
+        case TCV_C_R32: return grid_rows<TabR32>(p, data, c, c_scale, grid, st, c_type);
+        case TCV_C_CBF16: return grid_rows<TabCBF16>(p, data, c, c_scale, grid, st, c_type);
+        case TCV_C_RBF16: return grid_rows<TabRBF16>(p, data, c, c_scale, grid, st, c_type);
+        case TCV_C_CF16: return grid_rows<TabCF16>(p, data, c, c_scale, grid, st, c_type);
+        case TCV_C_RF16: return grid_rows<TabRF16>(p, data, c, c_scale, grid, st, c_type);
         default: return TCV_ERR_ARG;
     }
 }

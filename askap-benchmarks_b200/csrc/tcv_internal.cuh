@@ -6,6 +6,7 @@
 #include <cuda_fp16.h>
 #include <cstdint>
 #include <cstddef>
+#include <vector>
 
 #include "tconvolve.h"
 #include "tcv_device.cuh"
@@ -30,18 +31,24 @@ struct TabRF16 {
 // Plan: binning of samples into grid tiles (gridding) and anchor tiles (degridding).
 // ------------------------------------------------------------------------------------------
 struct PlanGeom {
-    int64_t n;          // samples
+    int64_t n;          // samples (all jobs)
     int support, s;     // support, sSize = 2*support+1
-    int g_size;
+    int g_size;         // grid side of a one-job plan; the largest job's side in a batch
     int64_t c_len;      // table entries
     int kid_bits;       // bits of the kernel index cOffset / sSize^2
     // kernels are processed in groups of kid_group consecutive indices (whole w-planes), sized
     // so that one group's slice of the table stays resident in L2 while every SM works on it
-    int kid_group, n_groups, group_bits;
-    // gridding: output-stationary tiles; work cells are (group, tile)
-    int tw, th, ntx, nty, max_tiles;   // max_tiles = tiles one footprint can touch
+    int kid_group, n_groups, group_bits, group_mib;
+    int n_jobs;
+    // gridding: output-stationary tiles of tw x th points (th = 4 * rows); work cells are
+    // (group, tile) with the tiles of all jobs numbered in one space
+    int rows, tw, th;
+    int ntx, nty;       // tiles per row / column of a one-job plan
+    int64_t ntiles;     // tiles of all jobs
+    int max_tiles;      // tiles one footprint can touch
     int tile_bits, key_bits;
-    // degridding: anchor tiles (footprint top-left corner), tile + halo staged in shared memory
+    // degridding anchor tiles (footprint top-left corner; one-job plans only)
+    bool anchors;
     int ta, natx, naty, atile_bits, akey_bits;
     int box_w, box_h;   // staged region (elements), box_w even
     int degrid_mode;    // 0 staged (TMA), 1 direct from global
@@ -53,13 +60,17 @@ struct PlanGeom {
 
 struct tcv_plan {
     tcv::PlanGeom g;
-    const int32_t *iu, *iv, *coff;  // the sample arrays the plan was built from (device)
+    const int32_t *iu, *iv, *coff;  // the sample arrays the plan was binned from (device)
     // device arrays inside the caller's workspace
+    tcv::JobDesc* jobs;            // job table, n_jobs
+    uint32_t* job_start;           // n_jobs + 1: first sample of each job
+    uint32_t* tinfo;               // per tile of all jobs: tile_record(job, column, row)
+    uint16_t* ntl;                 // per sample: tiles its footprint touches (0 = left out)
     void* keys[2];                 // grid pair keys (double buffer), n * max_tiles
     uint32_t* vals[2];             // grid pair sample indices
     void* akeys[2];                // anchor keys, n
     uint32_t* avals[2];            // anchor sample indices
-    uint32_t* tile_count;          // samples per cell (group, tile): n_groups * ntx * nty
+    uint32_t* tile_count;          // samples per cell (group, tile): n_groups * ntiles
     uint32_t* tile_start;          // first sorted pair of each cell
     uint32_t* items;               // non-empty gridding cells, group-major
     uint32_t* n_items;             // [0] = number of non-empty gridding cells
@@ -70,21 +81,29 @@ struct tcv_plan {
     uint32_t* n_aitems;
     unsigned long long* rejected;  // samples left out as out of bounds
     unsigned int* status;          // device status word: bit 0 = a bounded wait timed out
-    float2* slots;                 // degridding partial sums, n * max_tiles (pipeline kernels)
+    float2* slots;                 // degridding partial sums, n * max_tiles
     void* cub_temp;
     size_t cub_bytes;
     int sel;                       // which buffer holds the sorted grid pairs
     int asel;                      // which buffer holds the sorted anchor pairs
     int degrid_variant;            // TCV_DEGRID_TILES or TCV_DEGRID_ANCHOR (reference-layout tables)
+    bool batch;                    // jobs carry their own grids (tcv_batch_plan_create)
+    bool binned;
+    std::vector<tcv::JobDesc> host_jobs;  // the job table (kept alive for its asynchronous copy)
+    std::vector<uint32_t> host_job_start;
 };
 
 namespace tcv {
 
-// Host helpers implemented in tcv_plan.cu / tcv_api.cu
-PlanGeom make_geom(int64_t n, int support, int g_size, int64_t c_len);
+// Host helpers implemented in tcv_plan.cu
+// Geometry for jobs of the given grid sides (n samples in all); tuning may be nullptr.
+PlanGeom make_geom(int64_t n, int support, const int* g_sizes, int n_jobs, int64_t c_len, const tcv_tuning* t);
 size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out);
+// one-job plan in d_work, binned (tcv_plan_build)
 tcv_status plan_init(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff, int64_t n,
-                     int support, int g_size, int64_t c_len, void* d_work, size_t work_bytes, cudaStream_t st);
+                     int support, int g_size, int64_t c_len, void* d_work, size_t work_bytes, cudaStream_t st,
+                     const tcv_tuning* t = nullptr);
+tcv_status plan_bin(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff, cudaStream_t st);
 
 // Launchers implemented in tcv_grid.cu / tcv_degrid.cu
 tcv_status launch_grid(const tcv_plan* p, const float2* data, const void* c, int c_type,
@@ -94,7 +113,10 @@ tcv_status launch_degrid(const tcv_plan* p, const float2* grid, const void* c, i
 
 // tile kernels specialised on the footprint width (tcv_jit.cu): kind 0 gridding, 1 degridding;
 // nullptr when no specialised copy is available (the generic copy is used)
-const void* jit_tile_kernel(int kind, int c_type, int s);
+// rows: grid rows per warp (the tile shape)
+const void* jit_tile_kernel(int kind, int c_type, int s, int rows);
+// build both specialised tile kernels of (form, sSize, rows) ahead of a capture or a timing
+void jit_prepare(int c_type, int s, int rows);
 
 // degridding on the gridding plan (tcv_grid.cu), and the per-sample slot sum it ends with
 tcv_status launch_degrid_tiles(const tcv_plan* p, const float2* grid, const void* c, int c_type,

@@ -46,8 +46,8 @@ NvrtcApi g_api;
 bool g_api_tried = false;
 bool g_enabled = true;
 std::string g_info = "no specialised kernel built yet";
-std::map<std::tuple<int, int, int>, cudaKernel_t> g_cache;  // (kind, c_type, sSize) -> kernel
-std::map<std::tuple<int, int, int>, bool> g_failed;
+std::map<std::tuple<int, int, int, int>, cudaKernel_t> g_cache;  // (kind, c_type, sSize, rows) -> kernel
+std::map<std::tuple<int, int, int, int>, bool> g_failed;
 
 bool load_api()
 {
@@ -89,19 +89,19 @@ const char* tab_name(int c_type)
 }
 
 // Build (or fetch) the specialised kernel; nullptr if unavailable.  Caller holds g_mu.
-cudaKernel_t build(int kind, int c_type, int s)
+cudaKernel_t build(int kind, int c_type, int s, int rows)
 {
-    const auto key = std::make_tuple(kind, c_type, s);
+    const auto key = std::make_tuple(kind, c_type, s, rows);
     auto it = g_cache.find(key);
     if (it != g_cache.end()) return it->second;
     if (g_failed.count(key)) return nullptr;
     const char* tab = tab_name(c_type);
-    if (!tab || s < 1 || s > 4096 || !load_api()) {
+    if (!tab || s < 1 || s > 4096 || (rows != 8 && rows != 16 && rows != 32) || !load_api()) {
         g_failed[key] = true;
         return nullptr;
     }
     const std::string expr = std::string(kind == 0 ? "tcv::grid_tile_kernel<" : "tcv::degrid_tile_kernel<") + tab +
-                             ", " + std::to_string(s) + ">";
+                             ", " + std::to_string(s) + ", " + std::to_string(rows) + ">";
     const std::string body = "#include \"tcv_device.cuh\"\n";
     const char* hdr_src[] = {kDeviceSrc};
     const char* hdr_name[] = {"tcv_device.cuh"};
@@ -125,7 +125,8 @@ cudaKernel_t build(int kind, int c_type, int s)
             cudaLibrary_t lib = nullptr;
             if (cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) == cudaSuccess &&
                 cudaLibraryGetKernel(&k, lib, lowered) == cudaSuccess) {
-                g_info = "specialised tile kernels in use (NVRTC, sSize " + std::to_string(s) + ")";
+                g_info = "specialised tile kernels in use (NVRTC, sSize " + std::to_string(s) + ", " +
+                         std::to_string(rows) + " rows per warp)";
             } else {
                 k = nullptr;
                 cudaGetLastError();
@@ -149,11 +150,19 @@ cudaKernel_t build(int kind, int c_type, int s)
 
 }  // namespace
 
-const void* jit_tile_kernel(int kind, int c_type, int s)
+const void* jit_tile_kernel(int kind, int c_type, int s, int rows)
 {
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_enabled) return nullptr;
-    return reinterpret_cast<const void*>(build(kind, c_type, s));
+    return reinterpret_cast<const void*>(build(kind, c_type, s, rows));
+}
+
+void jit_prepare(int c_type, int s, int rows)
+{
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_enabled) return;
+    build(0, c_type & 0xff, s, rows);
+    build(1, c_type & 0xff, s, rows);
 }
 
 }  // namespace tcv
@@ -168,8 +177,8 @@ tcv_status tcv_jit_prepare(int c_type, int support)
     const int s = 2 * support + 1;
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_enabled) return TCV_OK;
-    build(0, c_type & 0xff, s);
-    build(1, c_type & 0xff, s);
+    build(0, c_type & 0xff, s, 16);
+    build(1, c_type & 0xff, s, 16);
     return TCV_OK;
 }
 

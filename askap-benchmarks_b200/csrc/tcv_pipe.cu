@@ -407,24 +407,17 @@ pipe_kernel(const __grid_constant__ CUtensorMap cmap, const float2* __restrict__
 }
 
 // out[k] = c_scale x the sum of the sample's tile slots in tile order (0 for rejected samples).
-__global__ void slot_reduce_kernel(const float2* __restrict__ slots, const int32_t* __restrict__ iu,
-                                   const int32_t* __restrict__ iv, const int32_t* __restrict__ coff,
-                                   int64_t n, int support, int s, int g_size, int64_t c_len,
+__global__ void slot_reduce_kernel(const float2* __restrict__ slots, const uint16_t* __restrict__ ntl, int64_t n,
                                    int max_tiles, float c_scale, float2* __restrict__ out)
 {
     const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const int64_t fx = (int64_t)iu[k] - support, fy = iv[k], co = coff[k];
-    const bool ok = fx >= 0 && fx + s <= g_size && fy >= 0 && fy + s <= g_size && co >= 0 &&
-                    co + int64_t(s) * s <= c_len;
+    const int nt = ntl[k];  // tiles of the sample's footprint, in the plan's order; 0 = left out
     float2 v = make_float2(0.f, 0.f);
-    if (ok) {
-        const int nt = int((fx + s - 1) / kTileW - fx / kTileW + 1) * int((fy + s - 1) / kTileH - fy / kTileH + 1);
-        const float2* sl = slots + k * max_tiles;
-        for (int t = 0; t < nt; ++t) {
-            v.x += sl[t].x;
-            v.y += sl[t].y;
-        }
+    const float2* sl = slots + k * max_tiles;
+    for (int t = 0; t < nt; ++t) {
+        v.x += sl[t].x;
+        v.y += sl[t].y;
     }
     out[k] = make_float2(v.x * c_scale, v.y * c_scale);
 }
@@ -551,8 +544,7 @@ tcv_status slot_reduce(const tcv_plan* p, float c_scale, float2* out, cudaStream
 {
     const PlanGeom& g = p->g;
     if (g.n == 0) return TCV_OK;
-    slot_reduce_kernel<<<unsigned((g.n + 255) / 256), 256, 0, st>>>(p->slots, p->iu, p->iv, p->coff, g.n, g.support,
-                                                                     g.s, g.g_size, g.c_len, g.max_tiles, c_scale, out);
+    slot_reduce_kernel<<<unsigned((g.n + 255) / 256), 256, 0, st>>>(p->slots, p->ntl, g.n, g.max_tiles, c_scale, out);
     TCV_CUDA(cudaGetLastError());
     return TCV_OK;
 }

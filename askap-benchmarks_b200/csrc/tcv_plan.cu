@@ -6,14 +6,16 @@
 //   gridding  : every output tile of tw x th points gets the list of samples whose footprint
 //               overlaps it (a footprint of sSize^2 touches up to max_tiles tiles);
 //   degridding: every anchor tile of ta x ta gets the samples whose footprint's top-left corner
-//               lies in it (each sample exactly once).
+//               lies in it (each sample exactly once; one-job plans only).
 // Kernel indices kid = cOffset / sSize^2 (w-plane major, then the oversampling offsets) are
 // grouped into runs of whole w-planes whose slice of the table fits in L2 with room to spare.
 // The sort key is the work cell (group, tile), ordered group-major, so all SMs work through the
 // table one group at a time and the slice in use stays resident in L2; within a cell the stable
 // sort keeps samples in index order (the reference's order).  The non-empty cells are compacted
 // into work lists (with per-group ranges) that persistent kernels walk.
-// Samples whose footprint or table range falls outside the grid or the table are counted and
+// A plan may hold several jobs sharing the table (a batch): their tiles are numbered in one
+// space, job after job, so one sort and one sequence of launches covers all of them.
+// Samples whose footprint or table range falls outside their grid or the table are counted and
 // left out (sentinel key, sorted past the end).
 #include "tcv_internal.cuh"
 
@@ -39,55 +41,105 @@ int bits_for(uint64_t v)  // bits needed to represent values 0..v
     return b < 1 ? 1 : b;
 }
 
+// job of sample d: the last job whose first sample is <= d (empty jobs share their start with
+// the next job, which is then the one holding d)
+__device__ __forceinline__ int job_of(const uint32_t* __restrict__ job_start, int n_jobs, uint32_t d)
+{
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (job_start[mid] <= d)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
 template <typename K>
 __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* __restrict__ iv,
-                                 const int32_t* __restrict__ coff, PlanGeom g, K* keys,
-                                 uint32_t* vals, K* akeys, uint32_t* avals, uint32_t* tile_count,
-                                 uint32_t* atile_count, unsigned long long* rejected)
+                                 const int32_t* __restrict__ coff, PlanGeom g, const JobDesc* __restrict__ jobs,
+                                 const uint32_t* __restrict__ job_start, K* keys, uint32_t* vals, K* akeys,
+                                 uint32_t* avals, uint32_t* tile_count, uint32_t* atile_count, uint16_t* ntl,
+                                 unsigned long long* rejected)
 {
     const int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (d >= g.n) return;
+    const int job = g.n_jobs > 1 ? job_of(job_start, g.n_jobs, uint32_t(d)) : 0;
+    const JobDesc jd = jobs[job];
     const int64_t fx = (int64_t)iu[d] - g.support;
     const int64_t fy = iv[d];
     const int64_t co = coff[d];
     const int64_t s = g.s;
-    const bool ok = fx >= 0 && fx + s <= g.g_size && fy >= 0 && fy + s <= g.g_size && co >= 0 &&
+    const bool ok = fx >= 0 && fx + s <= jd.g_size && fy >= 0 && fy + s <= jd.g_size && co >= 0 &&
                     co + s * s <= g.c_len;
     K* kp = keys + d * g.max_tiles;
     uint32_t* vp = vals + d * g.max_tiles;
     const K sentinel = K(1) << (g.key_bits - 1);
-    const K asentinel = K(1) << (g.akey_bits - 1);
     if (!ok) {
         atomicAdd(rejected, 1ull);
         for (int t = 0; t < g.max_tiles; ++t) {
             kp[t] = sentinel;
             vp[t] = uint32_t(d);
         }
-        akeys[d] = asentinel;
-        avals[d] = uint32_t(d);
+        ntl[d] = 0;
+        if (g.anchors) {
+            akeys[d] = K(1) << (g.akey_bits - 1);
+            avals[d] = uint32_t(d);
+        }
         return;
     }
     const uint32_t grp = uint32_t(co / (s * s) / g.kid_group);
-    const uint32_t cell0 = grp * uint32_t(g.ntx * g.nty);
+    const uint32_t cell0 = grp * uint32_t(g.ntiles) + jd.tile_base;
     const int tx0 = int(fx / g.tw), tx1 = int((fx + s - 1) / g.tw);
     const int ty0 = int(fy / g.th), ty1 = int((fy + s - 1) / g.th);
     int t = 0;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
-            const uint32_t cell = cell0 + uint32_t(ty) * g.ntx + tx;
+            const uint32_t cell = cell0 + uint32_t(ty) * uint32_t(jd.ntx) + uint32_t(tx);
             kp[t] = K(cell);
             vp[t] = uint32_t(d);
             atomicAdd(&tile_count[cell], 1u);
             ++t;
         }
+    ntl[d] = uint16_t(t);
     for (; t < g.max_tiles; ++t) {
         kp[t] = sentinel;
         vp[t] = uint32_t(d);
     }
-    const uint32_t at = grp * uint32_t(g.natx * g.naty) + uint32_t(fy / g.ta) * g.natx + uint32_t(fx / g.ta);
-    akeys[d] = K(at);
-    avals[d] = uint32_t(d);
-    atomicAdd(&atile_count[at], 1u);
+    if (g.anchors) {
+        const uint32_t at = grp * uint32_t(g.natx * g.naty) + uint32_t(fy / g.ta) * g.natx + uint32_t(fx / g.ta);
+        akeys[d] = K(at);
+        avals[d] = uint32_t(d);
+        atomicAdd(&atile_count[at], 1u);
+    }
+}
+
+// the job table of a one-job plan (written on the device, so building such a plan is device
+// work only)
+__global__ void one_job_kernel(JobDesc* jobs, uint32_t* job_start, int g_size, int ntx, uint32_t ntiles, uint32_t n)
+{
+    jobs[0] = JobDesc{nullptr, g_size, ntx, 0u, ntiles};
+    job_start[0] = 0;
+    job_start[1] = n;
+}
+
+// per tile of all jobs: its record (job, column, row)
+__global__ void tile_info_kernel(const JobDesc* __restrict__ jobs, int n_jobs, uint32_t ntiles, uint32_t* tinfo)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].tile_base <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const uint32_t local = t - jobs[lo].tile_base;
+    const uint32_t ntx = uint32_t(jobs[lo].ntx);
+    tinfo[t] = tile_record(uint32_t(lo), local % ntx, local / ntx);
 }
 
 struct NonZero {
@@ -114,197 +166,117 @@ __global__ void group_ranges_kernel(const uint32_t* items, const uint32_t* n_ite
 
 inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
+inline size_t grid_cells(const PlanGeom& g) { return size_t(g.n_groups) * size_t(g.ntiles); }
+inline size_t anchor_cells(const PlanGeom& g) { return g.anchors ? size_t(g.n_groups) * g.natx * g.naty : 0; }
+
 template <typename K>
 size_t cub_temp_bytes(const PlanGeom& g)
 {
     size_t a = 0, b = 0, c = 0, d = 0, e = 0, f = 0;
     const int64_t np = g.n * g.max_tiles;
-    const int cells = g.n_groups * g.ntx * g.nty, acells = g.n_groups * g.natx * g.naty;
+    const int cells = int(grid_cells(g)), acells = int(anchor_cells(g));
     cub::DoubleBuffer<K> kb(nullptr, nullptr);
     cub::DoubleBuffer<uint32_t> vb(nullptr, nullptr);
-    cub::DeviceRadixSort::SortPairs(nullptr, a, kb, vb, np, 0, g.key_bits);
-    cub::DeviceRadixSort::SortPairs(nullptr, b, kb, vb, g.n, 0, g.akey_bits);
-    cub::DeviceScan::ExclusiveSum(nullptr, c, (uint32_t*)nullptr, (uint32_t*)nullptr, cells);
-    cub::DeviceScan::ExclusiveSum(nullptr, d, (uint32_t*)nullptr, (uint32_t*)nullptr, acells);
     thrust::counting_iterator<uint32_t> it(0);
     thrust::transform_iterator<NonZero, const uint32_t*> fl((const uint32_t*)nullptr, NonZero());
+    cub::DeviceRadixSort::SortPairs(nullptr, a, kb, vb, np, 0, g.key_bits);
+    cub::DeviceScan::ExclusiveSum(nullptr, c, (uint32_t*)nullptr, (uint32_t*)nullptr, cells);
     cub::DeviceSelect::Flagged(nullptr, e, it, fl, (uint32_t*)nullptr, (uint32_t*)nullptr, cells);
-    cub::DeviceSelect::Flagged(nullptr, f, it, fl, (uint32_t*)nullptr, (uint32_t*)nullptr, acells);
+    if (g.anchors) {
+        cub::DeviceRadixSort::SortPairs(nullptr, b, kb, vb, g.n, 0, g.akey_bits);
+        cub::DeviceScan::ExclusiveSum(nullptr, d, (uint32_t*)nullptr, (uint32_t*)nullptr, acells);
+        cub::DeviceSelect::Flagged(nullptr, f, it, fl, (uint32_t*)nullptr, (uint32_t*)nullptr, acells);
+    }
     return std::max(std::max(std::max(a, b), std::max(c, d)), std::max(e, f));
 }
 
 template <typename K>
-tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_t* coff,
-                 cudaStream_t st)
+tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_t* coff, cudaStream_t st)
 {
     const PlanGeom& g = p->g;
     const int64_t np = g.n * g.max_tiles;
-    const int cells = g.n_groups * g.ntx * g.nty, acells = g.n_groups * g.natx * g.naty;
+    const int cells = int(grid_cells(g)), acells = int(anchor_cells(g));
     TCV_CUDA(cudaMemsetAsync(p->tile_count, 0, sizeof(uint32_t) * size_t(cells), st));
-    TCV_CUDA(cudaMemsetAsync(p->atile_count, 0, sizeof(uint32_t) * size_t(acells), st));
+    if (g.anchors) TCV_CUDA(cudaMemsetAsync(p->atile_count, 0, sizeof(uint32_t) * size_t(acells), st));
     TCV_CUDA(cudaMemsetAsync(p->rejected, 0, sizeof(unsigned long long), st));
     TCV_CUDA(cudaMemsetAsync(p->status, 0, sizeof(unsigned int), st));
     if (g.n > 0) {
         plan_keys_kernel<K><<<unsigned((g.n + 255) / 256), 256, 0, st>>>(
-            iu, iv, coff, g, static_cast<K*>(p->keys[0]), p->vals[0], static_cast<K*>(p->akeys[0]),
-            p->avals[0], p->tile_count, p->atile_count, p->rejected);
+            iu, iv, coff, g, p->jobs, p->job_start, static_cast<K*>(p->keys[0]), p->vals[0],
+            static_cast<K*>(p->akeys[0]), p->avals[0], p->tile_count, p->atile_count, p->ntl, p->rejected);
         TCV_CUDA(cudaGetLastError());
         cub::DoubleBuffer<K> kb(static_cast<K*>(p->keys[0]), static_cast<K*>(p->keys[1]));
         cub::DoubleBuffer<uint32_t> vb(p->vals[0], p->vals[1]);
         size_t tb = p->cub_bytes;
         TCV_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_temp, tb, kb, vb, np, 0, g.key_bits, st));
         p->sel = vb.selector;
-        cub::DoubleBuffer<K> akb(static_cast<K*>(p->akeys[0]), static_cast<K*>(p->akeys[1]));
-        cub::DoubleBuffer<uint32_t> avb(p->avals[0], p->avals[1]);
-        tb = p->cub_bytes;
-        TCV_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_temp, tb, akb, avb, g.n, 0, g.akey_bits, st));
-        p->asel = avb.selector;
+        if (g.anchors) {
+            cub::DoubleBuffer<K> akb(static_cast<K*>(p->akeys[0]), static_cast<K*>(p->akeys[1]));
+            cub::DoubleBuffer<uint32_t> avb(p->avals[0], p->avals[1]);
+            tb = p->cub_bytes;
+            TCV_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_temp, tb, akb, avb, g.n, 0, g.akey_bits, st));
+            p->asel = avb.selector;
+        }
     } else {
         p->sel = 0;
         p->asel = 0;
     }
+    thrust::counting_iterator<uint32_t> it(0);
     size_t tb = p->cub_bytes;
     TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->tile_count, p->tile_start, cells, st));
-    tb = p->cub_bytes;
-    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->atile_count, p->atile_start, acells, st));
-    thrust::counting_iterator<uint32_t> it(0);
     thrust::transform_iterator<NonZero, const uint32_t*> fl(p->tile_count, NonZero());
     tb = p->cub_bytes;
     TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, fl, p->items, p->n_items, cells, st));
-    thrust::transform_iterator<NonZero, const uint32_t*> afl(p->atile_count, NonZero());
-    tb = p->cub_bytes;
-    TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, afl, p->aitems, p->n_aitems, acells, st));
+    if (g.anchors) {
+        tb = p->cub_bytes;
+        TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->atile_count, p->atile_start, acells, st));
+        thrust::transform_iterator<NonZero, const uint32_t*> afl(p->atile_count, NonZero());
+        tb = p->cub_bytes;
+        TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, afl, p->aitems, p->n_aitems, acells, st));
+    }
     group_ranges_kernel<<<(g.n_groups + 1 + 127) / 128, 128, 0, st>>>(p->items, p->n_items, g.n_groups,
-                                                                       uint32_t(g.ntx * g.nty), p->group_start);
+                                                                       uint32_t(g.ntiles), p->group_start);
     TCV_CUDA(cudaGetLastError());
     return TCV_OK;
 }
 
-}  // namespace
-
-// Tile geometry.  Gridding tiles are 64 x 64 points (8 warps of 32 columns x 16 rows).
-// Degridding anchor tiles are the largest ta whose staged region (ta + sSize - 1)^2 complex
-// points fits in shared memory next to the partial sums; beyond that the direct kernel reads
-// the grid from global memory.
-PlanGeom make_geom(int64_t n, int support, int g_size, int64_t c_len)
+bool valid_tuning(const tcv_tuning* t)
 {
-    PlanGeom g{};
-    g.n = n;
-    g.support = support;
-    g.s = 2 * support + 1;
-    g.g_size = g_size;
-    g.c_len = c_len;
-    const int64_t s2 = int64_t(g.s) * g.s;
-    const int64_t nk = (c_len + s2 - 1) / s2;
-    g.kid_bits = bits_for(uint64_t(nk));
-    // kernels per group: whole planes of 64 (8 x 8 oversampling) whose complex64 slice is about
-    // 32 MiB, a quarter of the 126 MB L2
-    const int64_t per_kernel = s2 * 8;
-    int64_t kg = ((int64_t(32) << 20) / per_kernel) / 64 * 64;
-    if (kg < 64) kg = 64;
-    if (kg > nk) kg = nk < 1 ? 1 : nk;
-    g.kid_group = int(kg);
-    g.n_groups = int((nk + kg - 1) / kg);
-    if (g.n_groups < 1) g.n_groups = 1;
-    g.group_bits = bits_for(uint64_t(g.n_groups - 1));
-    g.tw = 64;
-    g.th = 64;
-    g.ntx = (g_size + g.tw - 1) / g.tw;
-    g.nty = (g_size + g.th - 1) / g.th;
-    g.max_tiles = ((g.s + g.tw - 2) / g.tw + 1) * ((g.s + g.th - 2) / g.th + 1);
-    g.tile_bits = bits_for(uint64_t(g.n_groups) * g.ntx * g.nty - 1);
-    g.key_bits = g.tile_bits + 1;  // cell, plus the sentinel bit
-
-    constexpr size_t kSmemBudget = 220 * 1024;  // of 227 KB per CTA; the rest holds partial sums
-    const int cand[] = {128, 96, 64, 48, 32, 16, 8};
-    g.degrid_mode = 1;
-    g.ta = 32;
-    for (int ta : cand) {
-        const int w = ((ta + g.s - 1) + 1) & ~1;
-        const int h = ta + g.s - 1;
-        if (w <= 256 && h <= 256 && size_t(w) * h * 8 <= kSmemBudget && ta <= g_size) {
-            g.ta = ta;
-            g.box_w = w;
-            g.box_h = h;
-            g.degrid_mode = (g_size % 2 == 0) ? 0 : 1;  // TMA row stride must be a multiple of 16 B
-            break;
-        }
-    }
-    g.natx = (g_size + g.ta - 1) / g.ta;
-    g.naty = (g_size + g.ta - 1) / g.ta;
-    g.atile_bits = bits_for(uint64_t(g.n_groups) * g.natx * g.naty - 1);
-    g.akey_bits = g.atile_bits + 1;
-    g.key64 = g.key_bits > 32 || g.akey_bits > 32;
-    g.degrid_parts = 4;
-    return g;
+    if (!t) return true;
+    const bool rows_ok = t->tile_rows == 0 || t->tile_rows == 8 || t->tile_rows == 16 || t->tile_rows == 32;
+    return rows_ok && t->group_mib >= -1;
 }
 
-size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out)
+// Lay the plan's arrays out in d_work and write the job table: from host memory for a batch,
+// by a one-thread kernel for a one-job plan (so that plan_init is device work only).
+tcv_status plan_create(tcv_plan* p, void* d_work, size_t work_bytes, cudaStream_t st)
 {
-    const size_t ks = g.key64 ? 8 : 4;
-    const size_t np = size_t(g.n) * g.max_tiles;
-    const size_t cb = g.key64 ? cub_temp_bytes<uint64_t>(g) : cub_temp_bytes<uint32_t>(g);
-    if (cub_bytes_out) *cub_bytes_out = cb;
-    size_t b = 0;
-    b += 2 * align_up(np * ks) + 2 * align_up(np * 4);
-    b += 2 * align_up(size_t(g.n) * ks) + 2 * align_up(size_t(g.n) * 4);
-    const size_t cells = size_t(g.n_groups) * g.ntx * g.nty, acells = size_t(g.n_groups) * g.natx * g.naty;
-    b += 3 * align_up(cells * 4) + align_up(4) + align_up(size_t(g.n_groups + 1) * 4);
-    b += 3 * align_up(acells * 4) + align_up(4);
-    b += align_up(sizeof(unsigned long long)) + align_up(sizeof(unsigned int));
-    b += align_up(np * sizeof(float2));
-    b += align_up(cb);
-    return b;
-}
-
-}  // namespace tcv
-
-using namespace tcv;
-
-extern "C" {
-
-size_t tcv_plan_workspace_bytes(int64_t n, int support, int g_size, int64_t c_len)
-{
-    if (n < 0 || support < 0 || g_size < 1 || c_len < 1) return 0;
-    PlanGeom g = make_geom(n, support, g_size, c_len);
-    return plan_bytes(g, nullptr);
-}
-
-}  // extern "C"
-
-namespace tcv {
-
-// Fill *p (a caller-owned object) with a plan built in d_work.
-tcv_status plan_init(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff, int64_t n,
-                     int support, int g_size, int64_t c_len, void* d_work, size_t work_bytes, cudaStream_t st)
-{
-    if (!p || n < 0 || support < 0 || g_size < 1 || c_len < 1) return TCV_ERR_ARG;
-    if (n > 0 && (!d_iu || !d_iv || !d_coff)) return TCV_ERR_ARG;
-    if (n >= (int64_t(1) << 32) / 16) return TCV_ERR_UNSUPPORTED;  // 32-bit sample indices
-    if (!d_work) return TCV_ERR_ARG;
-    *p = tcv_plan{};
-    p->g = make_geom(n, support, g_size, c_len);
-    size_t cb = 0;
-    const size_t need = plan_bytes(p->g, &cb);
-    if (work_bytes < need) return TCV_ERR_WORKSPACE;
     const PlanGeom& g = p->g;
+    size_t cb = 0;
+    const size_t need = plan_bytes(g, &cb);
+    if (work_bytes < need) return TCV_ERR_WORKSPACE;
     const size_t ks = g.key64 ? 8 : 4;
     const size_t np = size_t(g.n) * g.max_tiles;
+    const size_t an = g.anchors ? size_t(g.n) : 0;
     char* w = static_cast<char*>(d_work);
     auto take = [&](size_t bytes) {
         char* r = w;
         w += align_up(bytes);
         return static_cast<void*>(r);
     };
+    p->jobs = static_cast<JobDesc*>(take(size_t(g.n_jobs) * sizeof(JobDesc)));
+    p->job_start = static_cast<uint32_t*>(take(size_t(g.n_jobs + 1) * 4));
+    p->tinfo = static_cast<uint32_t*>(take(size_t(g.ntiles) * 4));
+    p->ntl = static_cast<uint16_t*>(take(size_t(g.n) * 2));
     p->keys[0] = take(np * ks);
     p->keys[1] = take(np * ks);
     p->vals[0] = static_cast<uint32_t*>(take(np * 4));
     p->vals[1] = static_cast<uint32_t*>(take(np * 4));
-    p->akeys[0] = take(size_t(g.n) * ks);
-    p->akeys[1] = take(size_t(g.n) * ks);
-    p->avals[0] = static_cast<uint32_t*>(take(size_t(g.n) * 4));
-    p->avals[1] = static_cast<uint32_t*>(take(size_t(g.n) * 4));
-    const size_t cells = size_t(g.n_groups) * g.ntx * g.nty, acells = size_t(g.n_groups) * g.natx * g.naty;
+    p->akeys[0] = take(an * ks);
+    p->akeys[1] = take(an * ks);
+    p->avals[0] = static_cast<uint32_t*>(take(an * 4));
+    p->avals[1] = static_cast<uint32_t*>(take(an * 4));
+    const size_t cells = grid_cells(g), acells = anchor_cells(g);
     p->tile_count = static_cast<uint32_t*>(take(cells * 4));
     p->tile_start = static_cast<uint32_t*>(take(cells * 4));
     p->items = static_cast<uint32_t*>(take(cells * 4));
@@ -319,26 +291,271 @@ tcv_status plan_init(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, cons
     p->slots = static_cast<float2*>(take(np * sizeof(float2)));
     p->cub_temp = take(cb);
     p->cub_bytes = cb;
+    p->degrid_variant = TCV_DEGRID_TILES;
+    if (p->batch) {
+        TCV_CUDA(cudaMemcpyAsync(p->jobs, p->host_jobs.data(), p->host_jobs.size() * sizeof(JobDesc),
+                                 cudaMemcpyHostToDevice, st));
+        TCV_CUDA(cudaMemcpyAsync(p->job_start, p->host_job_start.data(), p->host_job_start.size() * 4,
+                                 cudaMemcpyHostToDevice, st));
+    } else {
+        one_job_kernel<<<1, 1, 0, st>>>(p->jobs, p->job_start, g.g_size, g.ntx, uint32_t(g.ntiles), uint32_t(g.n));
+        TCV_CUDA(cudaGetLastError());
+    }
+    tile_info_kernel<<<unsigned((g.ntiles + 255) / 256), 256, 0, st>>>(p->jobs, g.n_jobs, uint32_t(g.ntiles), p->tinfo);
+    TCV_CUDA(cudaGetLastError());
+    return TCV_OK;
+}
+
+// limits of the plan's index types: 32-bit sample indices in the sort (16 tile pairs per sample
+// at most within 2^32), 32-bit cells, and the fields of the tile record (jobs, tile columns and
+// rows per job; g_max is the largest grid side)
+bool geom_supported(const PlanGeom& g)
+{
+    if (g.n_jobs > kMaxJobs) return false;
+    if ((g.g_size + g.tw - 1) / g.tw > kMaxTilesPerSide || (g.g_size + g.th - 1) / g.th > kMaxTilesPerSide) return false;
+    if (g.n >= (int64_t(1) << 32) / 16) return false;
+    if (g.n * g.max_tiles >= (int64_t(1) << 31)) return false;
+    if (int64_t(g.n_groups) * g.ntiles >= (int64_t(1) << 31)) return false;
+    if (g.max_tiles > 65535) return false;
+    return true;
+}
+
+}  // namespace
+
+// Tile geometry.  Gridding tiles are 64 x 4*rows points (8 warps of 32 columns x rows rows).
+// Degridding anchor tiles are the largest ta whose staged region (ta + sSize - 1)^2 complex
+// points fits in shared memory next to the partial sums; beyond that the direct kernel reads
+// the grid from global memory.
+PlanGeom make_geom(int64_t n, int support, const int* g_sizes, int n_jobs, int64_t c_len, const tcv_tuning* t)
+{
+    PlanGeom g{};
+    g.n = n;
+    g.support = support;
+    g.s = 2 * support + 1;
+    g.c_len = c_len;
+    g.n_jobs = n_jobs;
+    g.g_size = 0;
+    for (int j = 0; j < n_jobs; ++j) g.g_size = std::max(g.g_size, g_sizes[j]);
+    const int64_t s2 = int64_t(g.s) * g.s;
+    const int64_t nk = (c_len + s2 - 1) / s2;
+    g.kid_bits = bits_for(uint64_t(nk));
+    // kernels per group: whole planes of 64 (8 x 8 oversampling) whose complex64 slice is about
+    // group_mib MiB (32 by default, a quarter of the 126 MB L2)
+    g.group_mib = (t && t->group_mib) ? t->group_mib : 32;
+    int64_t kg = nk;
+    if (g.group_mib > 0) {
+        const int64_t per_kernel = s2 * 8;
+        kg = ((int64_t(g.group_mib) << 20) / per_kernel) / 64 * 64;
+        if (kg < 64) kg = 64;
+    }
+    if (kg > nk) kg = nk < 1 ? 1 : nk;
+    g.kid_group = int(kg);
+    g.n_groups = int((nk + kg - 1) / kg);
+    if (g.n_groups < 1) g.n_groups = 1;
+    g.group_bits = bits_for(uint64_t(g.n_groups - 1));
+    g.rows = (t && t->tile_rows) ? t->tile_rows : 16;
+    g.tw = kTileW;
+    g.th = tile_height(g.rows);
+    g.ntiles = 0;
+    for (int j = 0; j < n_jobs; ++j)
+        g.ntiles += int64_t((g_sizes[j] + g.tw - 1) / g.tw) * ((g_sizes[j] + g.th - 1) / g.th);
+    g.ntx = n_jobs == 1 ? (g.g_size + g.tw - 1) / g.tw : 0;
+    g.nty = n_jobs == 1 ? (g.g_size + g.th - 1) / g.th : 0;
+    g.max_tiles = ((g.s + g.tw - 2) / g.tw + 1) * ((g.s + g.th - 2) / g.th + 1);
+    g.tile_bits = bits_for(uint64_t(g.n_groups) * uint64_t(g.ntiles) - 1);
+    g.key_bits = g.tile_bits + 1;  // cell, plus the sentinel bit
+
+    g.anchors = n_jobs == 1;
+    g.degrid_mode = 1;
+    g.ta = 32;
+    g.degrid_parts = 4;
+    if (g.anchors) {
+        constexpr size_t kSmemBudget = 220 * 1024;  // of 227 KB per CTA; the rest holds partial sums
+        const int cand[] = {128, 96, 64, 48, 32, 16, 8};
+        for (int ta : cand) {
+            const int w = ((ta + g.s - 1) + 1) & ~1;
+            const int h = ta + g.s - 1;
+            if (w <= 256 && h <= 256 && size_t(w) * h * 8 <= kSmemBudget && ta <= g.g_size) {
+                g.ta = ta;
+                g.box_w = w;
+                g.box_h = h;
+                g.degrid_mode = (g.g_size % 2 == 0) ? 0 : 1;  // TMA row stride must be a multiple of 16 B
+                break;
+            }
+        }
+        g.natx = (g.g_size + g.ta - 1) / g.ta;
+        g.naty = (g.g_size + g.ta - 1) / g.ta;
+        g.atile_bits = bits_for(uint64_t(g.n_groups) * g.natx * g.naty - 1);
+        g.akey_bits = g.atile_bits + 1;
+    }
+    g.key64 = g.key_bits > 32 || (g.anchors && g.akey_bits > 32);
+    return g;
+}
+
+size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out)
+{
+    const size_t ks = g.key64 ? 8 : 4;
+    const size_t np = size_t(g.n) * g.max_tiles;
+    const size_t an = g.anchors ? size_t(g.n) : 0;
+    const size_t cb = g.key64 ? cub_temp_bytes<uint64_t>(g) : cub_temp_bytes<uint32_t>(g);
+    if (cub_bytes_out) *cub_bytes_out = cb;
+    size_t b = 0;
+    b += align_up(size_t(g.n_jobs) * sizeof(JobDesc)) + align_up(size_t(g.n_jobs + 1) * 4);
+    b += align_up(size_t(g.ntiles) * 4) + align_up(size_t(g.n) * 2);
+    b += 2 * align_up(np * ks) + 2 * align_up(np * 4);
+    b += 2 * align_up(an * ks) + 2 * align_up(an * 4);
+    const size_t cells = grid_cells(g), acells = anchor_cells(g);
+    b += 3 * align_up(cells * 4) + align_up(4) + align_up(size_t(g.n_groups + 1) * 4);
+    b += 3 * align_up(acells * 4) + align_up(4);
+    b += align_up(sizeof(unsigned long long)) + align_up(sizeof(unsigned int));
+    b += align_up(np * sizeof(float2));
+    b += align_up(cb);
+    return b;
+}
+
+tcv_status plan_bin(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff, cudaStream_t st)
+{
+    if (!p) return TCV_ERR_ARG;
+    if (p->g.n > 0 && (!d_iu || !d_iv || !d_coff)) return TCV_ERR_ARG;
     p->iu = d_iu;
     p->iv = d_iv;
     p->coff = d_coff;
-    p->degrid_variant = TCV_DEGRID_TILES;
-    return g.key64 ? build<uint64_t>(p, d_iu, d_iv, d_coff, st) : build<uint32_t>(p, d_iu, d_iv, d_coff, st);
+    const tcv_status s = p->g.key64 ? build<uint64_t>(p, d_iu, d_iv, d_coff, st) : build<uint32_t>(p, d_iu, d_iv, d_coff, st);
+    p->binned = s == TCV_OK;
+    return s;
+}
+
+// Fill *p (a caller-owned object) with a one-job plan built in d_work.
+tcv_status plan_init(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff, int64_t n,
+                     int support, int g_size, int64_t c_len, void* d_work, size_t work_bytes, cudaStream_t st,
+                     const tcv_tuning* t)
+{
+    if (!p || n < 0 || support < 0 || g_size < 1 || c_len < 1 || !valid_tuning(t)) return TCV_ERR_ARG;
+    if (n > 0 && (!d_iu || !d_iv || !d_coff)) return TCV_ERR_ARG;
+    if (!d_work) return TCV_ERR_ARG;
+    *p = tcv_plan{};
+    p->g = make_geom(n, support, &g_size, 1, c_len, t);
+    if (!geom_supported(p->g)) return TCV_ERR_UNSUPPORTED;
+    const tcv_status s = plan_create(p, d_work, work_bytes, st);
+    if (s != TCV_OK) return s;
+    return plan_bin(p, d_iu, d_iv, d_coff, st);
 }
 
 }  // namespace tcv
 
+using namespace tcv;
+
+namespace {
+
+// checks shared by the batch entry points; fills the per-job grid sides and the sample total
+tcv_status batch_args(const tcv_job* jobs, int n_jobs, int support, int64_t c_len, const tcv_tuning* t,
+                      std::vector<int>& sides, int64_t& n_total)
+{
+    if (!jobs || n_jobs < 1 || support < 0 || c_len < 1 || !valid_tuning(t)) return TCV_ERR_ARG;
+    sides.resize(size_t(n_jobs));
+    n_total = 0;
+    for (int j = 0; j < n_jobs; ++j) {
+        if (jobs[j].n < 0 || jobs[j].g_size < 1 || !jobs[j].d_grid) return TCV_ERR_ARG;
+        sides[size_t(j)] = jobs[j].g_size;
+        n_total += jobs[j].n;
+    }
+    return TCV_OK;
+}
+
+}  // namespace
+
 extern "C" {
+
+size_t tcv_plan_workspace_bytes(int64_t n, int support, int g_size, int64_t c_len)
+{
+    if (n < 0 || support < 0 || g_size < 1 || c_len < 1) return 0;
+    PlanGeom g = make_geom(n, support, &g_size, 1, c_len, nullptr);
+    return plan_bytes(g, nullptr);
+}
+
+size_t tcv_batch_workspace_bytes(const tcv_job* jobs, int n_jobs, int support, int64_t c_len, const tcv_tuning* tuning)
+{
+    std::vector<int> sides;
+    int64_t n = 0;
+    if (batch_args(jobs, n_jobs, support, c_len, tuning, sides, n) != TCV_OK) return 0;
+    PlanGeom g = make_geom(n, support, sides.data(), n_jobs, c_len, tuning);
+    return plan_bytes(g, nullptr);
+}
+
+tcv_status tcv_batch_plan_create(tcv_plan** plan_out, const tcv_job* jobs, int n_jobs, int support, int64_t c_len,
+                                 const tcv_tuning* tuning, void* d_work, size_t work_bytes, void* stream)
+{
+    if (!plan_out || !d_work) return TCV_ERR_ARG;
+    std::vector<int> sides;
+    int64_t n = 0;
+    tcv_status s = batch_args(jobs, n_jobs, support, c_len, tuning, sides, n);
+    if (s != TCV_OK) return s;
+    tcv_plan* p = new (std::nothrow) tcv_plan{};
+    if (!p) return TCV_ERR_OOM;
+    p->g = make_geom(n, support, sides.data(), n_jobs, c_len, tuning);
+    if (!geom_supported(p->g)) {
+        delete p;
+        return TCV_ERR_UNSUPPORTED;
+    }
+    p->batch = true;
+    p->host_jobs.resize(size_t(n_jobs));
+    p->host_job_start.resize(size_t(n_jobs) + 1);
+    uint32_t tile_base = 0, first = 0;
+    for (int j = 0; j < n_jobs; ++j) {
+        const int ntx = (jobs[j].g_size + p->g.tw - 1) / p->g.tw, nty = (jobs[j].g_size + p->g.th - 1) / p->g.th;
+        p->host_jobs[size_t(j)] = JobDesc{reinterpret_cast<float2*>(jobs[j].d_grid), jobs[j].g_size, ntx, tile_base,
+                                          uint32_t(ntx) * uint32_t(nty)};
+        p->host_job_start[size_t(j)] = first;
+        tile_base += uint32_t(ntx) * uint32_t(nty);
+        first += uint32_t(jobs[j].n);
+    }
+    p->host_job_start[size_t(n_jobs)] = first;
+    s = plan_create(p, d_work, work_bytes, static_cast<cudaStream_t>(stream));
+    if (s != TCV_OK) {
+        delete p;
+        return s;
+    }
+    *plan_out = p;
+    return TCV_OK;
+}
+
+tcv_status tcv_plan_bin(tcv_plan* plan, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff, void* stream)
+{
+    return plan_bin(plan, d_iu, d_iv, d_coff, static_cast<cudaStream_t>(stream));
+}
+
+tcv_status tcv_plan_tuning(const tcv_plan* plan, tcv_tuning* tuning_out)
+{
+    if (!plan || !tuning_out) return TCV_ERR_ARG;
+    tuning_out->tile_rows = plan->g.rows;
+    tuning_out->group_mib = plan->g.group_mib;
+    return TCV_OK;
+}
+
+size_t tcv_plan_workspace_bytes_tuned(int64_t n, int support, int g_size, int64_t c_len, const tcv_tuning* tuning)
+{
+    if (n < 0 || support < 0 || g_size < 1 || c_len < 1 || !valid_tuning(tuning)) return 0;
+    PlanGeom g = make_geom(n, support, &g_size, 1, c_len, tuning);
+    return plan_bytes(g, nullptr);
+}
 
 tcv_status tcv_plan_build(tcv_plan** plan_out, const int32_t* d_iu, const int32_t* d_iv,
                           const int32_t* d_coff, int64_t n, int support, int g_size,
                           int64_t c_len, void* d_work, size_t work_bytes, void* stream)
 {
+    return tcv_plan_build_tuned(plan_out, d_iu, d_iv, d_coff, n, support, g_size, c_len, nullptr, d_work,
+                                work_bytes, stream);
+}
+
+tcv_status tcv_plan_build_tuned(tcv_plan** plan_out, const int32_t* d_iu, const int32_t* d_iv,
+                                const int32_t* d_coff, int64_t n, int support, int g_size, int64_t c_len,
+                                const tcv_tuning* tuning, void* d_work, size_t work_bytes, void* stream)
+{
     if (!plan_out) return TCV_ERR_ARG;
     tcv_plan* p = new (std::nothrow) tcv_plan{};
     if (!p) return TCV_ERR_OOM;
     const tcv_status s = plan_init(p, d_iu, d_iv, d_coff, n, support, g_size, c_len, d_work, work_bytes,
-                                   static_cast<cudaStream_t>(stream));
+                                   static_cast<cudaStream_t>(stream), tuning);
     if (s != TCV_OK) {
         delete p;
         return s;
@@ -376,7 +593,7 @@ tcv_status tcv_plan_info(const tcv_plan* plan, int* tile_w, int* tile_h, int* an
     if (tile_h) *tile_h = plan->g.th;
     if (anchor) *anchor = plan->g.ta;
     if (degrid_mode) *degrid_mode = plan->g.degrid_mode;
-    if (n_tiles) *n_tiles = plan->g.ntx * plan->g.nty * plan->g.n_groups;
+    if (n_tiles) *n_tiles = int(plan->g.ntiles * plan->g.n_groups);
     return TCV_OK;
 }
 
@@ -385,14 +602,21 @@ void tcv_plan_destroy(tcv_plan* plan) { delete plan; }
 tcv_status tcv_plan_grid(const tcv_plan* plan, const float* d_data, const void* d_c, int c_type,
                          float c_scale, float* d_grid, void* stream)
 {
-    if (!plan || !d_c || !d_grid || (plan->g.n > 0 && !d_data)) return TCV_ERR_ARG;
+    if (!plan || !d_c || (plan->g.n > 0 && !d_data)) return TCV_ERR_ARG;
+    if (plan->batch ? d_grid != nullptr : d_grid == nullptr) return TCV_ERR_ARG;
     if (tcv_ctype_bytes(c_type) == 0) return TCV_ERR_ARG;
-    if (c_type & TCV_C_PADDED)
+    if (!plan->binned) return TCV_ERR_STATE;
+    const bool plain_tiles = !plan->batch && plan->g.rows == 16;  // what the other kernel families need
+    if (c_type & TCV_C_PADDED) {
+        if (!plain_tiles) return TCV_ERR_UNSUPPORTED;
         return launch_grid_pipe(plan, reinterpret_cast<const float2*>(d_data), d_c, c_type & 0xff, c_scale,
                                 reinterpret_cast<float2*>(d_grid), static_cast<cudaStream_t>(stream));
-    if (c_type & TCV_C_PAIRED)
+    }
+    if (c_type & TCV_C_PAIRED) {
+        if (!plain_tiles) return TCV_ERR_UNSUPPORTED;
         return launch_grid_pair(plan, reinterpret_cast<const float2*>(d_data), d_c, c_type & 0xff, c_scale,
                                 reinterpret_cast<float2*>(d_grid), static_cast<cudaStream_t>(stream));
+    }
     return launch_grid(plan, reinterpret_cast<const float2*>(d_data), d_c, c_type, c_scale,
                        reinterpret_cast<float2*>(d_grid), static_cast<cudaStream_t>(stream));
 }
@@ -400,19 +624,24 @@ tcv_status tcv_plan_grid(const tcv_plan* plan, const float* d_data, const void* 
 tcv_status tcv_plan_degrid(const tcv_plan* plan, const float* d_grid, const void* d_c, int c_type,
                            float c_scale, float* d_data, void* stream)
 {
-    if (!plan || !d_c || !d_grid || (plan->g.n > 0 && !d_data)) return TCV_ERR_ARG;
+    if (!plan || !d_c || (plan->g.n > 0 && !d_data)) return TCV_ERR_ARG;
+    if (plan->batch ? d_grid != nullptr : d_grid == nullptr) return TCV_ERR_ARG;
     if (tcv_ctype_bytes(c_type) == 0) return TCV_ERR_ARG;
+    if (!plan->binned) return TCV_ERR_STATE;
+    const bool plain_tiles = !plan->batch && plan->g.rows == 16;
     if (c_type & TCV_C_PADDED) {
+        if (!plain_tiles) return TCV_ERR_UNSUPPORTED;
         if (plan->g.n == 0) return TCV_OK;
         return launch_degrid_pipe(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type & 0xff, c_scale,
                                   reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
     }
     if (c_type & TCV_C_PAIRED) {
+        if (!plain_tiles) return TCV_ERR_UNSUPPORTED;
         if (plan->g.n == 0) return TCV_OK;
         return launch_degrid_pair(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type & 0xff, c_scale,
                                   reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
     }
-    if (plan->degrid_variant == TCV_DEGRID_TILES) {
+    if (plan->degrid_variant == TCV_DEGRID_TILES || plan->batch) {
         if (plan->g.n == 0) return TCV_OK;
         return launch_degrid_tiles(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type, c_scale,
                                    reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
@@ -424,6 +653,7 @@ tcv_status tcv_plan_degrid(const tcv_plan* plan, const float* d_grid, const void
 tcv_status tcv_plan_set_degrid_variant(tcv_plan* plan, int variant)
 {
     if (!plan || (variant != TCV_DEGRID_TILES && variant != TCV_DEGRID_ANCHOR)) return TCV_ERR_ARG;
+    if (variant == TCV_DEGRID_ANCHOR && !plan->g.anchors) return TCV_ERR_UNSUPPORTED;
     plan->degrid_variant = variant;
     return TCV_OK;
 }

@@ -28,6 +28,7 @@ PADDED = 0x100          # TCV_C_PADDED: prepared (TMA) table layout
 PAIRED = 0x200          # TCV_C_PAIRED: paired table layout (two columns per lane)
 PATH_TMA, PATH_DIRECT, PATH_PAIRED = 0, 1, 2
 DEGRID_TILES, DEGRID_ANCHOR = 0, 1
+PASS_BIN, PASS_GRID, PASS_DEGRID = 1, 2, 4
 
 
 class TcvError(RuntimeError):
@@ -60,6 +61,17 @@ class TcvDeviceBuffers(ctypes.Structure):
     ]
 
 
+class TcvJob(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("g_size", ctypes.c_int32), ("d_grid", ctypes.c_void_p)]
+
+
+class TcvTuning(ctypes.Structure):
+    _fields_ = [("tile_rows", ctypes.c_int32), ("group_mib", ctypes.c_int32)]
+
+    def as_tuple(self):
+        return (int(self.tile_rows), int(self.group_mib))
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I64 = ctypes.c_int64
@@ -90,6 +102,17 @@ SIGNATURES = {
     "tcv_plan_set_degrid_variant": (_I, [_P, _I]),
     "tcv_plan_info": (_I, [_P, _P, _P, _P, _P, _P]),
     "tcv_plan_destroy": (None, [_P]),
+    "tcv_plan_workspace_bytes_tuned": (_S, [_I64, _I, _I, _I64, _P]),
+    "tcv_plan_build_tuned": (_I, [_PP, _P, _P, _P, _I64, _I, _I, _I64, _P, _P, _S, _P]),
+    "tcv_batch_workspace_bytes": (_S, [_P, _I, _I, _I64, _P]),
+    "tcv_batch_plan_create": (_I, [_PP, _P, _I, _I, _I64, _P, _P, _S, _P]),
+    "tcv_plan_bin": (_I, [_P, _P, _P, _P, _P]),
+    "tcv_plan_tuning": (_I, [_P, _P]),
+    "tcv_autotune": (_I, [_P, _I, _P, _P, _P, _P, _P, _I, _F, _I64, _I, _I, _P, _P, _P]),
+    "tcv_autotune_report": (_I, [_P, _P, _I, _P]),
+    "tcv_graph_capture": (_I, [_PP, _P, _I, _P, _P, _P, _P, _P, _I, _F, _P, _P]),
+    "tcv_graph_launch": (_I, [_P, _P]),
+    "tcv_graph_destroy": (None, [_P]),
     "tcv_jit_prepare": (_I, [_I, _I]),
     "tcv_jit_enable": (None, [_I]),
     "tcv_jit_info": (ctypes.c_char_p, []),
@@ -120,6 +143,9 @@ SIGNATURES = {
     "tcv_set_ctype": (_I, [_P, _I]),
     "tcv_set_path": (_I, [_P, _I]),
     "tcv_get_path": (_I, [_P]),
+    "tcv_set_tuning": (_I, [_P, _P]),
+    "tcv_get_tuning": (_I, [_P, _P]),
+    "tcv_tune": (_I, [_P, _I, _P, _P]),
     "tcv_set_data": (_I, [_P, _P, _I64]),
     "tcv_get_data": (_I, [_P, _P, _I64]),
     "tcv_get_outdata": (_I, [_P, _P, _I64]),

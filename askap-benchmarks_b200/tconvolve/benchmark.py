@@ -109,6 +109,26 @@ class Benchmark:
         plan = ctypes.c_void_p(self.device_buffers().plan)
         check(lib().tcv_plan_set_degrid_variant(plan, int(variant)), "tcv_plan_set_degrid_variant")
 
+    def set_tuning(self, tile_rows: int = 16, group_mib: int = 32):
+        """Tile shape (grid rows per warp: 8, 16 or 32) and plane-group slice (MiB of complex64
+        table; -1 = the whole table in one group) of the plan.  Rebuilds the plan (the degridding
+        variant returns to "tiles")."""
+        t = _lib.TcvTuning(int(tile_rows), int(group_mib))
+        check(lib().tcv_set_tuning(self._ctx, ctypes.byref(t)), "tcv_set_tuning", self._ctx)
+
+    def tuning(self) -> tuple:
+        t = _lib.TcvTuning()
+        check(lib().tcv_get_tuning(self._ctx, ctypes.byref(t)), "tcv_get_tuning", self._ctx)
+        return t.as_tuple()
+
+    def tune(self, reps: int = 3):
+        """Autotune the plan on this problem, table form and grid (tcv_tune): the fastest
+        (tile_rows, group_mib) and its median ms per bin + grid + degrid pass."""
+        t = _lib.TcvTuning()
+        ms = ctypes.c_float()
+        check(lib().tcv_tune(self._ctx, int(reps), ctypes.byref(t), ctypes.byref(ms)), "tcv_tune", self._ctx)
+        return t.as_tuple(), float(ms.value)
+
     @property
     def path(self) -> int:
         return lib().tcv_get_path(self._ctx)

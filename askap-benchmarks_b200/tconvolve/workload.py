@@ -75,3 +75,14 @@ def normal_vis(n: int, seed: int) -> np.ndarray:
     out.real = re
     out.imag = im
     return out
+
+
+def batch_sizes(n_jobs: int = 64, seed: int = 0, n_min: float = 1e4, n_max: float = 4e5,
+                g_sizes=(2048, 4096)) -> list:
+    """Jobs of the batched workload: [(n_samples, g_size)] with n log-uniform in [n_min, n_max] and
+    g_size drawn uniformly from g_sizes (PCG64(seed)).  With the default 5 wavelength cells and
+    2000 m baseline every footprint reaches at most 999 cells from the centre, inside both sizes."""
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(math.log(n_min), math.log(n_max), n_jobs)).astype(np.int64)
+    g = rng.choice(np.asarray(g_sizes, dtype=np.int64), n_jobs)
+    return [(int(a), int(b)) for a, b in zip(n, g)]

@@ -55,6 +55,8 @@ def parse_args():
     p.add_argument("--path", default="direct", choices=["direct", "paired", "tma"], help="kernel family")
     p.add_argument("--degrid", default="tiles", choices=["tiles", "anchor"],
                    help="degridding kernel on the direct path")
+    p.add_argument("--no-tune", action="store_true", help="default tile shape and plane groups, no autotuning")
+    p.add_argument("--no-batched", action="store_true", help="skip the 64-job batched measurement")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=4.0, help="target wall time of the CPU sample")
     return p.parse_args()
@@ -217,17 +219,29 @@ def b200_arm(args):
     b.set_stream(stream.cuda_stream)
     b.set_path(args.path)
     b.init()
-    if form != tconvolve.C64:
-        b.set_ctype(form)
     vis = normal_vis(n, VIS_SEED)
     b.set_data(vis)
+    tunings = {}
+    if not args.no_tune and args.path == "direct":
+        # autotuned tile shape and plane groups for each form measured (tcv_tune on this problem)
+        if args.form != "c64":
+            b.set_ctype("c64")
+            tunings["c64"] = b.tune(3)
+        b.set_ctype(form)
+        tunings[args.form] = b.tune(3)
+    elif form != tconvolve.C64:
+        b.set_ctype(form)
     b.sync()
     bufs = b.device_buffers()
     support = b.getSupport()
     updates = b.updates_per_pass()
     c_len = b.c_len
     L = lib()
-    wbytes = L.tcv_plan_workspace_bytes(n, support, prob.g_size, c_len)
+    TcvTuning = tconvolve._lib.TcvTuning
+    tuning = {"t": TcvTuning(*(tunings[args.form][0] if args.form in tunings else (16, 32)))}
+    wbytes = max(L.tcv_plan_workspace_bytes_tuned(n, support, prob.g_size, c_len, ctypes.byref(TcvTuning(r, m)))
+                 for r in (8, 16, 32) for m in (32,))
+    wbytes = max(wbytes, L.tcv_plan_workspace_bytes_tuned(n, support, prob.g_size, c_len, ctypes.byref(tuning["t"])))
     work = torch.empty(wbytes, dtype=torch.uint8, device="cuda")
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     sp = ctypes.c_void_p(stream.cuda_stream)
@@ -241,8 +255,9 @@ def b200_arm(args):
         plan = ctypes.c_void_p()
         if evs:
             evs[0].record(stream)
-        check(L.tcv_plan_build(ctypes.byref(plan), P(tab.iu), P(tab.iv), P(tab.coff), n, support,
-                               prob.g_size, c_len, P(work.data_ptr()), wbytes, sp), "plan")
+        check(L.tcv_plan_build_tuned(ctypes.byref(plan), P(tab.iu), P(tab.iv), P(tab.coff), n, support,
+                                     prob.g_size, c_len, ctypes.byref(tuning["t"]), P(work.data_ptr()), wbytes,
+                                     sp), "plan")
         L.tcv_plan_set_degrid_variant(plan, dvariant)
         if evs:
             evs[1].record(stream)
@@ -289,12 +304,17 @@ def b200_arm(args):
     if args.form != "c64":
         # the plain form (complex64 table, the reference's storage) measured beside the chosen one
         b.set_ctype("c64")
+        chosen_t = tuning["t"]
+        if "c64" in tunings:
+            tuning["t"] = TcvTuning(*tunings["c64"][0])
         p_plan, p_grid, p_degrid, p_step, _ = timed(b.device_buffers(), args.steps)
+        tuning["t"] = chosen_t
         b.set_ctype(form)
         bufs = b.device_buffers()
         plain = {"form": "c64", "value": world * 2 * updates / (statistics.mean(p_step) * 1e-3),
                  "grid_ms": statistics.mean(p_grid), "degrid_ms": statistics.mean(p_degrid),
-                 "plan_ms": statistics.mean(p_plan)}
+                 "plan_ms": statistics.mean(p_plan),
+                 "tuning": tunings["c64"][0] if "c64" in tunings else (16, 32)}
 
     # e2e: the same step through the C ABI with host buffers: H2D of the batch's samples from
     # pinned memory, plan, grid, degrid, D2H of the degridded visibilities, every step
@@ -317,9 +337,9 @@ def b200_arm(args):
         d_co.copy_(h_co, non_blocking=True)
         plan = ctypes.c_void_p()
         sp = ctypes.c_void_p(stream.cuda_stream)
-        check(L.tcv_plan_build(ctypes.byref(plan), P(d_iu.data_ptr()), P(d_iv.data_ptr()),
-                               P(d_co.data_ptr()), n, support, prob.g_size, c_len,
-                               P(work.data_ptr()), wbytes, sp), "plan")
+        check(L.tcv_plan_build_tuned(ctypes.byref(plan), P(d_iu.data_ptr()), P(d_iv.data_ptr()),
+                                     P(d_co.data_ptr()), n, support, prob.g_size, c_len, ctypes.byref(tuning["t"]),
+                                     P(work.data_ptr()), wbytes, sp), "plan")
         L.tcv_plan_set_degrid_variant(plan, dvariant)
         check(L.tcv_plan_grid(plan, P(d_vis.data_ptr()), P(bufs.c_active), bufs.c_type, bufs.c_scale,
                               P(bufs.grid), sp), "grid")
@@ -370,6 +390,12 @@ def b200_arm(args):
              ("degrid", "direct"): ("degrid_tile_kernel + slot_reduce_kernel" if args.degrid == "tiles"
                                     else "degrid_staged_kernel")}[(dom, args.path)]
 
+    batched = None
+    if not args.no_batched:
+        b.close()
+        torch.cuda.empty_cache()
+        batched = batched_section(args, torch, stream, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args)
@@ -388,6 +414,8 @@ def b200_arm(args):
                                 "imaginary parts are zero; bit-identical to the plain c64 result)"
                                 if args.form == "r32" else args.form),
                        "path": args.path, "degrid": args.degrid,
+                       "tuning": {"tile_rows": tuning["t"].tile_rows, "group_mib": tuning["t"].group_mib,
+                                  "chosen_by": "autotuner (tcv_tune)" if tunings else "default"},
                        "parallelism": f"replicas x{world}",
                        "l2": f"{L2_FLUSH_BYTES >> 20} MiB buffer written between timed steps",
                        "step": "binning plan + gridding pass + degridding pass"},
@@ -401,6 +429,7 @@ def b200_arm(args):
                         "grid_updates_per_s": updates / (g_ms * 1e-3),
                         "degrid_updates_per_s": updates / (d_ms * 1e-3)},
             "plain_form": plain,
+            "batched": batched,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * (8 + 4 * 3),
                     "d2h_bytes_per_step": n * 8, "ms_per_step": e2e_mean},
             "gpu_launches": launches_per_step * args.steps if launches_per_step else None,
@@ -412,10 +441,89 @@ def b200_arm(args):
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    b.close()
+    if args.no_batched:
+        b.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def batched_section(args, torch, stream, world):
+    """The batched workload: 64 jobs (channels / Taylor terms) with sample counts log-uniform in
+    [1e4, 4e5] and grids of 2048^2 or 4096^2 sharing the 33-plane table, binned by one plan and run
+    as one captured CUDA graph (bin + grid + degrid of every job) per step, with the tile shape and
+    plane groups from the autotuner.  The grids (5 GB) are far larger than L2.  Measured for the
+    chosen form, the plain c64 form and the bf16 form; the bf16 result's relative L2 distance from
+    the plain result is measured here (the FP64-oracle errors are in the precision tests)."""
+    import tconvolve
+    from tconvolve import raw
+    from tconvolve._lib import PASS_BIN, PASS_DEGRID, PASS_GRID
+    from tconvolve.batch import Batch, autotune, make_problem
+    from tconvolve.workload import batch_sizes
+
+    sizes = batch_sizes(64, seed=0)
+    p = make_problem(sizes, vis_seed=VIS_SEED)
+    s2 = (2 * p["support"] + 1) ** 2
+    torch.cuda.synchronize()
+    res = {"workload": "64 jobs, n log-uniform in [1e4, 4e5] (PCG64 seed 0), gSize 2048 or 4096, wSize 33, "
+                       "support 64, one shared table",
+           "samples": p["total"], "step": "one CUDA graph launch: bin + grid + degrid of all jobs",
+           "forms": {}}
+    outs = {}
+    rejected = None
+    for name in dict.fromkeys([args.form, "c64", "rbf16"]):
+        ct = tconvolve.CTYPE_BY_NAME[name]
+        c, scale, _ = (p["c64"], 1.0, 0) if ct == tconvolve.C64 else raw.convert_c(p["c64"], ct)
+        t0 = time.perf_counter()
+        best, best_ms, report = autotune(sizes, p["iu"], p["iv"], p["coff"], p["data"], c, ct, p["support"], scale,
+                                         reps=3, stream=stream)
+        tune_s = time.perf_counter() - t0
+        grids = [torch.zeros(g * g, dtype=torch.complex64, device="cuda") for _, g in sizes]
+        bt = Batch(sizes, grids, p["iu"], p["iv"], p["coff"], p["support"], p["c_len"], tuning=best, stream=stream)
+        if rejected is None:
+            rejected = bt.rejected(stream)
+        out = torch.empty(p["total"], dtype=torch.complex64, device="cuda")
+        graph = bt.capture(PASS_BIN | PASS_GRID | PASS_DEGRID, p["data"], c, ct, vis=out, c_scale=scale)
+        for _ in range(max(args.warmup, 3)):
+            graph.launch(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        k = 5
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(k + 1)]
+        ev[0].record(stream)
+        for i in range(k):
+            graph.launch(stream)
+            ev[i + 1].record(stream)
+        torch.cuda.synchronize()
+        ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(k)]
+        step_ms = statistics.mean(ms)
+        if world > 1:
+            from tconvolve import replicas
+            step_ms = replicas.max_over_ranks([step_ms], device="cuda")[0]
+        # one more pass into zeroed grids for the comparison of forms
+        for gr in grids:
+            gr.zero_()
+        graph.launch(stream)
+        torch.cuda.synchronize()
+        outs[name] = out.clone()
+        upd = (p["total"] - rejected) * s2
+        res["forms"][name] = {"value": world * 2 * upd / (step_ms * 1e-3), "unit": UNIT, "ms_per_step": step_ms,
+                              "steps": k, "tuning": list(best), "autotune_s": tune_s,
+                              "candidates": [[list(t), m] for t, m in report]}
+        graph.close()
+        bt.close()
+        del grids, out
+        torch.cuda.empty_cache()
+    if "rbf16" in outs and "c64" in outs:
+        a, r = outs["rbf16"], outs["c64"]
+        res["forms"]["rbf16"]["rel_l2_vs_plain"] = float(torch.linalg.vector_norm(a - r) /
+                                                         torch.linalg.vector_norm(r))
+    res["rejected_samples"] = rejected
+    res["rejected_note"] = ("samples whose footprint (rows iv..iv+128) leaves a 2048 grid; skipped and counted, "
+                            "not in the update count")
+    return res
 
 
 def count_step_kernels(torch, step):

@@ -140,10 +140,12 @@ size_t tcv_plan_workspace_bytes(int64_t n, int support, int g_size, int64_t c_le
 tcv_status tcv_plan_build(tcv_plan **plan_out, const int32_t *d_iu, const int32_t *d_iv,
                           const int32_t *d_coff, int64_t n, int support, int g_size,
                           int64_t c_len, void *d_work, size_t work_bytes, void *stream);
-/* grid += gridding of d_data (n complex64) with table d_c of type c_type (Benchmark.cc:125-155). */
+/* grid += gridding of d_data (n complex64) with table d_c of type c_type (Benchmark.cc:125-155).
+ * d_grid is NULL for a batched plan (each job's own grid). */
 tcv_status tcv_plan_grid(const tcv_plan *plan, const float *d_data, const void *d_c, int c_type,
                          float c_scale, float *d_grid, void *stream);
-/* d_data[n] = degridding of d_grid (Benchmark.cc:158-195); overwrites d_data. */
+/* d_data[n] = degridding of d_grid (Benchmark.cc:158-195); overwrites d_data.  d_grid is NULL
+ * for a batched plan. */
 tcv_status tcv_plan_degrid(const tcv_plan *plan, const float *d_grid, const void *d_c, int c_type,
                            float c_scale, float *d_data, void *stream);
 /* Number of samples the plan rejected as out of bounds (synchronises the stream). */
@@ -162,6 +164,83 @@ tcv_status tcv_plan_set_degrid_variant(tcv_plan *plan, int variant);
 tcv_status tcv_plan_info(const tcv_plan *plan, int *tile_w, int *tile_h, int *anchor,
                          int *degrid_mode, int *n_tiles);
 void tcv_plan_destroy(tcv_plan *plan);
+
+/* ------------------------------------------------------------------------------------------
+ * Batched plans: many jobs (channels, Taylor terms) of uneven sample counts and grid sizes that
+ * share one table, binned together so that a gridding or degridding pass over all of them is
+ * one sequence of persistent launches.  No counterpart in the reference, which runs one job per
+ * process (attic/tConvolveMPI/tConvolveMPI.cc:78-119) or per thread (attic/tConvolveMT).
+ * ---------------------------------------------------------------------------------------- */
+typedef struct tcv_job {
+    int64_t n;     /* samples of the job; the jobs' samples are consecutive in the sample
+                      arrays, job 0 first */
+    int g_size;    /* side of the job's grid */
+    float *d_grid; /* the job's grid, g_size^2 complex64 (device): gridding adds into it,
+                      degridding reads it */
+} tcv_job;
+
+/* Tile shape and sort granularity of a plan (tcv_autotune chooses them by timing). */
+struct tcv_tuning {
+    int tile_rows; /* grid rows per warp of the tile kernels: 8, 16 or 32, i.e. tiles of
+                      64 x 4*tile_rows points; 0 = 16 */
+    int group_mib; /* table slice per plane group, MiB of complex64 (whole w-planes, at least
+                      one); 0 = 32; -1 = the whole table in one group */
+};
+
+/* Workspace of a batched plan (0 for invalid arguments).  tuning may be NULL (defaults). */
+size_t tcv_batch_workspace_bytes(const tcv_job *jobs, int n_jobs, int support, int64_t c_len,
+                                 const tcv_tuning *tuning);
+/* Create a batched plan in d_work: copies the job table to the device and numbers the jobs'
+ * tiles.  Set-up path (the job table is copied from host memory, so do not capture this call);
+ * bin the samples with tcv_plan_bin.  Gridding and degridding take d_grid = NULL and use the
+ * jobs' grids. */
+tcv_status tcv_batch_plan_create(tcv_plan **plan_out, const tcv_job *jobs, int n_jobs, int support,
+                                 int64_t c_len, const tcv_tuning *tuning, void *d_work,
+                                 size_t work_bytes, void *stream);
+/* Bin (or re-bin) the samples of a plan: device work only, safe to capture in a CUDA graph.
+ * tcv_plan_build does this for a one-job plan. */
+tcv_status tcv_plan_bin(tcv_plan *plan, const int32_t *d_iu, const int32_t *d_iv,
+                        const int32_t *d_coff, void *stream);
+/* The tuning a plan was made with. */
+tcv_status tcv_plan_tuning(const tcv_plan *plan, tcv_tuning *tuning_out);
+
+/* Autotuner: time every candidate tuning (tile_rows 8/16/32 x plane-group slices) on this batch,
+ * each as one bin + grid + degrid pass into scratch grids the tuner allocates (the jobs' grids
+ * are not touched), the median of reps passes after a warm-up, and return the fastest.  When the
+ * jobs' grids exceed 2 GiB the passes run on an evenly spread subset of jobs.  Set-up path:
+ * allocates, builds the specialised kernels it needs and synchronises.  The result is cached
+ * for the process per (support, c_type, table size, job sizes). */
+tcv_status tcv_autotune(const tcv_job *jobs, int n_jobs, const int32_t *d_iu, const int32_t *d_iv,
+                        const int32_t *d_coff, const float *d_data, const void *d_c, int c_type,
+                        float c_scale, int64_t c_len, int support, int reps,
+                        tcv_tuning *best_out, float *best_ms_out, void *stream);
+/* Candidates and median times (ms) of the last tcv_autotune run that timed (not a cache hit). */
+tcv_status tcv_autotune_report(tcv_tuning *cands, float *ms, int max, int *n_out);
+
+/* CUDA graph of the passes of one plan: bin (TCV_PASS_BIN), gridding (TCV_PASS_GRID) and
+ * degridding into d_vis (TCV_PASS_DEGRID), in that order, captured once and replayed with one
+ * launch.  d_grid: the grid of a one-job plan (NULL for a batched plan, whose jobs carry their
+ * grids).  The pointers are baked into the graph.  Builds the specialised kernels before
+ * capturing; a plan captured without TCV_PASS_BIN must be binned already. */
+enum { TCV_PASS_BIN = 1, TCV_PASS_GRID = 2, TCV_PASS_DEGRID = 4 };
+typedef struct tcv_graph tcv_graph;
+tcv_status tcv_graph_capture(tcv_graph **graph_out, tcv_plan *plan, int passes,
+                             const int32_t *d_iu, const int32_t *d_iv, const int32_t *d_coff,
+                             const float *d_data, const void *d_c, int c_type, float c_scale,
+                             float *d_grid, float *d_vis);
+tcv_status tcv_graph_launch(const tcv_graph *graph, void *stream);
+void tcv_graph_destroy(tcv_graph *graph);
+
+/* A one-job plan with a chosen tile shape and sort granularity (tcv_tuning, below; NULL for the
+ * defaults, which tcv_plan_workspace_bytes / tcv_plan_build use).  The TMA pipeline and paired
+ * kernel families need the default tile shape (TCV_ERR_UNSUPPORTED otherwise). */
+typedef struct tcv_tuning tcv_tuning;
+size_t tcv_plan_workspace_bytes_tuned(int64_t n, int support, int g_size, int64_t c_len,
+                                      const tcv_tuning *tuning);
+tcv_status tcv_plan_build_tuned(tcv_plan **plan_out, const int32_t *d_iu, const int32_t *d_iv,
+                                const int32_t *d_coff, int64_t n, int support, int g_size,
+                                int64_t c_len, const tcv_tuning *tuning, void *d_work,
+                                size_t work_bytes, void *stream);
 
 /* Tile kernels specialised on the footprint width.  The first launch of the tile kernels for a
  * (table form, support) builds copies with sSize = 2*support+1 a compile-time constant (NVRTC,
@@ -272,6 +351,13 @@ tcv_status tcv_set_ctype(tcv_ctx *ctx, int c_type);
 enum { TCV_PATH_TMA = 0, TCV_PATH_DIRECT = 1, TCV_PATH_PAIRED = 2 };
 tcv_status tcv_set_path(tcv_ctx *ctx, int path);
 int tcv_get_path(const tcv_ctx *ctx);
+/* Tile shape and sort granularity of the context's plan (rebuilds the plan; the default is
+ * {16, 32}).  tcv_tune times the candidates on the context's own samples, table form and grid
+ * size (tcv_autotune, reps timed passes each) and keeps the fastest; *best_out and *best_ms_out
+ * may be NULL.  Tile shapes other than the default need the direct path. */
+tcv_status tcv_set_tuning(tcv_ctx *ctx, const tcv_tuning *tuning);
+tcv_status tcv_get_tuning(const tcv_ctx *ctx, tcv_tuning *tuning_out);
+tcv_status tcv_tune(tcv_ctx *ctx, int reps, tcv_tuning *best_out, float *best_ms_out);
 
 /* Host <-> device transfers of the context's buffers (synchronous; host pointers). */
 tcv_status tcv_set_data(tcv_ctx *ctx, const float *vis, int64_t n);          /* n complex */

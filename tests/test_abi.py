@@ -106,3 +106,57 @@ def test_workspace_grows_with_samples(tcv):
     assert b > a
     # 160 k samples x 9 tiles: keys + values, double-buffered, plus the anchor sort; < 64 MiB
     assert b < 64 << 20
+
+
+def test_batch_argument_validation(tcv):
+    """Batched plans, tuning and graphs: invalid arguments are refused on the host."""
+    from tconvolve._lib import TcvJob, TcvTuning
+
+    L = tcv.lib()
+    jobs = (TcvJob * 3)()
+    for j, (n, g) in enumerate([(1000, 2048), (0, 4096), (5000, 2048)]):
+        jobs[j].n, jobs[j].g_size, jobs[j].d_grid = n, g, ctypes.c_void_p(256 * (j + 1))
+    clen = 35145792
+    ws = L.tcv_batch_workspace_bytes(jobs, 3, 64, clen, None)
+    assert ws > 0
+    # the workspace holds the cells of every job's tiles: it grows with each job
+    assert ws > L.tcv_batch_workspace_bytes(jobs, 2, 64, clen, None) > 0
+    for rows, mib in [(8, 32), (16, -1), (32, 8)]:
+        t = TcvTuning(rows, mib)
+        assert L.tcv_batch_workspace_bytes(jobs, 3, 64, clen, ctypes.byref(t)) > 0
+    for rows, mib in [(7, 32), (64, 32), (16, -2)]:
+        t = TcvTuning(rows, mib)
+        assert L.tcv_batch_workspace_bytes(jobs, 3, 64, clen, ctypes.byref(t)) == 0
+    assert L.tcv_batch_workspace_bytes(jobs, 0, 64, clen, None) == 0
+    jobs[1].d_grid = None
+    assert L.tcv_batch_workspace_bytes(jobs, 3, 64, clen, None) == 0  # every job needs a grid
+    jobs[1].d_grid = ctypes.c_void_p(512)
+    jobs[2].n = -1
+    assert L.tcv_batch_workspace_bytes(jobs, 3, 64, clen, None) == 0
+    plan = ctypes.c_void_p()
+    assert L.tcv_batch_plan_create(ctypes.byref(plan), jobs, 3, 64, clen, None, None, 0, None) == 1
+    assert L.tcv_plan_bin(None, None, None, None, None) == 1
+    assert L.tcv_plan_tuning(None, None) == 1
+    g = ctypes.c_void_p()
+    assert L.tcv_graph_capture(ctypes.byref(g), None, 7, None, None, None, None, None, 0, 1.0, None, None) == 1
+    assert L.tcv_graph_launch(None, None) == 1
+    best = TcvTuning()
+    assert L.tcv_autotune(jobs, 0, None, None, None, None, None, 0, 1.0, clen, 64, 3, ctypes.byref(best),
+                          None, None) == 1
+    n = ctypes.c_int()
+    assert L.tcv_autotune_report(None, None, 0, ctypes.byref(n)) == 0 and n.value >= 0
+
+
+def test_batch_geometry_limits(tcv):
+    """More jobs than the tile record holds, or tiles per side beyond it, are refused as
+    unsupported rather than mis-binned (no device work: the limits are host checks)."""
+    from tconvolve._lib import TcvJob
+
+    L = tcv.lib()
+    many = (TcvJob * 1025)()
+    for j in range(1025):
+        many[j].n, many[j].g_size, many[j].d_grid = 1, 64, ctypes.c_void_p(256)
+    plan = ctypes.c_void_p()
+    work = ctypes.c_void_p(256)
+    assert L.tcv_batch_plan_create(ctypes.byref(plan), many, 1025, 3, 7 * 7 * 64, None, work, 1 << 40,
+                                   None) == 8  # TCV_ERR_UNSUPPORTED
