@@ -5,8 +5,9 @@
 // degridding + the slot sum) is a few dozen launches; captured once into a CUDA graph it is
 // replayed with one launch and no host work.  The autotuner times the candidate tunings
 // (rows per warp 8/16/32, i.e. tiles of 64 x 32/64/128 points, and plane-group slices of
-// 8/16/32/64 MiB or the whole table) on the caller's own batch, into scratch grids, and keeps the
-// fastest.  Neither has a counterpart in the reference, whose kernels run one job per call
+// 8/16/32/64 MiB or the whole table; then work units of 512/256/128/64 samples for busy cells)
+// on the caller's own batch, into scratch grids, and keeps the fastest.  Neither has a
+// counterpart in the reference, whose kernels run one job per call
 // (attic/tConvolveMPI/Benchmark.cc:98-106).
 #include "tcv_internal.cuh"
 
@@ -186,7 +187,8 @@ tcv_status tcv_autotune(const tcv_job* jobs, int n_jobs, const int32_t* d_iu, co
         goff += size_t(jobs[j].g_size) * jobs[j].g_size * 8;
     }
 
-    // candidates; plane-group slices that give the same grouping are timed once
+    // stage 1: tile shape x plane groups, cells whole; slices that give the same grouping are
+    // timed once.  Stage 2: work-unit sizes on the stage-1 winner.
     std::vector<tcv_tuning> cands;
     std::vector<std::pair<int, int>> seen;  // (rows, kid_group)
     const int gs_max = [&] {
@@ -196,18 +198,13 @@ tcv_status tcv_autotune(const tcv_job* jobs, int n_jobs, const int32_t* d_iu, co
     }();
     for (int rows : {16, 8, 32})
         for (int mib : {32, 16, 64, 8, -1}) {
-            const tcv_tuning t{rows, mib};
-            const PlanGeom g = make_geom(n_sub, support, &gs_max, 1, c_len, &t);
+            const tcv_tuning t{rows, mib, 0};
+            const PlanGeom g = make_geom(n_sub, support, &gs_max, 1, c_len, &t, false);
             const std::pair<int, int> id(rows, g.kid_group);
             if (std::find(seen.begin(), seen.end(), id) != seen.end()) continue;
             seen.push_back(id);
             cands.push_back(t);
         }
-    size_t need = 0;
-    for (const tcv_tuning& t : cands)
-        need = std::max(need, tcv_batch_workspace_bytes(sub.data(), int(sub.size()), support, c_len, &t));
-    if (need == 0) return TCV_ERR_UNSUPPORTED;
-    if ((s = work.alloc(need)) != TCV_OK) return s;
 
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     TCV_CUDA(cudaEventCreate(&e0));
@@ -216,26 +213,38 @@ tcv_status tcv_autotune(const tcv_job* jobs, int n_jobs, const int32_t* d_iu, co
         return TCV_ERR_CUDA;
     }
     std::vector<std::pair<tcv_tuning, float>> report;
-    tcv_tuning best{16, 32};
+    tcv_tuning best{16, 32, 0};
     float best_ms = -1.f;
-    for (const tcv_tuning& t : cands) {
+    size_t have = 0;
+    auto time_one = [&](const tcv_tuning& t) -> tcv_status {
+        const size_t need = tcv_batch_workspace_bytes(sub.data(), int(sub.size()), support, c_len, &t);
+        if (need == 0) return TCV_ERR_UNSUPPORTED;
+        if (need > have) {
+            TCV_CUDA(cudaStreamSynchronize(st));
+            if (work.p) cudaFree(work.p);
+            work.p = nullptr;
+            have = 0;
+            const tcv_status a = work.alloc(need);
+            if (a != TCV_OK) return a;
+            have = need;
+        }
         jit_prepare(c_type, 2 * support + 1, t.tile_rows);
         tcv_plan* plan = nullptr;
-        s = tcv_batch_plan_create(&plan, sub.data(), int(sub.size()), support, c_len, &t, work.p, need, st);
-        if (s != TCV_OK) break;
+        tcv_status r = tcv_batch_plan_create(&plan, sub.data(), int(sub.size()), support, c_len, &t, work.p, have, st);
+        if (r != TCV_OK) return r;
         std::vector<float> ms;
-        for (int r = 0; r <= reps && s == TCV_OK; ++r) {  // pass 0 warms up
+        for (int k = 0; k <= reps && r == TCV_OK; ++k) {  // pass 0 warms up
             cudaEventRecord(e0, st);
-            s = run_passes(plan, TCV_PASS_BIN | TCV_PASS_GRID | TCV_PASS_DEGRID, s_iu, s_iv, s_co, s_data, d_c,
+            r = run_passes(plan, TCV_PASS_BIN | TCV_PASS_GRID | TCV_PASS_DEGRID, s_iu, s_iv, s_co, s_data, d_c,
                            c_type, c_scale, nullptr, static_cast<float*>(vis.p), st);
             cudaEventRecord(e1, st);
-            if (s == TCV_OK) s = cuda_status(cudaEventSynchronize(e1));
+            if (r == TCV_OK) r = cuda_status(cudaEventSynchronize(e1));
             float m = 0.f;
-            if (s == TCV_OK) cudaEventElapsedTime(&m, e0, e1);
-            if (r > 0) ms.push_back(m);
+            if (r == TCV_OK) cudaEventElapsedTime(&m, e0, e1);
+            if (k > 0) ms.push_back(m);
         }
         tcv_plan_destroy(plan);
-        if (s != TCV_OK) break;
+        if (r != TCV_OK) return r;
         std::sort(ms.begin(), ms.end());
         const float med = ms[ms.size() / 2];
         report.emplace_back(t, med);
@@ -243,6 +252,14 @@ tcv_status tcv_autotune(const tcv_job* jobs, int n_jobs, const int32_t* d_iu, co
             best_ms = med;
             best = t;
         }
+        return TCV_OK;
+    };
+    for (const tcv_tuning& t : cands)
+        if ((s = time_one(t)) != TCV_OK) break;
+    if (s == TCV_OK) {
+        const tcv_tuning base = best;
+        for (int split : {512, 256, 128, 64})
+            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, split})) != TCV_OK) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -50,7 +50,13 @@ struct GridArgs {
     float2* grid;                   // grid of a one-job plan given at launch, else nullptr
     const JobDesc* __restrict__ jobs;
     const u32* __restrict__ tinfo;  // per tile: column | row << 11 | job << 22
+    float2* partial;                // partial tiles of split cells (gridding), tile after tile
 };
+
+// A work unit: a cell's samples [first, first + count) of the sorted order, and the partial tile
+// it writes when its cell is split among several units (kDirect: the unit owns the whole cell
+// and adds its tile into the grid itself).
+constexpr u32 kDirect = 0xffffffffu;
 
 // per-tile record: tile column (11 bits), tile row (11 bits), job (10 bits)
 __host__ __device__ constexpr u32 tile_record(u32 job, u32 tx, u32 ty) { return tx | (ty << 11) | (job << 22); }
@@ -119,42 +125,41 @@ __host__ __device__ constexpr int grid_min_blocks() { return kR >= 32 ? 2 : Tab:
 template <int kR>
 __host__ __device__ constexpr int degrid_min_blocks() { return kR >= 32 ? 2 : 3; }
 
-// The CTA's work is the sequence of chunks (up to kTileChunk samples) of the cells it owns (every
-// gridDim.x-th non-empty cell of the plane group).  Chunk i is staged in shared memory while chunk
-// i-1 is processed, so each chunk costs one barrier and the next cell's samples arrive early.
+// The CTA's work is the sequence of chunks (up to kTileChunk samples) of the work units it owns
+// (every gridDim.x-th unit of the plane group).  Chunk i is staged in shared memory while chunk
+// i-1 is processed, so each chunk costs one barrier and the next unit's samples arrive early.
 struct ChunkCursor {
-    u32 it, base;  // cell list position, first sample of the chunk in that cell
+    u32 it, base;  // unit list position, first sample of the chunk in that unit
     u32 cnt, start;
-    u32 ti;        // the cell's tile record (tile_record)
+    u32 ti;        // the unit's tile record (tile_record)
+    u32 pslot;     // partial tile of a split cell, or kDirect
     int m;         // samples in the chunk (0: no more work)
 };
 
-__device__ __forceinline__ void cursor_load(ChunkCursor& c, u32 it, u32 i1, const u32* __restrict__ items,
-                                            const u32* __restrict__ tile_start, const u32* __restrict__ tile_count,
+__device__ __forceinline__ void cursor_load(ChunkCursor& c, u32 it, u32 i1, const uint4* __restrict__ units,
                                             const GridArgs& a)
 {
     c.it = it;
     c.base = 0;
     c.m = 0;
     if (it < i1) {
-        const u32 cell = items[it];
-        c.cnt = tile_count[cell];
-        c.start = tile_start[cell];
-        c.ti = a.tinfo[cell - u32(a.group) * u32(a.ntiles)];
+        const uint4 u = units[it];
+        c.start = u.y;
+        c.cnt = u.z;
+        c.pslot = u.w;
+        c.ti = a.tinfo[u.x - u32(a.group) * u32(a.ntiles)];
         c.m = int(c.cnt < u32(kTileChunk) ? c.cnt : u32(kTileChunk));
     }
 }
 
-__device__ __forceinline__ void cursor_next(ChunkCursor& c, u32 i1, const u32* __restrict__ items,
-                                            const u32* __restrict__ tile_start, const u32* __restrict__ tile_count,
-                                            const GridArgs& a)
+__device__ __forceinline__ void cursor_next(ChunkCursor& c, u32 i1, const uint4* __restrict__ units, const GridArgs& a)
 {
     if (c.base + u32(kTileChunk) < c.cnt) {
         c.base += u32(kTileChunk);
         const u32 left = c.cnt - c.base;
         c.m = int(left < u32(kTileChunk) ? left : u32(kTileChunk));
     } else {
-        cursor_load(c, c.it + gridDim.x, i1, items, tile_start, tile_count, a);
+        cursor_load(c, c.it + gridDim.x, i1, units, a);
     }
 }
 
@@ -163,15 +168,14 @@ __global__ void __launch_bounds__(kTileThreads, grid_min_blocks<Tab, kR>())
 grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
                  const int* __restrict__ iu, const int* __restrict__ iv,
                  const int* __restrict__ coff, const u32* __restrict__ order,
-                 const u32* __restrict__ tile_start, const u32* __restrict__ tile_count,
-                 const u32* __restrict__ items, const u32* __restrict__ group_start, GridArgs a)
+                 const uint4* __restrict__ units, const u32* __restrict__ group_ustart, GridArgs a)
 {
     constexpr int kTH = tile_height(kR);
     __shared__ float4 sm_rec[2][kTileChunk];  // (data.re, data.im, first column, first row)
     __shared__ int sm_coff[2][kTileChunk];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
-    const u32 i1 = group_start[a.group + 1];
+    const u32 i1 = group_ustart[a.group + 1];
     auto stage = [&](const ChunkCursor& c, int buf) {
         if (int(threadIdx.x) < c.m) {
             const u32 k = order[c.start + c.base + threadIdx.x];
@@ -182,7 +186,7 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
         }
     };
     ChunkCursor cur;
-    cursor_load(cur, group_start[a.group] + blockIdx.x, i1, items, tile_start, tile_count, a);
+    cursor_load(cur, group_ustart[a.group] + blockIdx.x, i1, units, a);
     stage(cur, 0);
     __syncthreads();
     float2 acc[kR];
@@ -191,7 +195,7 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
     int buf = 0;
     while (cur.m > 0) {
         ChunkCursor nxt = cur;
-        cursor_next(nxt, i1, items, tile_start, tile_count, a);
+        cursor_next(nxt, i1, units, a);
         stage(nxt, buf ^ 1);  // overlaps with the work below
 
         const int tx = rec_tx(cur.ti), ty = rec_ty(cur.ti);
@@ -225,7 +229,16 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
                 }
             }
         }
-        if (nxt.it != cur.it || nxt.m == 0) {
+        if ((nxt.it != cur.it || nxt.m == 0) && cur.pslot != kDirect) {
+            // a unit of a split cell: its partial tile, summed into the grid by fold_kernel
+            float2* pt = a.partial + (unsigned long long)(cur.pslot) * (kTileW * kTH) +
+                         ((warp / (kTileW / 32)) * kR) * kTileW + (warp % (kTileW / 32)) * 32 + lane;
+#pragma unroll
+            for (int r = 0; r < kR; ++r) {
+                pt[r * kTileW] = acc[r];
+                acc[r] = make_float2(0.f, 0.f);
+            }
+        } else if (nxt.it != cur.it || nxt.m == 0) {
             // the cell is complete: add its tile into the job's grid (each point has this one owner)
             const JobDesc& jd = a.jobs[rec_job(cur.ti)];
             const int gs = jd.g_size;
@@ -262,8 +275,7 @@ __global__ void __launch_bounds__(kTileThreads, degrid_min_blocks<kR>())
 degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                    const int* __restrict__ iu, const int* __restrict__ iv,
                    const int* __restrict__ coff, const u32* __restrict__ order,
-                   const u32* __restrict__ tile_start, const u32* __restrict__ tile_count,
-                   const u32* __restrict__ items, const u32* __restrict__ group_start,
+                   const uint4* __restrict__ units, const u32* __restrict__ group_ustart,
                    float2* __restrict__ slots, int max_tiles, GridArgs a)
 {
     constexpr int kTH = tile_height(kR);
@@ -271,12 +283,11 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
     __shared__ float2 sm_part[kTileChunk][kTileWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
-    const u32 i1 = group_start[a.group + 1];
-    for (u32 it = group_start[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
-        const u32 cell = items[it];
-        const u32 cnt = tile_count[cell];
-        const u32 start = tile_start[cell];
-        const u32 ti = a.tinfo[cell - u32(a.group) * u32(a.ntiles)];
+    const u32 i1 = group_ustart[a.group + 1];
+    for (u32 it = group_ustart[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
+        const uint4 u = units[it];  // the units of a split cell each read the tile; no partials
+        const u32 start = u.y, cnt = u.z;
+        const u32 ti = a.tinfo[u.x - u32(a.group) * u32(a.ntiles)];
         const JobDesc& jd = a.jobs[rec_job(ti)];
         const int gs = jd.g_size;
         const float2* grid = a.grid ? a.grid : jd.grid;
@@ -344,6 +355,59 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                 const int sx0 = q.y / kTileW, sx1 = (q.y + s - 1) / kTileW, sy0 = q.z / kTH;
                 const int slot = (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0);
                 slots[(unsigned long long)(u32(q.x)) * max_tiles + slot] = v;
+            }
+        }
+    }
+}
+
+// Fold the partial tiles of the split cells of one plane group into the grid: for every point,
+// the units' partial sums in unit order, then one add into the grid (deterministic).  Work items
+// are (cell, 256-point slice of its tile), block-stride over the group's non-empty cells; cells
+// that were not split are skipped.
+template <int kR>
+__global__ void __launch_bounds__(kTileThreads)
+fold_kernel(const u32* __restrict__ items, const u32* __restrict__ group_start, const u32* __restrict__ nunits,
+            const u32* __restrict__ pstart, GridArgs a)
+{
+    constexpr int kTH = tile_height(kR);
+    constexpr int kPoints = kTileW * kTH;
+    constexpr u32 kSlices = kPoints / kTileThreads;
+    const u32 i0 = group_start[a.group], i1 = group_start[a.group + 1];
+    for (u32 w = blockIdx.x; w < (i1 - i0) * kSlices; w += gridDim.x) {
+        const u32 k = i0 + w / kSlices;
+        const u32 nu = nunits[k];
+        if (nu < 2) continue;  // block-uniform
+        const u32 ti = a.tinfo[items[k] - u32(a.group) * u32(a.ntiles)];
+        const JobDesc& jd = a.jobs[rec_job(ti)];
+        const int gs = jd.g_size;
+        float2* grid = a.grid ? a.grid : jd.grid;
+        const float2* pt = a.partial + (unsigned long long)(pstart[k]) * kPoints;
+        {
+            const int p = int(w % kSlices) * kTileThreads + threadIdx.x;
+            const int gx = rec_tx(ti) * kTileW + (p % kTileW), gy = rec_ty(ti) * kTH + (p / kTileW);
+            float2 v = pt[p];
+            u32 q = 1;
+            for (; q + 4 <= nu; q += 4) {  // four loads in flight, added in unit order
+                float2 w4[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) w4[e] = pt[(unsigned long long)(q + e) * kPoints + p];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    v.x += w4[e].x;
+                    v.y += w4[e].y;
+                }
+            }
+            for (; q < nu; ++q) {
+                const float2 w1 = pt[(unsigned long long)(q) * kPoints + p];
+                v.x += w1.x;
+                v.y += w1.y;
+            }
+            if (gx < gs && gy < gs) {
+                float2* gp = grid + ((unsigned long long)(gy) * gs + gx);
+                float2 o = *gp;
+                o.x += v.x;
+                o.y += v.y;
+                *gp = o;
             }
         }
     }

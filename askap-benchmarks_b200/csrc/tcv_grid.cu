@@ -19,6 +19,15 @@ int resident_of(const void* kernel)
     return per_sm * sms;
 }
 
+// CTAs of a fold launch: a few per SM, each walking the group's cells
+int fold_ctas()
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return 4 * sms;
+}
+
 GridArgs make_args(const tcv_plan* p, int grp, float c_scale, float2* grid)
 {
     const PlanGeom& g = p->g;
@@ -31,6 +40,7 @@ GridArgs make_args(const tcv_plan* p, int grp, float c_scale, float2* grid)
     a.grid = grid;
     a.jobs = p->jobs;
     a.tinfo = p->tinfo;
+    a.partial = p->partial;
     return a;
 }
 
@@ -51,10 +61,14 @@ tcv_status launch(const tcv_plan* p, const float2* data, const void* c, float c_
     for (int grp = 0; grp < g.n_groups; ++grp) {
         GridArgs a = make_args(p, grp, c_scale, grid);
         void* args[] = {&data, &tab, const_cast<const int32_t**>(&p->iu), const_cast<const int32_t**>(&p->iv),
-                        const_cast<const int32_t**>(&p->coff), &order,
-                        const_cast<uint32_t**>(&p->tile_start), const_cast<uint32_t**>(&p->tile_count),
-                        const_cast<uint32_t**>(&p->items), const_cast<uint32_t**>(&p->group_start), &a};
+                        const_cast<const int32_t**>(&p->coff), &order, const_cast<uint4**>(&p->units),
+                        const_cast<uint32_t**>(&p->group_ustart), &a};
         TCV_CUDA(cudaLaunchKernel(kernel, dim3(ctas), dim3(kTileThreads), args, 0, st));
+        if (g.split) {
+            // the split cells' partial tiles into the grid, before the next group touches it
+            fold_kernel<kR><<<fold_ctas(), kTileThreads, 0, st>>>(p->items, p->group_start, p->nunits, p->pstart, a);
+            TCV_CUDA(cudaGetLastError());
+        }
     }
     return TCV_OK;
 }
@@ -76,10 +90,8 @@ tcv_status launch_adjoint(const tcv_plan* p, const float2* grid, const void* c, 
     for (int grp = 0; grp < g.n_groups; ++grp) {
         GridArgs a = make_args(p, grp, c_scale, gridp);
         void* args[] = {&tab, const_cast<const int32_t**>(&p->iu), const_cast<const int32_t**>(&p->iv),
-                        const_cast<const int32_t**>(&p->coff), &order,
-                        const_cast<uint32_t**>(&p->tile_start), const_cast<uint32_t**>(&p->tile_count),
-                        const_cast<uint32_t**>(&p->items), const_cast<uint32_t**>(&p->group_start),
-                        const_cast<float2**>(&p->slots), &max_tiles, &a};
+                        const_cast<const int32_t**>(&p->coff), &order, const_cast<uint4**>(&p->units),
+                        const_cast<uint32_t**>(&p->group_ustart), const_cast<float2**>(&p->slots), &max_tiles, &a};
         TCV_CUDA(cudaLaunchKernel(kernel, dim3(ctas), dim3(kTileThreads), args, 0, st));
     }
     return slot_reduce(p, c_scale, out, st);

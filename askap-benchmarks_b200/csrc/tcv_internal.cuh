@@ -43,6 +43,7 @@ struct PlanGeom {
     // gridding: output-stationary tiles of tw x th points (th = 4 * rows); work cells are
     // (group, tile) with the tiles of all jobs numbered in one space
     int rows, tw, th;
+    int split;          // samples per work unit of a split cell (0: cells are never split)
     int ntx, nty;       // tiles per row / column of a one-job plan
     int64_t ntiles;     // tiles of all jobs
     int max_tiles;      // tiles one footprint can touch
@@ -75,6 +76,12 @@ struct tcv_plan {
     uint32_t* items;               // non-empty gridding cells, group-major
     uint32_t* n_items;             // [0] = number of non-empty gridding cells
     uint32_t* group_start;         // n_groups + 1: items of group g are [group_start[g], group_start[g+1])
+    uint32_t* group_ustart;        // n_groups + 1: work units of group g
+    uint32_t* nunits;              // per item: work units of its cell
+    uint32_t* ustart;              // per item: its first unit
+    uint32_t* pstart;              // per item: its first partial tile (split cells)
+    uint4* units;                  // work units (cell, first sorted pair, count, partial tile or kDirect)
+    float2* partial;               // partial tiles of split cells, tw x th points each
     uint32_t* atile_count;         // samples per anchor cell (group, anchor tile)
     uint32_t* atile_start;
     uint32_t* aitems;              // non-empty anchor cells, group-major
@@ -96,8 +103,10 @@ struct tcv_plan {
 namespace tcv {
 
 // Host helpers implemented in tcv_plan.cu
-// Geometry for jobs of the given grid sides (n samples in all); tuning may be nullptr.
-PlanGeom make_geom(int64_t n, int support, const int* g_sizes, int n_jobs, int64_t c_len, const tcv_tuning* t);
+// Geometry for jobs of the given grid sides (n samples in all); tuning may be nullptr.  anchors:
+// also bin for the anchor-tile degridding kernels (one-job plans of tcv_plan_build only).
+PlanGeom make_geom(int64_t n, int support, const int* g_sizes, int n_jobs, int64_t c_len, const tcv_tuning* t,
+                   bool anchors);
 size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out);
 // one-job plan in d_work, binned (tcv_plan_build)
 tcv_status plan_init(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff, int64_t n,

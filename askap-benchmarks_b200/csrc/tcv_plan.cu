@@ -15,6 +15,9 @@
 // into work lists (with per-group ranges) that persistent kernels walk.
 // A plan may hold several jobs sharing the table (a batch): their tiles are numbered in one
 // space, job after job, so one sort and one sequence of launches covers all of them.
+// Cells with many samples are split into work units of about `split` samples (the units of a
+// gridding cell write partial tiles that a fold adds into the grid in unit order), so that a
+// plan with few busy tiles still spreads over every SM.
 // Samples whose footprint or table range falls outside their grid or the table are counted and
 // left out (sentinel key, sorted past the end).
 #include "tcv_internal.cuh"
@@ -124,6 +127,22 @@ __global__ void one_job_kernel(JobDesc* jobs, uint32_t* job_start, int g_size, i
     job_start[1] = n;
 }
 
+// the job table of a batch of up to kParamJobs jobs, passed by value: no host-memory copy, so
+// creating such a plan neither waits for the stream nor keeps a host buffer alive
+constexpr int kParamJobs = 128;
+struct JobTableParam {
+    JobDesc jobs[kParamJobs];
+    uint32_t start[kParamJobs + 1];
+};
+static_assert(sizeof(JobTableParam) <= 4000, "kernel parameter space");
+
+__global__ void job_table_kernel(const JobTableParam t, int n_jobs, JobDesc* jobs, uint32_t* job_start)
+{
+    const int j = threadIdx.x;
+    if (j < n_jobs) jobs[j] = t.jobs[j];
+    if (j <= n_jobs) job_start[j] = t.start[j];
+}
+
 // per tile of all jobs: its record (job, column, row)
 __global__ void tile_info_kernel(const JobDesc* __restrict__ jobs, int n_jobs, uint32_t ntiles, uint32_t* tinfo)
 {
@@ -146,14 +165,50 @@ struct NonZero {
     __host__ __device__ __forceinline__ bool operator()(const uint32_t& v) const { return v != 0; }
 };
 
-// group_start[g] = first item whose cell belongs to group g or later (items are sorted)
+// per non-empty cell k: the work units it is split into (cells of fewer than 2*split samples
+// stay whole) and the partial tiles those write (none for a whole cell)
+__global__ void unit_count_kernel(const uint32_t* __restrict__ items, const uint32_t* __restrict__ n_items,
+                                  const uint32_t* __restrict__ tile_count, uint32_t cap, uint32_t split,
+                                  uint32_t* nunits, uint32_t* nparts)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cap) return;
+    uint32_t nu = 0, np = 0;
+    if (k < *n_items) {
+        const uint32_t cnt = tile_count[items[k]];
+        nu = (split && cnt >= 2 * split) ? cnt / split : 1;
+        np = nu > 1 ? nu : 0;
+    }
+    nunits[k] = nu;
+    nparts[k] = np;
+}
+
+// the unit list: unit q of cell k takes samples [q*cnt/nu, (q+1)*cnt/nu) of the cell
+__global__ void unit_expand_kernel(const uint32_t* __restrict__ items, const uint32_t* __restrict__ n_items,
+                                   const uint32_t* __restrict__ tile_count, const uint32_t* __restrict__ tile_start,
+                                   const uint32_t* __restrict__ nunits, const uint32_t* __restrict__ ustart,
+                                   const uint32_t* __restrict__ pstart, uint4* units)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= *n_items) return;
+    const uint32_t cell = items[k], cnt = tile_count[cell], first = tile_start[cell], nu = nunits[k];
+    for (uint32_t q = 0; q < nu; ++q) {
+        const uint32_t b0 = uint32_t(uint64_t(q) * cnt / nu), b1 = uint32_t(uint64_t(q + 1) * cnt / nu);
+        units[ustart[k] + q] = make_uint4(cell, first + b0, b1 - b0, nu > 1 ? pstart[k] + q : kDirect);
+    }
+}
+
+// group_start[g] = first item whose cell belongs to group g or later (items are sorted), and
+// group_ustart[g] the first unit of that item
 __global__ void group_ranges_kernel(const uint32_t* items, const uint32_t* n_items, int n_groups,
-                                    uint32_t cells_per_group, uint32_t* group_start)
+                                    uint32_t cells_per_group, const uint32_t* nunits, const uint32_t* ustart,
+                                    uint32_t* group_start, uint32_t* group_ustart)
 {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g > n_groups) return;
     const uint32_t key = uint32_t(g) * cells_per_group;
-    uint32_t lo = 0, hi = *n_items;
+    const uint32_t n = *n_items;
+    uint32_t lo = 0, hi = n;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
         if (items[mid] < key)
@@ -162,11 +217,16 @@ __global__ void group_ranges_kernel(const uint32_t* items, const uint32_t* n_ite
             hi = mid;
     }
     group_start[g] = lo;
+    group_ustart[g] = lo < n ? ustart[lo] : (n ? ustart[n - 1] + nunits[n - 1] : 0);
 }
 
 inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
 inline size_t grid_cells(const PlanGeom& g) { return size_t(g.n_groups) * size_t(g.ntiles); }
+// a split cell of cnt >= 2*split samples makes floor(cnt/split) units, so the units of split cells
+// number at most pairs/split, and every other non-empty cell makes one
+inline size_t max_partials(const PlanGeom& g) { return g.split ? size_t(g.n) * g.max_tiles / size_t(g.split) : 0; }
+inline size_t max_units(const PlanGeom& g) { return grid_cells(g) + max_partials(g); }
 inline size_t anchor_cells(const PlanGeom& g) { return g.anchors ? size_t(g.n_groups) * g.natx * g.naty : 0; }
 
 template <typename K>
@@ -234,8 +294,22 @@ tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_
         tb = p->cub_bytes;
         TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, afl, p->aitems, p->n_aitems, acells, st));
     }
+    // work units
+    unit_count_kernel<<<unsigned((cells + 255) / 256), 256, 0, st>>>(p->items, p->n_items, p->tile_count,
+                                                                      uint32_t(cells), uint32_t(g.split), p->nunits,
+                                                                      p->pstart);
+    TCV_CUDA(cudaGetLastError());
+    tb = p->cub_bytes;
+    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->nunits, p->ustart, cells, st));
+    tb = p->cub_bytes;
+    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->pstart, p->pstart, cells, st));
+    unit_expand_kernel<<<unsigned((cells + 255) / 256), 256, 0, st>>>(p->items, p->n_items, p->tile_count,
+                                                                       p->tile_start, p->nunits, p->ustart, p->pstart,
+                                                                       p->units);
+    TCV_CUDA(cudaGetLastError());
     group_ranges_kernel<<<(g.n_groups + 1 + 127) / 128, 128, 0, st>>>(p->items, p->n_items, g.n_groups,
-                                                                       uint32_t(g.ntiles), p->group_start);
+                                                                       uint32_t(g.ntiles), p->nunits, p->ustart,
+                                                                       p->group_start, p->group_ustart);
     TCV_CUDA(cudaGetLastError());
     return TCV_OK;
 }
@@ -244,7 +318,7 @@ bool valid_tuning(const tcv_tuning* t)
 {
     if (!t) return true;
     const bool rows_ok = t->tile_rows == 0 || t->tile_rows == 8 || t->tile_rows == 16 || t->tile_rows == 32;
-    return rows_ok && t->group_mib >= -1;
+    return rows_ok && t->group_mib >= -1 && t->split >= 0 && t->split <= (1 << 24);
 }
 
 // Lay the plan's arrays out in d_work and write the job table: from host memory for a batch,
@@ -282,6 +356,12 @@ tcv_status plan_create(tcv_plan* p, void* d_work, size_t work_bytes, cudaStream_
     p->items = static_cast<uint32_t*>(take(cells * 4));
     p->n_items = static_cast<uint32_t*>(take(4));
     p->group_start = static_cast<uint32_t*>(take(size_t(g.n_groups + 1) * 4));
+    p->group_ustart = static_cast<uint32_t*>(take(size_t(g.n_groups + 1) * 4));
+    p->nunits = static_cast<uint32_t*>(take(cells * 4));
+    p->ustart = static_cast<uint32_t*>(take(cells * 4));
+    p->pstart = static_cast<uint32_t*>(take(cells * 4));
+    p->units = static_cast<uint4*>(take(max_units(g) * sizeof(uint4)));
+    p->partial = static_cast<float2*>(take(max_partials(g) * size_t(g.tw) * g.th * sizeof(float2)));
     p->atile_count = static_cast<uint32_t*>(take(acells * 4));
     p->atile_start = static_cast<uint32_t*>(take(acells * 4));
     p->aitems = static_cast<uint32_t*>(take(acells * 4));
@@ -292,7 +372,13 @@ tcv_status plan_create(tcv_plan* p, void* d_work, size_t work_bytes, cudaStream_
     p->cub_temp = take(cb);
     p->cub_bytes = cb;
     p->degrid_variant = TCV_DEGRID_TILES;
-    if (p->batch) {
+    if (p->batch && g.n_jobs <= kParamJobs) {
+        JobTableParam t{};
+        for (int j = 0; j < g.n_jobs; ++j) t.jobs[j] = p->host_jobs[size_t(j)];
+        for (int j = 0; j <= g.n_jobs; ++j) t.start[j] = p->host_job_start[size_t(j)];
+        job_table_kernel<<<1, kParamJobs + 1, 0, st>>>(t, g.n_jobs, p->jobs, p->job_start);
+        TCV_CUDA(cudaGetLastError());
+    } else if (p->batch) {
         TCV_CUDA(cudaMemcpyAsync(p->jobs, p->host_jobs.data(), p->host_jobs.size() * sizeof(JobDesc),
                                  cudaMemcpyHostToDevice, st));
         TCV_CUDA(cudaMemcpyAsync(p->job_start, p->host_job_start.data(), p->host_job_start.size() * 4,
@@ -317,6 +403,7 @@ bool geom_supported(const PlanGeom& g)
     if (g.n * g.max_tiles >= (int64_t(1) << 31)) return false;
     if (int64_t(g.n_groups) * g.ntiles >= (int64_t(1) << 31)) return false;
     if (g.max_tiles > 65535) return false;
+    if (max_units(g) >= (size_t(1) << 31)) return false;
     return true;
 }
 
@@ -326,7 +413,8 @@ bool geom_supported(const PlanGeom& g)
 // Degridding anchor tiles are the largest ta whose staged region (ta + sSize - 1)^2 complex
 // points fits in shared memory next to the partial sums; beyond that the direct kernel reads
 // the grid from global memory.
-PlanGeom make_geom(int64_t n, int support, const int* g_sizes, int n_jobs, int64_t c_len, const tcv_tuning* t)
+PlanGeom make_geom(int64_t n, int support, const int* g_sizes, int n_jobs, int64_t c_len, const tcv_tuning* t,
+                   bool anchors)
 {
     PlanGeom g{};
     g.n = n;
@@ -354,6 +442,7 @@ PlanGeom make_geom(int64_t n, int support, const int* g_sizes, int n_jobs, int64
     if (g.n_groups < 1) g.n_groups = 1;
     g.group_bits = bits_for(uint64_t(g.n_groups - 1));
     g.rows = (t && t->tile_rows) ? t->tile_rows : 16;
+    g.split = t ? t->split : 0;
     g.tw = kTileW;
     g.th = tile_height(g.rows);
     g.ntiles = 0;
@@ -365,7 +454,7 @@ PlanGeom make_geom(int64_t n, int support, const int* g_sizes, int n_jobs, int64
     g.tile_bits = bits_for(uint64_t(g.n_groups) * uint64_t(g.ntiles) - 1);
     g.key_bits = g.tile_bits + 1;  // cell, plus the sentinel bit
 
-    g.anchors = n_jobs == 1;
+    g.anchors = anchors && n_jobs == 1;
     g.degrid_mode = 1;
     g.ta = 32;
     g.degrid_parts = 4;
@@ -406,6 +495,8 @@ size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out)
     b += 2 * align_up(an * ks) + 2 * align_up(an * 4);
     const size_t cells = grid_cells(g), acells = anchor_cells(g);
     b += 3 * align_up(cells * 4) + align_up(4) + align_up(size_t(g.n_groups + 1) * 4);
+    b += align_up(size_t(g.n_groups + 1) * 4) + 3 * align_up(cells * 4) + align_up(max_units(g) * sizeof(uint4));
+    b += align_up(max_partials(g) * size_t(g.tw) * g.th * sizeof(float2));
     b += 3 * align_up(acells * 4) + align_up(4);
     b += align_up(sizeof(unsigned long long)) + align_up(sizeof(unsigned int));
     b += align_up(np * sizeof(float2));
@@ -434,7 +525,7 @@ tcv_status plan_init(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, cons
     if (n > 0 && (!d_iu || !d_iv || !d_coff)) return TCV_ERR_ARG;
     if (!d_work) return TCV_ERR_ARG;
     *p = tcv_plan{};
-    p->g = make_geom(n, support, &g_size, 1, c_len, t);
+    p->g = make_geom(n, support, &g_size, 1, c_len, t, true);
     if (!geom_supported(p->g)) return TCV_ERR_UNSUPPORTED;
     const tcv_status s = plan_create(p, d_work, work_bytes, st);
     if (s != TCV_OK) return s;
@@ -469,7 +560,7 @@ extern "C" {
 size_t tcv_plan_workspace_bytes(int64_t n, int support, int g_size, int64_t c_len)
 {
     if (n < 0 || support < 0 || g_size < 1 || c_len < 1) return 0;
-    PlanGeom g = make_geom(n, support, &g_size, 1, c_len, nullptr);
+    PlanGeom g = make_geom(n, support, &g_size, 1, c_len, nullptr, true);
     return plan_bytes(g, nullptr);
 }
 
@@ -478,7 +569,7 @@ size_t tcv_batch_workspace_bytes(const tcv_job* jobs, int n_jobs, int support, i
     std::vector<int> sides;
     int64_t n = 0;
     if (batch_args(jobs, n_jobs, support, c_len, tuning, sides, n) != TCV_OK) return 0;
-    PlanGeom g = make_geom(n, support, sides.data(), n_jobs, c_len, tuning);
+    PlanGeom g = make_geom(n, support, sides.data(), n_jobs, c_len, tuning, false);
     return plan_bytes(g, nullptr);
 }
 
@@ -492,7 +583,7 @@ tcv_status tcv_batch_plan_create(tcv_plan** plan_out, const tcv_job* jobs, int n
     if (s != TCV_OK) return s;
     tcv_plan* p = new (std::nothrow) tcv_plan{};
     if (!p) return TCV_ERR_OOM;
-    p->g = make_geom(n, support, sides.data(), n_jobs, c_len, tuning);
+    p->g = make_geom(n, support, sides.data(), n_jobs, c_len, tuning, false);
     if (!geom_supported(p->g)) {
         delete p;
         return TCV_ERR_UNSUPPORTED;
@@ -529,13 +620,14 @@ tcv_status tcv_plan_tuning(const tcv_plan* plan, tcv_tuning* tuning_out)
     if (!plan || !tuning_out) return TCV_ERR_ARG;
     tuning_out->tile_rows = plan->g.rows;
     tuning_out->group_mib = plan->g.group_mib;
+    tuning_out->split = plan->g.split;
     return TCV_OK;
 }
 
 size_t tcv_plan_workspace_bytes_tuned(int64_t n, int support, int g_size, int64_t c_len, const tcv_tuning* tuning)
 {
     if (n < 0 || support < 0 || g_size < 1 || c_len < 1 || !valid_tuning(tuning)) return 0;
-    PlanGeom g = make_geom(n, support, &g_size, 1, c_len, tuning);
+    PlanGeom g = make_geom(n, support, &g_size, 1, c_len, tuning, true);
     return plan_bytes(g, nullptr);
 }
 

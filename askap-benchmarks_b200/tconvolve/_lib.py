@@ -66,11 +66,37 @@ class TcvJob(ctypes.Structure):
 
 
 class TcvTuning(ctypes.Structure):
-    _fields_ = [("tile_rows", ctypes.c_int32), ("group_mib", ctypes.c_int32)]
+    _fields_ = [("tile_rows", ctypes.c_int32), ("group_mib", ctypes.c_int32), ("split", ctypes.c_int32)]
 
     def as_tuple(self):
-        return (int(self.tile_rows), int(self.group_mib))
+        return (int(self.tile_rows), int(self.group_mib), int(self.split))
 
+
+class TcvServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("g_size", ctypes.c_int32), ("w_size", ctypes.c_int32), ("cell_size", ctypes.c_double),
+        ("baseline", ctypes.c_int32), ("c_type", ctypes.c_int32), ("streams", ctypes.c_int32),
+        ("max_batch", ctypes.c_int32), ("batch_samples", ctypes.c_int64), ("hbm_budget", ctypes.c_size_t),
+        ("tuning", TcvTuning), ("device", ctypes.c_int32),
+    ]
+
+
+class TcvRequest(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32), ("grid", ctypes.c_int32), ("n", ctypes.c_int64),
+        ("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("w", ctypes.c_void_p),
+        ("vis", ctypes.c_void_p), ("vis_out", ctypes.c_void_p),
+    ]
+
+
+class TcvRequestInfo(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32), ("batch_requests", ctypes.c_int32), ("rejected", ctypes.c_int64),
+        ("t_submit", ctypes.c_double), ("t_start", ctypes.c_double), ("t_done", ctypes.c_double),
+    ]
+
+
+REQ_GRID, REQ_DEGRID = 0, 1
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -113,6 +139,16 @@ SIGNATURES = {
     "tcv_graph_capture": (_I, [_PP, _P, _I, _P, _P, _P, _P, _P, _I, _F, _P, _P]),
     "tcv_graph_launch": (_I, [_P, _P]),
     "tcv_graph_destroy": (None, [_P]),
+    "tcv_server_config_default": (None, [_P]),
+    "tcv_server_create": (_I, [_P, _PP]),
+    "tcv_server_destroy": (None, [_P]),
+    "tcv_server_grid_alloc": (_I, [_P, _P]),
+    "tcv_server_grid_free": (_I, [_P, _I]),
+    "tcv_server_grid_read": (_I, [_P, _I, _P]),
+    "tcv_server_grid_write": (_I, [_P, _I, _P]),
+    "tcv_server_submit": (_I, [_P, _P, _P]),
+    "tcv_server_wait": (_I, [_P, ctypes.c_uint64, _D, _P]),
+    "tcv_server_stats": (_I, [_P, _P, _P, _P, _P]),
     "tcv_jit_prepare": (_I, [_I, _I]),
     "tcv_jit_enable": (None, [_I]),
     "tcv_jit_info": (ctypes.c_char_p, []),

@@ -57,6 +57,8 @@ def parse_args():
                    help="degridding kernel on the direct path")
     p.add_argument("--no-tune", action="store_true", help="default tile shape and plane groups, no autotuning")
     p.add_argument("--no-batched", action="store_true", help="skip the 64-job batched measurement")
+    p.add_argument("--no-serving", action="store_true", help="skip the serving (Poisson arrivals) measurement")
+    p.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window per serving rate")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=4.0, help="target wall time of the CPU sample")
     return p.parse_args()
@@ -239,9 +241,9 @@ def b200_arm(args):
     L = lib()
     TcvTuning = tconvolve._lib.TcvTuning
     tuning = {"t": TcvTuning(*(tunings[args.form][0] if args.form in tunings else (16, 32)))}
-    wbytes = max(L.tcv_plan_workspace_bytes_tuned(n, support, prob.g_size, c_len, ctypes.byref(TcvTuning(r, m)))
-                 for r in (8, 16, 32) for m in (32,))
-    wbytes = max(wbytes, L.tcv_plan_workspace_bytes_tuned(n, support, prob.g_size, c_len, ctypes.byref(tuning["t"])))
+    # one workspace for every plan the bench builds (each measured form's tuning)
+    wbytes = max(L.tcv_plan_workspace_bytes_tuned(n, support, prob.g_size, c_len, ctypes.byref(TcvTuning(*t)))
+                 for t in [(16, 32, 0)] + [v[0] for v in tunings.values()])
     work = torch.empty(wbytes, dtype=torch.uint8, device="cuda")
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     sp = ctypes.c_void_p(stream.cuda_stream)
@@ -390,11 +392,16 @@ def b200_arm(args):
              ("degrid", "direct"): ("degrid_tile_kernel + slot_reduce_kernel" if args.degrid == "tiles"
                                     else "degrid_staged_kernel")}[(dom, args.path)]
 
-    batched = None
-    if not args.no_batched:
+    # the other workloads run after the headline's context is released
+    batched = serving = None
+    if not (args.no_batched and args.no_serving):
         b.close()
         torch.cuda.empty_cache()
+    if not args.no_batched:
         batched = batched_section(args, torch, stream, world)
+        torch.cuda.empty_cache()
+    if not args.no_serving:
+        serving = serving_section(args, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -415,6 +422,7 @@ def b200_arm(args):
                                 if args.form == "r32" else args.form),
                        "path": args.path, "degrid": args.degrid,
                        "tuning": {"tile_rows": tuning["t"].tile_rows, "group_mib": tuning["t"].group_mib,
+                                  "split": tuning["t"].split,
                                   "chosen_by": "autotuner (tcv_tune)" if tunings else "default"},
                        "parallelism": f"replicas x{world}",
                        "l2": f"{L2_FLUSH_BYTES >> 20} MiB buffer written between timed steps",
@@ -430,6 +438,7 @@ def b200_arm(args):
                         "degrid_updates_per_s": updates / (d_ms * 1e-3)},
             "plain_form": plain,
             "batched": batched,
+            "serving": serving,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * (8 + 4 * 3),
                     "d2h_bytes_per_step": n * 8, "ms_per_step": e2e_mean},
             "gpu_launches": launches_per_step * args.steps if launches_per_step else None,
@@ -441,8 +450,8 @@ def b200_arm(args):
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    if args.no_batched:
-        b.close()
+    if args.no_batched and args.no_serving:
+        b.close()  # not released above
     if world > 1:
         dist.destroy_process_group()
     return 0
@@ -524,6 +533,33 @@ def batched_section(args, torch, stream, world):
     res["rejected_note"] = ("samples whose footprint (rows iv..iv+128) leaves a 2048 grid; skipped and counted, "
                             "not in the update count")
     return res
+
+
+def serving_section(args, device):
+    """Serving: Poisson arrivals of gridding and degridding requests (half each) of 16000 samples
+    on the 1024^2-grid, 9-plane, 5 arcsec problem (32.4e6 updates each) at 50, 100, 200 and 500
+    requests/s, over 64 resident grids, under a 150 GB device-memory budget; latency is submission
+    to result-ready, measured by the server."""
+    from tconvolve.serve import Server, poisson_run, request_pool
+
+    srv = Server(c_type=args.form if args.form in ("r32", "c64", "rbf16", "cbf16") else "r32", streams=2,
+                 max_batch=32, batch_samples=32 * 16000, hbm_budget=150e9, device=device)
+    grids = [srv.grid_alloc() for _ in range(64)]
+    pool = request_pool(32, 16000, seed=7)
+    poisson_run(srv, rate=200, duration=0.3, pool=pool, grids=grids, seed=99)  # warm-up
+    upd = 16000 * 45 * 45
+    rates = []
+    for rate in (50, 100, 200, 500):
+        r = poisson_run(srv, rate=rate, duration=args.serve_seconds, pool=pool, grids=grids, seed=rate)
+        r["updates_per_s"] = r["throughput_req_s"] * upd if r["throughput_req_s"] else None
+        rates.append(r)
+    st = srv.stats()
+    srv.close()
+    return {"workload": "Poisson arrivals, half gridding / half degridding requests of 16000 samples "
+                        "(1024^2 grid, 9 w-planes, support 22: 32.4e6 updates each), 64 resident grids",
+            "form": args.form if args.form in ("r32", "c64", "rbf16", "cbf16") else "r32",
+            "hbm_budget_bytes": int(150e9), "bytes_held": st["bytes_held"], "slots": 2, "max_batch": 32,
+            "latency": "submission to result-ready (server clock)", "rates": rates}
 
 
 def count_step_kernels(torch, step):

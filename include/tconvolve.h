@@ -180,20 +180,24 @@ typedef struct tcv_job {
 } tcv_job;
 
 /* Tile shape and sort granularity of a plan (tcv_autotune chooses them by timing). */
-struct tcv_tuning {
+typedef struct tcv_tuning {
     int tile_rows; /* grid rows per warp of the tile kernels: 8, 16 or 32, i.e. tiles of
                       64 x 4*tile_rows points; 0 = 16 */
     int group_mib; /* table slice per plane group, MiB of complex64 (whole w-planes, at least
                       one); 0 = 32; -1 = the whole table in one group */
-};
+    int split;     /* cells of at least 2*split samples are split into work units of about
+                      split samples, so that a plan with few busy tiles still fills the GPU
+                      (gridding units write partial tiles that are folded into the grid in unit
+                      order); 0 = cells are never split */
+} tcv_tuning;
 
 /* Workspace of a batched plan (0 for invalid arguments).  tuning may be NULL (defaults). */
 size_t tcv_batch_workspace_bytes(const tcv_job *jobs, int n_jobs, int support, int64_t c_len,
                                  const tcv_tuning *tuning);
-/* Create a batched plan in d_work: copies the job table to the device and numbers the jobs'
- * tiles.  Set-up path (the job table is copied from host memory, so do not capture this call);
- * bin the samples with tcv_plan_bin.  Gridding and degridding take d_grid = NULL and use the
- * jobs' grids. */
+/* Create a batched plan in d_work: writes the job table to the device and numbers the jobs'
+ * tiles.  Up to 128 jobs the table travels as a kernel argument (device work only, capturable);
+ * beyond that it is copied from host memory (set-up path, not capturable).  Bin the samples with
+ * tcv_plan_bin.  Gridding and degridding take d_grid = NULL and use the jobs' grids. */
 tcv_status tcv_batch_plan_create(tcv_plan **plan_out, const tcv_job *jobs, int n_jobs, int support,
                                  int64_t c_len, const tcv_tuning *tuning, void *d_work,
                                  size_t work_bytes, void *stream);
@@ -231,10 +235,75 @@ tcv_status tcv_graph_capture(tcv_graph **graph_out, tcv_plan *plan, int passes,
 tcv_status tcv_graph_launch(const tcv_graph *graph, void *stream);
 void tcv_graph_destroy(tcv_graph *graph);
 
-/* A one-job plan with a chosen tile shape and sort granularity (tcv_tuning, below; NULL for the
+/* ------------------------------------------------------------------------------------------
+ * Serving: a request loop with continuous batching.  The server keeps the table and the grids
+ * resident on one GPU; gridding and degridding requests (u, v, w in metres and visibilities in
+ * host memory, one channel at the reference's first frequency, Benchmark.cc:89) queue on
+ * submission, and a scheduler thread forms a batch whenever one of `streams` batch slots is
+ * free: pending requests in arrival order, up to max_batch requests and batch_samples samples,
+ * at most one request per grid per batch, requests on one grid in submission order (a grid with
+ * a request in flight waits).  Each batch runs as batched plans (above) on its slot's stream, so
+ * requests that arrive while others are on the GPU are admitted as slots free up and their work
+ * overlaps.  Device memory is admitted against hbm_budget: the table, every batch slot's
+ * buffers and every grid; a grid allocation that would exceed it fails with TCV_ERR_OOM.
+ * A request's result is the same alone and in any mix (bit-identical: a job's sums do not
+ * depend on the other jobs of its batch).  No counterpart in the reference, whose benchmark runs
+ * one fixed problem per process (attic/tConvolveMPI/tConvolveMPI.cc:78-119).
+ * ---------------------------------------------------------------------------------------- */
+typedef struct tcv_server_config {
+    int32_t g_size;        /* side of the served grids */
+    int32_t w_size;        /* w-planes of the table (Benchmark::initC) */
+    double cell_size;      /* cellSize in wavelengths */
+    int32_t baseline;      /* metres */
+    int32_t c_type;        /* table form the requests run with (TCV_C_R32 / TCV_C_C64 / ...) */
+    int32_t streams;       /* batch slots in flight (default 2) */
+    int32_t max_batch;     /* requests per batch (default 32, at most 128) */
+    int64_t batch_samples; /* samples per batch; also the largest request (default 262144) */
+    size_t hbm_budget;     /* device bytes the server may hold (default 150e9) */
+    tcv_tuning tuning;     /* tile shape / plane groups ({0, 0}: defaults) */
+    int32_t device;
+} tcv_server_config;
+
+enum { TCV_REQ_GRID = 0, TCV_REQ_DEGRID = 1 };
+typedef struct tcv_request {
+    int32_t kind;          /* TCV_REQ_GRID: grid += gridding of vis; TCV_REQ_DEGRID: vis_out = degridding */
+    int32_t grid;          /* a grid id from tcv_server_grid_alloc */
+    int64_t n;             /* samples (<= batch_samples) */
+    const double *u, *v, *w; /* n positions in metres (host); must stay valid until the request completes */
+    const float *vis;      /* TCV_REQ_GRID: n complex64 (host), valid until completion */
+    float *vis_out;        /* TCV_REQ_DEGRID: n complex64 (host), written when the request completes */
+} tcv_request;
+
+typedef struct tcv_request_info {
+    int32_t status;        /* tcv_status of the request */
+    int32_t batch_requests;/* requests in the batch it ran in */
+    int64_t rejected;      /* samples of its batch (all requests) left out as out of bounds */
+    double t_submit, t_start, t_done; /* seconds since the server started: submission, batch
+                                         launch, result ready (outputs on the host) */
+} tcv_request_info;
+
+typedef struct tcv_server tcv_server;
+void tcv_server_config_default(tcv_server_config *cfg);
+/* Allocates the table and the batch slots, starts the scheduler. */
+tcv_status tcv_server_create(const tcv_server_config *cfg, tcv_server **out);
+/* Drains the queue (every submitted request completes), stops the threads, frees everything. */
+void tcv_server_destroy(tcv_server *srv);
+tcv_status tcv_server_grid_alloc(tcv_server *srv, int32_t *grid_out);   /* a zeroed resident grid */
+tcv_status tcv_server_grid_free(tcv_server *srv, int32_t grid);         /* after its requests */
+tcv_status tcv_server_grid_read(tcv_server *srv, int32_t grid, float *host); /* waits for its requests */
+tcv_status tcv_server_grid_write(tcv_server *srv, int32_t grid, const float *host);
+/* Queue a request; *ticket_out identifies it.  TCV_ERR_UNSUPPORTED if n > batch_samples. */
+tcv_status tcv_server_submit(tcv_server *srv, const tcv_request *req, uint64_t *ticket_out);
+/* Wait up to timeout_s (< 0: no limit) for a request; TCV_ERR_TIMEOUT if it has not completed.
+ * A completed request's info is returned (info may be NULL) and the ticket is released. */
+tcv_status tcv_server_wait(tcv_server *srv, uint64_t ticket, double timeout_s, tcv_request_info *info);
+/* Device bytes held (table + slots + grids), and counters. */
+tcv_status tcv_server_stats(const tcv_server *srv, size_t *bytes_held, int64_t *completed,
+                            int64_t *batches, int64_t *pending);
+
+/* A one-job plan with a chosen tile shape and sort granularity (tcv_tuning, above; NULL for the
  * defaults, which tcv_plan_workspace_bytes / tcv_plan_build use).  The TMA pipeline and paired
  * kernel families need the default tile shape (TCV_ERR_UNSUPPORTED otherwise). */
-typedef struct tcv_tuning tcv_tuning;
 size_t tcv_plan_workspace_bytes_tuned(int64_t n, int support, int g_size, int64_t c_len,
                                       const tcv_tuning *tuning);
 tcv_status tcv_plan_build_tuned(tcv_plan **plan_out, const int32_t *d_iu, const int32_t *d_iv,

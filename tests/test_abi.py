@@ -160,3 +160,40 @@ def test_batch_geometry_limits(tcv):
     work = ctypes.c_void_p(256)
     assert L.tcv_batch_plan_create(ctypes.byref(plan), many, 1025, 3, 7 * 7 * 64, None, work, 1 << 40,
                                    None) == 8  # TCV_ERR_UNSUPPORTED
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/tconvolve.h compiles as C99 (the boundary is a C ABI, bindable from cgo/JNI/ctypes)."""
+    src = tmp_path / "use.c"
+    src.write_text('#include "tconvolve.h"\nint main(void) { tcv_server_config c; tcv_tuning t = {16, 32};\n'
+                   '  c.tuning = t; return (int)sizeof(tcv_request) + c.tuning.tile_rows * 0; }\n')
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(REPO, "include"),
+                    str(src)], check=True)
+
+
+def test_server_argument_validation(tcv):
+    import torch
+
+    from tconvolve._lib import TcvRequest, TcvServerConfig
+
+    L = tcv.lib()
+    cfg = TcvServerConfig()
+    L.tcv_server_config_default(ctypes.byref(cfg))
+    assert (cfg.g_size, cfg.w_size, cfg.baseline, cfg.streams, cfg.max_batch) == (1024, 9, 2000, 2, 32)
+    assert cfg.hbm_budget == int(150e9) and cfg.c_type == 1  # TCV_C_R32
+    srv = ctypes.c_void_p()
+    for field, value in [("streams", 9), ("max_batch", 129), ("g_size", 1), ("c_type", 0x100), ("batch_samples", -1)]:
+        bad = TcvServerConfig()
+        L.tcv_server_config_default(ctypes.byref(bad))
+        setattr(bad, field, value)
+        assert L.tcv_server_create(ctypes.byref(bad), ctypes.byref(srv)) == 1, field
+    assert L.tcv_server_create(None, ctypes.byref(srv)) == 1
+    req = TcvRequest()
+    t = ctypes.c_uint64()
+    assert L.tcv_server_submit(None, ctypes.byref(req), ctypes.byref(t)) == 1
+    assert L.tcv_server_wait(None, 1, 0.0, None) == 1
+    assert L.tcv_server_stats(None, None, None, None, None) == 1
+    assert L.tcv_server_grid_alloc(None, None) == 1
+    if not torch.cuda.is_available():
+        # a valid configuration needs the GPU: no CPU fallback
+        assert L.tcv_server_create(ctypes.byref(cfg), ctypes.byref(srv)) == 4  # TCV_ERR_CUDA
