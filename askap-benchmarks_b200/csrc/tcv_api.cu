@@ -30,7 +30,7 @@ struct tcv_ctx {
     size_t work_bytes = 0;
     void* c_scratch = nullptr;
     tcv_plan* plan = nullptr;
-    tcv_tuning tuning{16, 32, 0};
+    tcv_tuning tuning{16, 32, 0, 0};
     bool initialized = false;
     std::string err;
 };
@@ -328,8 +328,10 @@ int tcv_get_path(const tcv_ctx* c) { return c ? c->path : -1; }
 tcv_status tcv_set_tuning(tcv_ctx* c, const tcv_tuning* t)
 {
     if (!c || !t) return TCV_ERR_ARG;
-    const tcv_tuning nt{t->tile_rows ? t->tile_rows : 16, t->group_mib ? t->group_mib : 32, t->split};
-    if ((nt.tile_rows != 8 && nt.tile_rows != 16 && nt.tile_rows != 32) || nt.group_mib < -1 || nt.split < 0)
+    const tcv_tuning nt{t->tile_rows ? t->tile_rows : 16, t->group_mib ? t->group_mib : 32, t->split,
+                        t->degrid_split};
+    if ((nt.tile_rows != 8 && nt.tile_rows != 16 && nt.tile_rows != 32) || nt.group_mib < -1 || nt.split < 0 ||
+        nt.degrid_split < 0)
         return TCV_ERR_ARG;
     const tcv_tuning prev = c->tuning;
     c->tuning = nt;
@@ -356,7 +358,7 @@ tcv_status tcv_tune(tcv_ctx* c, int reps, tcv_tuning* best_out, float* best_ms_o
     if (!c->initialized) return fail(c, TCV_ERR_STATE, "tune before init");
     if (c->path != TCV_PATH_DIRECT) return fail(c, TCV_ERR_UNSUPPORTED, "tuning needs the direct path");
     const tcv_job job{c->n_data, c->cfg.g_size, reinterpret_cast<float*>(c->grid)};
-    tcv_tuning best{16, 32, 0};
+    tcv_tuning best{16, 32, 0, 0};
     float ms = 0.f;
     CTX_TRY(c, tcv_autotune(&job, 1, c->iu, c->iv, c->coff, reinterpret_cast<const float*>(c->data), active_table(c),
                             active_code(c), active_scale(c), c->c_len, c->support, reps, &best, &ms, c->stream));

@@ -5,7 +5,8 @@
 // degridding + the slot sum) is a few dozen launches; captured once into a CUDA graph it is
 // replayed with one launch and no host work.  The autotuner times the candidate tunings
 // (rows per warp 8/16/32, i.e. tiles of 64 x 32/64/128 points, and plane-group slices of
-// 8/16/32/64 MiB or the whole table; then work units of 512/256/128/64 samples for busy cells)
+// 8/16/32/64 MiB or the whole table; then gridding and degridding work units of 512/256/128/64
+// samples for busy cells)
 // on the caller's own batch, into scratch grids, and keeps the fastest.  Neither has a
 // counterpart in the reference, whose kernels run one job per call
 // (attic/tConvolveMPI/Benchmark.cc:98-106).
@@ -198,7 +199,7 @@ tcv_status tcv_autotune(const tcv_job* jobs, int n_jobs, const int32_t* d_iu, co
     }();
     for (int rows : {16, 8, 32})
         for (int mib : {32, 16, 64, 8, -1}) {
-            const tcv_tuning t{rows, mib, 0};
+            const tcv_tuning t{rows, mib, 0, 0};
             const PlanGeom g = make_geom(n_sub, support, &gs_max, 1, c_len, &t, false);
             const std::pair<int, int> id(rows, g.kid_group);
             if (std::find(seen.begin(), seen.end(), id) != seen.end()) continue;
@@ -213,7 +214,7 @@ tcv_status tcv_autotune(const tcv_job* jobs, int n_jobs, const int32_t* d_iu, co
         return TCV_ERR_CUDA;
     }
     std::vector<std::pair<tcv_tuning, float>> report;
-    tcv_tuning best{16, 32, 0};
+    tcv_tuning best{16, 32, 0, 0};
     float best_ms = -1.f;
     size_t have = 0;
     auto time_one = [&](const tcv_tuning& t) -> tcv_status {
@@ -256,10 +257,15 @@ tcv_status tcv_autotune(const tcv_job* jobs, int n_jobs, const int32_t* d_iu, co
     };
     for (const tcv_tuning& t : cands)
         if ((s = time_one(t)) != TCV_OK) break;
-    if (s == TCV_OK) {
+    if (s == TCV_OK) {  // stage 2: gridding units
         const tcv_tuning base = best;
         for (int split : {512, 256, 128, 64})
-            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, split})) != TCV_OK) break;
+            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, split, 0})) != TCV_OK) break;
+    }
+    if (s == TCV_OK) {  // stage 3: degridding units
+        const tcv_tuning base = best;
+        for (int split : {512, 256, 128, 64})
+            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, base.split, split})) != TCV_OK) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

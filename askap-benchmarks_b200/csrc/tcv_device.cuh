@@ -267,8 +267,9 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
 
 // Degridding on the gridding plan (the adjoint of grid_tile_kernel).  A lane holds its kR grid
 // points in registers; for each sample of the cell a warp whose block meets the footprint forms
-// the partial dot product of its block with the table, reduces it with shuffles, and the CTA
-// adds its 8 warp partials in warp order into the sample's slot for this tile.  A final pass
+// the partial dot product of its block with the table, four samples at a time reduced together
+// with shuffles, and the CTA adds its 8 warp partials in warp order into the sample's slot for
+// this tile.  A final pass
 // (slot_reduce_kernel) adds each sample's tile slots in tile order: no atomics, deterministic.
 template <class Tab, int kS, int kR>
 __global__ void __launch_bounds__(kTileThreads, degrid_min_blocks<kR>())
@@ -308,40 +309,60 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                 sm_rec[threadIdx.x] = make_int4(int(k), iu[k] - a.support, iv[k], coff[k]);
             }
             __syncthreads();
-            for (int j = 0; j < m; ++j) {
-                const int4 q = sm_rec[j];
-                const int fx = q.y, fy = q.z;
-                const int dy0 = gy0 - fy;
-                float2 v = make_float2(0.f, 0.f);
-                if (!(dy0 >= s || dy0 + kR <= 0) && !(fx > bx0 + 31 || fx + s <= bx0)) {  // warp-uniform
+            // four samples at a time: each lane's partial dot products of the four, then one
+            // transposing warp reduction for all of them (6 complex shuffles instead of 20)
+            for (int jg = 0; jg < m; jg += 4) {
+                float2 v[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    v[e] = make_float2(0.f, 0.f);
+                    const int j = jg + e;
+                    if (j >= m) continue;  // warp-uniform
+                    const int4 q = sm_rec[j];
+                    const int fx = q.y, fy = q.z;
+                    const int dy0 = gy0 - fy;
+                    if (dy0 >= s || dy0 + kR <= 0 || fx > bx0 + 31 || fx + s <= bx0) continue;  // warp-uniform
                     const int dx = gx - fx;
                     const bool colok = unsigned(dx) < unsigned(s);
                     const int ci = q.w + dy0 * s + dx;
-                    // four independent partial sums keep the FMA chains short
-                    float2 pv[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
-                                    make_float2(0.f, 0.f)};
+                    float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);  // two FMA chains
                     if (dy0 >= 0 && dy0 + kR <= s) {
                         if (colok) {
 #pragma unroll
-                            for (int r = 0; r < kR; ++r) cmac<Tab::kReal>(pv[r & 3], gv[r], Tab::load(ctab + (ci + r * s)));
+                            for (int r = 0; r < kR; r += 2) {
+                                cmac<Tab::kReal>(p0, gv[r], Tab::load(ctab + (ci + r * s)));
+                                cmac<Tab::kReal>(p1, gv[r + 1], Tab::load(ctab + (ci + (r + 1) * s)));
+                            }
                         }
                     } else {
 #pragma unroll
                         for (int r = 0; r < kR; ++r) {
-                            if (colok && unsigned(dy0 + r) < unsigned(s)) {
-                                const float2 c = Tab::load(ctab + (ci + r * s));
-                                cmac<Tab::kReal>(pv[r & 3], gv[r], c);
-                            }
+                            if (colok && unsigned(dy0 + r) < unsigned(s))
+                                cmac<Tab::kReal>((r & 1) ? p1 : p0, gv[r], Tab::load(ctab + (ci + r * s)));
                         }
                     }
-                    v = make_float2((pv[0].x + pv[1].x) + (pv[2].x + pv[3].x), (pv[0].y + pv[1].y) + (pv[2].y + pv[3].y));
-#pragma unroll
-                    for (int o = 16; o; o >>= 1) {
-                        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-                        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-                    }
+                    v[e] = make_float2(p0.x + p1.x, p0.y + p1.y);
                 }
-                if (lane == 0) sm_part[j][warp] = v;
+                // exchange over lane bit 4 (lanes keep samples 0,1 or 2,3) and bit 3 (one sample
+                // each): lane holds sample (lane >> 3) & 3 summed over 4 lanes; butterflies over
+                // bits 2..0 finish the sum
+                const bool h16 = (lane & 16) != 0, h8 = (lane & 8) != 0;
+                const float2 s0 = h16 ? v[0] : v[2], k0 = h16 ? v[2] : v[0];
+                const float2 s1 = h16 ? v[1] : v[3], k1 = h16 ? v[3] : v[1];
+                const float2 w0 = make_float2(k0.x + __shfl_xor_sync(0xffffffffu, s0.x, 16),
+                                              k0.y + __shfl_xor_sync(0xffffffffu, s0.y, 16));
+                const float2 w1 = make_float2(k1.x + __shfl_xor_sync(0xffffffffu, s1.x, 16),
+                                              k1.y + __shfl_xor_sync(0xffffffffu, s1.y, 16));
+                const float2 sd = h8 ? w0 : w1, kp = h8 ? w1 : w0;
+                float2 y = make_float2(kp.x + __shfl_xor_sync(0xffffffffu, sd.x, 8),
+                                       kp.y + __shfl_xor_sync(0xffffffffu, sd.y, 8));
+#pragma unroll
+                for (int o = 4; o; o >>= 1) {
+                    y.x += __shfl_xor_sync(0xffffffffu, y.x, o);
+                    y.y += __shfl_xor_sync(0xffffffffu, y.y, o);
+                }
+                const int js = jg + (lane >> 3);
+                if ((lane & 7) == 0 && js < m) sm_part[js][warp] = y;
             }
             __syncthreads();
             if (threadIdx.x < m) {

@@ -90,8 +90,8 @@ tcv_status launch_adjoint(const tcv_plan* p, const float2* grid, const void* c, 
     for (int grp = 0; grp < g.n_groups; ++grp) {
         GridArgs a = make_args(p, grp, c_scale, gridp);
         void* args[] = {&tab, const_cast<const int32_t**>(&p->iu), const_cast<const int32_t**>(&p->iv),
-                        const_cast<const int32_t**>(&p->coff), &order, const_cast<uint4**>(&p->units),
-                        const_cast<uint32_t**>(&p->group_ustart), const_cast<float2**>(&p->slots), &max_tiles, &a};
+                        const_cast<const int32_t**>(&p->coff), &order, const_cast<uint4**>(&p->d_units),
+                        const_cast<uint32_t**>(&p->d_group_ustart), const_cast<float2**>(&p->slots), &max_tiles, &a};
         TCV_CUDA(cudaLaunchKernel(kernel, dim3(ctas), dim3(kTileThreads), args, 0, st));
     }
     return slot_reduce(p, c_scale, out, st);

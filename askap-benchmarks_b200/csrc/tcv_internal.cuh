@@ -43,7 +43,8 @@ struct PlanGeom {
     // gridding: output-stationary tiles of tw x th points (th = 4 * rows); work cells are
     // (group, tile) with the tiles of all jobs numbered in one space
     int rows, tw, th;
-    int split;          // samples per work unit of a split cell (0: cells are never split)
+    int split;          // samples per gridding work unit of a split cell (0: cells are never split)
+    int dsplit;         // the same for degridding
     int ntx, nty;       // tiles per row / column of a one-job plan
     int64_t ntiles;     // tiles of all jobs
     int max_tiles;      // tiles one footprint can touch
@@ -82,6 +83,9 @@ struct tcv_plan {
     uint32_t* pstart;              // per item: its first partial tile (split cells)
     uint4* units;                  // work units (cell, first sorted pair, count, partial tile or kDirect)
     float2* partial;               // partial tiles of split cells, tw x th points each
+    uint4* d_units;                // degridding work units (the gridding list when the sizes agree)
+    uint32_t* d_group_ustart;
+    uint32_t *d_nunits, *d_ustart, *d_pstart;
     uint32_t* atile_count;         // samples per anchor cell (group, anchor tile)
     uint32_t* atile_start;
     uint32_t* aitems;              // non-empty anchor cells, group-major

@@ -15,9 +15,10 @@
 // into work lists (with per-group ranges) that persistent kernels walk.
 // A plan may hold several jobs sharing the table (a batch): their tiles are numbered in one
 // space, job after job, so one sort and one sequence of launches covers all of them.
-// Cells with many samples are split into work units of about `split` samples (the units of a
-// gridding cell write partial tiles that a fold adds into the grid in unit order), so that a
-// plan with few busy tiles still spreads over every SM.
+// Cells with many samples are split into work units of about `split` samples for gridding (the
+// units of a cell write partial tiles that a fold adds into the grid in unit order) and of about
+// `dsplit` samples for degridding (units are independent there), so that a plan with few busy
+// tiles still spreads over every SM.
 // Samples whose footprint or table range falls outside their grid or the table are counted and
 // left out (sentinel key, sorted past the end).
 #include "tcv_internal.cuh"
@@ -198,11 +199,9 @@ __global__ void unit_expand_kernel(const uint32_t* __restrict__ items, const uin
     }
 }
 
-// group_start[g] = first item whose cell belongs to group g or later (items are sorted), and
-// group_ustart[g] the first unit of that item
+// group_start[g] = first item whose cell belongs to group g or later (items are sorted)
 __global__ void group_ranges_kernel(const uint32_t* items, const uint32_t* n_items, int n_groups,
-                                    uint32_t cells_per_group, const uint32_t* nunits, const uint32_t* ustart,
-                                    uint32_t* group_start, uint32_t* group_ustart)
+                                    uint32_t cells_per_group, uint32_t* group_start)
 {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g > n_groups) return;
@@ -217,6 +216,15 @@ __global__ void group_ranges_kernel(const uint32_t* items, const uint32_t* n_ite
             hi = mid;
     }
     group_start[g] = lo;
+}
+
+// group_ustart[g] = the first unit of group g's first item
+__global__ void group_units_kernel(const uint32_t* group_start, const uint32_t* n_items, int n_groups,
+                                   const uint32_t* nunits, const uint32_t* ustart, uint32_t* group_ustart)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g > n_groups) return;
+    const uint32_t lo = group_start[g], n = *n_items;
     group_ustart[g] = lo < n ? ustart[lo] : (n ? ustart[n - 1] + nunits[n - 1] : 0);
 }
 
@@ -225,8 +233,9 @@ inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 inline size_t grid_cells(const PlanGeom& g) { return size_t(g.n_groups) * size_t(g.ntiles); }
 // a split cell of cnt >= 2*split samples makes floor(cnt/split) units, so the units of split cells
 // number at most pairs/split, and every other non-empty cell makes one
-inline size_t max_partials(const PlanGeom& g) { return g.split ? size_t(g.n) * g.max_tiles / size_t(g.split) : 0; }
-inline size_t max_units(const PlanGeom& g) { return grid_cells(g) + max_partials(g); }
+inline size_t max_partials(const PlanGeom& g, int split) { return split ? size_t(g.n) * g.max_tiles / size_t(split) : 0; }
+inline size_t max_units(const PlanGeom& g, int split) { return grid_cells(g) + max_partials(g, split); }
+inline bool own_degrid_units(const PlanGeom& g) { return g.dsplit != g.split; }
 inline size_t anchor_cells(const PlanGeom& g) { return g.anchors ? size_t(g.n_groups) * g.natx * g.naty : 0; }
 
 template <typename K>
@@ -248,6 +257,34 @@ size_t cub_temp_bytes(const PlanGeom& g)
         cub::DeviceSelect::Flagged(nullptr, f, it, fl, (uint32_t*)nullptr, (uint32_t*)nullptr, acells);
     }
     return std::max(std::max(std::max(a, b), std::max(c, d)), std::max(e, f));
+}
+
+#define TCV_CHECK(call)                    \
+    do {                                   \
+        const tcv_status _s = (call);      \
+        if (_s != TCV_OK) return _s;       \
+    } while (0)
+
+// the unit list of one unit size over the plan's non-empty cells, with its per-group ranges
+tcv_status build_units(tcv_plan* p, int split, uint32_t* nunits, uint32_t* ustart, uint32_t* pstart, uint4* units,
+                       uint32_t* group_ustart, cudaStream_t st)
+{
+    const PlanGeom& g = p->g;
+    const int cells = int(grid_cells(g));
+    unit_count_kernel<<<unsigned((cells + 255) / 256), 256, 0, st>>>(p->items, p->n_items, p->tile_count,
+                                                                      uint32_t(cells), uint32_t(split), nunits, pstart);
+    TCV_CUDA(cudaGetLastError());
+    size_t tb = p->cub_bytes;
+    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, nunits, ustart, cells, st));
+    tb = p->cub_bytes;
+    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, pstart, pstart, cells, st));
+    unit_expand_kernel<<<unsigned((cells + 255) / 256), 256, 0, st>>>(p->items, p->n_items, p->tile_count,
+                                                                       p->tile_start, nunits, ustart, pstart, units);
+    TCV_CUDA(cudaGetLastError());
+    group_units_kernel<<<(g.n_groups + 1 + 127) / 128, 128, 0, st>>>(p->group_start, p->n_items, g.n_groups, nunits,
+                                                                      ustart, group_ustart);
+    TCV_CUDA(cudaGetLastError());
+    return TCV_OK;
 }
 
 template <typename K>
@@ -294,23 +331,13 @@ tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_
         tb = p->cub_bytes;
         TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, afl, p->aitems, p->n_aitems, acells, st));
     }
-    // work units
-    unit_count_kernel<<<unsigned((cells + 255) / 256), 256, 0, st>>>(p->items, p->n_items, p->tile_count,
-                                                                      uint32_t(cells), uint32_t(g.split), p->nunits,
-                                                                      p->pstart);
-    TCV_CUDA(cudaGetLastError());
-    tb = p->cub_bytes;
-    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->nunits, p->ustart, cells, st));
-    tb = p->cub_bytes;
-    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->pstart, p->pstart, cells, st));
-    unit_expand_kernel<<<unsigned((cells + 255) / 256), 256, 0, st>>>(p->items, p->n_items, p->tile_count,
-                                                                       p->tile_start, p->nunits, p->ustart, p->pstart,
-                                                                       p->units);
-    TCV_CUDA(cudaGetLastError());
     group_ranges_kernel<<<(g.n_groups + 1 + 127) / 128, 128, 0, st>>>(p->items, p->n_items, g.n_groups,
-                                                                       uint32_t(g.ntiles), p->nunits, p->ustart,
-                                                                       p->group_start, p->group_ustart);
+                                                                       uint32_t(g.ntiles), p->group_start);
     TCV_CUDA(cudaGetLastError());
+    // work units: the gridding list, and the degridding list when its unit size differs
+    TCV_CHECK(build_units(p, g.split, p->nunits, p->ustart, p->pstart, p->units, p->group_ustart, st));
+    if (own_degrid_units(g))
+        TCV_CHECK(build_units(p, g.dsplit, p->d_nunits, p->d_ustart, p->d_pstart, p->d_units, p->d_group_ustart, st));
     return TCV_OK;
 }
 
@@ -318,7 +345,8 @@ bool valid_tuning(const tcv_tuning* t)
 {
     if (!t) return true;
     const bool rows_ok = t->tile_rows == 0 || t->tile_rows == 8 || t->tile_rows == 16 || t->tile_rows == 32;
-    return rows_ok && t->group_mib >= -1 && t->split >= 0 && t->split <= (1 << 24);
+    return rows_ok && t->group_mib >= -1 && t->split >= 0 && t->split <= (1 << 24) && t->degrid_split >= 0 &&
+           t->degrid_split <= (1 << 24);
 }
 
 // Lay the plan's arrays out in d_work and write the job table: from host memory for a batch,
@@ -360,8 +388,18 @@ tcv_status plan_create(tcv_plan* p, void* d_work, size_t work_bytes, cudaStream_
     p->nunits = static_cast<uint32_t*>(take(cells * 4));
     p->ustart = static_cast<uint32_t*>(take(cells * 4));
     p->pstart = static_cast<uint32_t*>(take(cells * 4));
-    p->units = static_cast<uint4*>(take(max_units(g) * sizeof(uint4)));
-    p->partial = static_cast<float2*>(take(max_partials(g) * size_t(g.tw) * g.th * sizeof(float2)));
+    p->units = static_cast<uint4*>(take(max_units(g, g.split) * sizeof(uint4)));
+    p->partial = static_cast<float2*>(take(max_partials(g, g.split) * size_t(g.tw) * g.th * sizeof(float2)));
+    if (own_degrid_units(g)) {
+        p->d_group_ustart = static_cast<uint32_t*>(take(size_t(g.n_groups + 1) * 4));
+        p->d_nunits = static_cast<uint32_t*>(take(cells * 4));
+        p->d_ustart = static_cast<uint32_t*>(take(cells * 4));
+        p->d_pstart = static_cast<uint32_t*>(take(cells * 4));
+        p->d_units = static_cast<uint4*>(take(max_units(g, g.dsplit) * sizeof(uint4)));
+    } else {
+        p->d_group_ustart = p->group_ustart;
+        p->d_units = p->units;
+    }
     p->atile_count = static_cast<uint32_t*>(take(acells * 4));
     p->atile_start = static_cast<uint32_t*>(take(acells * 4));
     p->aitems = static_cast<uint32_t*>(take(acells * 4));
@@ -403,7 +441,7 @@ bool geom_supported(const PlanGeom& g)
     if (g.n * g.max_tiles >= (int64_t(1) << 31)) return false;
     if (int64_t(g.n_groups) * g.ntiles >= (int64_t(1) << 31)) return false;
     if (g.max_tiles > 65535) return false;
-    if (max_units(g) >= (size_t(1) << 31)) return false;
+    if (max_units(g, g.split) >= (size_t(1) << 31) || max_units(g, g.dsplit) >= (size_t(1) << 31)) return false;
     return true;
 }
 
@@ -443,6 +481,7 @@ PlanGeom make_geom(int64_t n, int support, const int* g_sizes, int n_jobs, int64
     g.group_bits = bits_for(uint64_t(g.n_groups - 1));
     g.rows = (t && t->tile_rows) ? t->tile_rows : 16;
     g.split = t ? t->split : 0;
+    g.dsplit = t ? t->degrid_split : 0;
     g.tw = kTileW;
     g.th = tile_height(g.rows);
     g.ntiles = 0;
@@ -495,8 +534,11 @@ size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out)
     b += 2 * align_up(an * ks) + 2 * align_up(an * 4);
     const size_t cells = grid_cells(g), acells = anchor_cells(g);
     b += 3 * align_up(cells * 4) + align_up(4) + align_up(size_t(g.n_groups + 1) * 4);
-    b += align_up(size_t(g.n_groups + 1) * 4) + 3 * align_up(cells * 4) + align_up(max_units(g) * sizeof(uint4));
-    b += align_up(max_partials(g) * size_t(g.tw) * g.th * sizeof(float2));
+    b += align_up(size_t(g.n_groups + 1) * 4) + 3 * align_up(cells * 4) + align_up(max_units(g, g.split) * sizeof(uint4));
+    b += align_up(max_partials(g, g.split) * size_t(g.tw) * g.th * sizeof(float2));
+    if (own_degrid_units(g))
+        b += align_up(size_t(g.n_groups + 1) * 4) + 3 * align_up(cells * 4) +
+             align_up(max_units(g, g.dsplit) * sizeof(uint4));
     b += 3 * align_up(acells * 4) + align_up(4);
     b += align_up(sizeof(unsigned long long)) + align_up(sizeof(unsigned int));
     b += align_up(np * sizeof(float2));
@@ -621,6 +663,7 @@ tcv_status tcv_plan_tuning(const tcv_plan* plan, tcv_tuning* tuning_out)
     tuning_out->tile_rows = plan->g.rows;
     tuning_out->group_mib = plan->g.group_mib;
     tuning_out->split = plan->g.split;
+    tuning_out->degrid_split = plan->g.dsplit;
     return TCV_OK;
 }
 

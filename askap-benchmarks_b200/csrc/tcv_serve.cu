@@ -334,7 +334,7 @@ void tcv_server_config_default(tcv_server_config* c)
     c->max_batch = 32;
     c->batch_samples = 262144;
     c->hbm_budget = size_t(150e9);
-    c->tuning = tcv_tuning{16, 32, 64};
+    c->tuning = tcv_tuning{16, 32, 64, 64};
     c->device = 0;
 }
 
@@ -354,7 +354,7 @@ tcv_status tcv_server_create(const tcv_server_config* cfg, tcv_server** out)
         c.max_batch < 1 || c.max_batch > 128 || c.batch_samples < 1 || c.batch_samples > (int64_t(1) << 26) ||
         tcv_ctype_bytes(ct) == 0 || (ct & (TCV_C_PADDED | TCV_C_PAIRED)) ||
         (c.tuning.tile_rows != 8 && c.tuning.tile_rows != 16 && c.tuning.tile_rows != 32) || c.tuning.group_mib < -1 ||
-        c.tuning.split < 0)
+        c.tuning.split < 0 || c.tuning.degrid_split < 0)
         return TCV_ERR_ARG;
     tcv_server* s = new (std::nothrow) tcv_server;
     if (!s) return TCV_ERR_OOM;

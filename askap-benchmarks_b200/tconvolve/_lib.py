@@ -66,10 +66,11 @@ class TcvJob(ctypes.Structure):
 
 
 class TcvTuning(ctypes.Structure):
-    _fields_ = [("tile_rows", ctypes.c_int32), ("group_mib", ctypes.c_int32), ("split", ctypes.c_int32)]
+    _fields_ = [("tile_rows", ctypes.c_int32), ("group_mib", ctypes.c_int32), ("split", ctypes.c_int32),
+                ("degrid_split", ctypes.c_int32)]
 
     def as_tuple(self):
-        return (int(self.tile_rows), int(self.group_mib), int(self.split))
+        return (int(self.tile_rows), int(self.group_mib), int(self.split), int(self.degrid_split))
 
 
 class TcvServerConfig(ctypes.Structure):

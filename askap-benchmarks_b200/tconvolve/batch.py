@@ -29,8 +29,8 @@ def _tuning(t):
         return None
     if isinstance(t, TcvTuning):
         return t
-    rows, mib, split = (tuple(t) + (0,))[:3]
-    return TcvTuning(int(rows), int(mib), int(split))
+    rows, mib, split, dsplit = (tuple(t) + (0, 0))[:4]
+    return TcvTuning(int(rows), int(mib), int(split), int(dsplit))
 
 
 def table_len(c, c_type: int) -> int:
@@ -132,8 +132,8 @@ class Batch:
 
 def autotune(sizes, iu, iv, coff, data, c, c_type: int, support: int, c_scale: float = 1.0, reps: int = 3,
              stream=None):
-    """Fastest tuning (tile_rows, group_mib, split) for this batch, its median ms per bin+grid+degrid
-    pass, and the candidates of the last timing run [((rows, mib, split), ms)] (a cached result times
+    """Fastest tuning (tile_rows, group_mib, split, degrid_split) for this batch, its median ms per bin+grid+degrid
+    pass, and the candidates of the last timing run [((rows, mib, split, dsplit), ms)] (a cached result times
     nothing and leaves that report as it was)."""
     jobs = _jobs_array(sizes, None)  # the tuner grids into scratch grids of its own
     best = TcvTuning()

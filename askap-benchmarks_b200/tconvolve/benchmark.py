@@ -109,11 +109,12 @@ class Benchmark:
         plan = ctypes.c_void_p(self.device_buffers().plan)
         check(lib().tcv_plan_set_degrid_variant(plan, int(variant)), "tcv_plan_set_degrid_variant")
 
-    def set_tuning(self, tile_rows: int = 16, group_mib: int = 32, split: int = 0):
+    def set_tuning(self, tile_rows: int = 16, group_mib: int = 32, split: int = 0, degrid_split: int = 0):
         """Tile shape (grid rows per warp: 8, 16 or 32), plane-group slice (MiB of complex64
-        table; -1 = the whole table in one group) and work-unit size of busy cells (samples; 0 =
-        cells whole) of the plan.  Rebuilds the plan (the degridding variant returns to "tiles")."""
-        t = _lib.TcvTuning(int(tile_rows), int(group_mib), int(split))
+        table; -1 = the whole table in one group) and work-unit sizes of busy cells for gridding
+        and degridding (samples; 0 = cells whole) of the plan.  Rebuilds the plan (the degridding
+        variant returns to "tiles")."""
+        t = _lib.TcvTuning(int(tile_rows), int(group_mib), int(split), int(degrid_split))
         check(lib().tcv_set_tuning(self._ctx, ctypes.byref(t)), "tcv_set_tuning", self._ctx)
 
     def tuning(self) -> tuple:
@@ -123,7 +124,7 @@ class Benchmark:
 
     def tune(self, reps: int = 3):
         """Autotune the plan on this problem, table form and grid (tcv_tune): the fastest
-        (tile_rows, group_mib, split) and its median ms per bin + grid + degrid pass."""
+        (tile_rows, group_mib, split, degrid_split) and its median ms per bin + grid + degrid pass."""
         t = _lib.TcvTuning()
         ms = ctypes.c_float()
         check(lib().tcv_tune(self._ctx, int(reps), ctypes.byref(t), ctypes.byref(ms)), "tcv_tune", self._ctx)

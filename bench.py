@@ -56,6 +56,9 @@ def parse_args():
     p.add_argument("--degrid", default="tiles", choices=["tiles", "anchor"],
                    help="degridding kernel on the direct path")
     p.add_argument("--no-tune", action="store_true", help="default tile shape and plane groups, no autotuning")
+    p.add_argument("--tuning", default=None,
+                   help="tile rows,group MiB,grid split,degrid split for every measured form instead of "
+                        "autotuning (e.g. 16,64,0,128)")
     p.add_argument("--no-batched", action="store_true", help="skip the 64-job batched measurement")
     p.add_argument("--no-serving", action="store_true", help="skip the serving (Poisson arrivals) measurement")
     p.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window per serving rate")
@@ -145,6 +148,12 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        # the first sample is written once nvidia-smi is up: start timing after its start-up, which
+        # would otherwise compete with the host thread that enqueues the timed launches
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+            time.sleep(0.02)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -224,7 +233,13 @@ def b200_arm(args):
     vis = normal_vis(n, VIS_SEED)
     b.set_data(vis)
     tunings = {}
-    if not args.no_tune and args.path == "direct":
+    if args.tuning and args.path == "direct":
+        fixed = (tuple(int(x) for x in args.tuning.split(",")) + (0, 0, 0, 0))[:4]
+        for name in dict.fromkeys([args.form, "c64"]):
+            tunings[name] = (fixed, None)
+        b.set_ctype(form)
+        b.set_tuning(*fixed)
+    elif not args.no_tune and args.path == "direct":
         # autotuned tile shape and plane groups for each form measured (tcv_tune on this problem)
         if args.form != "c64":
             b.set_ctype("c64")
@@ -243,7 +258,7 @@ def b200_arm(args):
     tuning = {"t": TcvTuning(*(tunings[args.form][0] if args.form in tunings else (16, 32)))}
     # one workspace for every plan the bench builds (each measured form's tuning)
     wbytes = max(L.tcv_plan_workspace_bytes_tuned(n, support, prob.g_size, c_len, ctypes.byref(TcvTuning(*t)))
-                 for t in [(16, 32, 0)] + [v[0] for v in tunings.values()])
+                 for t in [(16, 32, 0, 0)] + [v[0] for v in tunings.values()])
     work = torch.empty(wbytes, dtype=torch.uint8, device="cuda")
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     sp = ctypes.c_void_p(stream.cuda_stream)
@@ -422,8 +437,9 @@ def b200_arm(args):
                                 if args.form == "r32" else args.form),
                        "path": args.path, "degrid": args.degrid,
                        "tuning": {"tile_rows": tuning["t"].tile_rows, "group_mib": tuning["t"].group_mib,
-                                  "split": tuning["t"].split,
-                                  "chosen_by": "autotuner (tcv_tune)" if tunings else "default"},
+                                  "split": tuning["t"].split, "degrid_split": tuning["t"].degrid_split,
+                                  "chosen_by": ("fixed (--tuning)" if args.tuning else "autotuner (tcv_tune)")
+                                  if tunings else "default"},
                        "parallelism": f"replicas x{world}",
                        "l2": f"{L2_FLUSH_BYTES >> 20} MiB buffer written between timed steps",
                        "step": "binning plan + gridding pass + degridding pass"},

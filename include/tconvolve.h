@@ -185,10 +185,11 @@ typedef struct tcv_tuning {
                       64 x 4*tile_rows points; 0 = 16 */
     int group_mib; /* table slice per plane group, MiB of complex64 (whole w-planes, at least
                       one); 0 = 32; -1 = the whole table in one group */
-    int split;     /* cells of at least 2*split samples are split into work units of about
-                      split samples, so that a plan with few busy tiles still fills the GPU
-                      (gridding units write partial tiles that are folded into the grid in unit
+    int split;     /* gridding: cells of at least 2*split samples are split into work units of
+                      about split samples, so that a plan with few busy tiles still fills the GPU
+                      (the units write partial tiles that are folded into the grid in unit
                       order); 0 = cells are never split */
+    int degrid_split; /* the same for degridding (units need no fold there) */
 } tcv_tuning;
 
 /* Workspace of a batched plan (0 for invalid arguments).  tuning may be NULL (defaults). */

@@ -110,13 +110,13 @@ def test_batch_matches_single_jobs_and_oracle(tcv, orc, prob):
 
 @pytest.mark.parametrize("rows", [8, 16, 32])
 @pytest.mark.parametrize("mib", [32, 8, -1])
-@pytest.mark.parametrize("split", [0, 64])
-def test_tunings_agree(tcv, orc, prob, rows, mib, split):
+@pytest.mark.parametrize("split,dsplit", [(0, 0), (64, 64), (0, 128)])
+def test_tunings_agree(tcv, orc, prob, rows, mib, split, dsplit):
     """Every tile shape, plane-group size and work-unit size gives the oracle's answer; with cells
     whole, gridding is bit-identical across tile shapes with the same plane groups."""
-    b, grids, out = _run_batch(tcv, prob, SIZES, tuning=(rows, mib, split))
-    assert b.tuning() == (rows, mib, split)
-    _, base_grids, _ = _run_batch(tcv, prob, SIZES, tuning=(16, mib, 0))
+    b, grids, out = _run_batch(tcv, prob, SIZES, tuning=(rows, mib, split, dsplit))
+    assert b.tuning() == (rows, mib, split, dsplit)
+    _, base_grids, _ = _run_batch(tcv, prob, SIZES, tuning=(16, mib, 0, 0))
     h = _host(prob)
     at = 0
     for j, (n, g) in enumerate(SIZES):
@@ -135,10 +135,10 @@ def test_graph_replay_matches_direct_calls(tcv, prob):
     from tconvolve._lib import PASS_BIN, PASS_DEGRID, PASS_GRID
     from tconvolve.batch import Batch
 
-    _, direct, direct_out = _run_batch(tcv, prob, SIZES, tuning=(8, 32, 64))
+    _, direct, direct_out = _run_batch(tcv, prob, SIZES, tuning=(8, 32, 64, 256))
     grids = _zeros(SIZES)
     b = Batch(SIZES, grids, prob["iu"], prob["iv"], prob["coff"], prob["support"], prob["c_len"],
-              tuning=(8, 32, 64))
+              tuning=(8, 32, 64, 256))
     out = torch.empty(prob["total"], dtype=torch.complex64, device="cuda")
     graph = b.capture(PASS_BIN | PASS_GRID | PASS_DEGRID, prob["data"], prob["c64"], tcv.C64, vis=out)
     for gr in grids:
@@ -165,6 +165,7 @@ def test_autotuner(tcv, prob):
     assert ms == min(m for _, m in report)
     assert {t[0] for t, _ in report} == {8, 16, 32}
     assert {t[2] for t, _ in report} == {0, 512, 256, 128, 64}
+    assert {t[3] for t, _ in report} == {0, 512, 256, 128, 64}
     again, ms2, _ = autotune(SIZES, prob["iu"], prob["iv"], prob["coff"], prob["data"], prob["c64"], tcv.C64,
                              prob["support"], reps=2)
     assert again == best and ms2 == ms  # cached

@@ -68,7 +68,7 @@ def test_precision_batched_form(tcv, orc, cuda_ok, form):
     ct = tcv.CTYPE_BY_NAME[form]
     c, scale, _ = raw.convert_c(p["c64"], ct)
     grids = [torch.zeros(g * g, dtype=torch.complex64, device="cuda") for _, g in sub]
-    bt = Batch(sub, grids, p["iu"], p["iv"], p["coff"], p["support"], p["c_len"], tuning=(16, 64, 512))
+    bt = Batch(sub, grids, p["iu"], p["iv"], p["coff"], p["support"], p["c_len"], tuning=(16, 64, 0, 512))
     bt.grid(p["data"], c, ct, scale)
     out = torch.empty(p["total"], dtype=torch.complex64, device="cuda")
     bt.degrid(c, ct, out, scale)
