@@ -105,17 +105,14 @@ struct TabRBF16 {
     }
 };
 
-// acc += a * b (complex), FP32 fused multiply-adds.  With a real table (b.y == 0 by construction)
-// only the two real-by-complex products are issued.
+// acc += a * b (complex), FP32 fused multiply-adds issued as paired FMAs (one instruction for the
+// real and imaginary lanes; each lane rounds as a separate fmaf).  With a real table (b.y == 0
+// by construction) only the real-by-complex pair is issued.
 template <bool kReal>
 __device__ __forceinline__ void cmac(float2& acc, const float2 a, const float2 b)
 {
-    acc.x = fmaf(a.x, b.x, acc.x);
-    acc.y = fmaf(a.y, b.x, acc.y);
-    if (!kReal) {
-        acc.x = fmaf(-a.y, b.y, acc.x);
-        acc.y = fmaf(a.x, b.y, acc.y);
-    }
+    acc = __ffma2_rn(a, make_float2(b.x, b.x), acc);                        // (re, im) += a * b.re
+    if (!kReal) acc = __ffma2_rn(make_float2(-a.y, a.x), make_float2(b.y, b.y), acc);  // += i * a * b.im
 }
 
 // CTAs per SM the register budget of a tile kernel is sized for: kR accumulators (gridding) or
