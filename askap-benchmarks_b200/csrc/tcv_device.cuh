@@ -119,8 +119,8 @@ __device__ __forceinline__ void cmac(float2& acc, const float2 a, const float2 b
 // grid values (degridding) per lane, two floats each.
 template <class Tab, int kR>
 __host__ __device__ constexpr int grid_min_blocks() { return kR >= 32 ? 2 : Tab::kMinBlocks; }
-template <int kR>
-__host__ __device__ constexpr int degrid_min_blocks() { return kR >= 32 ? 2 : 3; }
+template <class Tab, int kR>
+__host__ __device__ constexpr int degrid_min_blocks() { return kR >= 32 ? 2 : Tab::kMinBlocks; }
 
 // The CTA's work is the sequence of chunks (up to kTileChunk samples) of the work units it owns
 // (every gridDim.x-th unit of the plane group).  Chunk i is staged in shared memory while chunk
@@ -269,7 +269,7 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
 // this tile.  A final pass
 // (slot_reduce_kernel) adds each sample's tile slots in tile order: no atomics, deterministic.
 template <class Tab, int kS, int kR>
-__global__ void __launch_bounds__(kTileThreads, degrid_min_blocks<kR>())
+__global__ void __launch_bounds__(kTileThreads, degrid_min_blocks<Tab, kR>())
 degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                    const int* __restrict__ iu, const int* __restrict__ iv,
                    const int* __restrict__ coff, const u32* __restrict__ order,
