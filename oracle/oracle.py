@@ -50,6 +50,13 @@ def lib():
         L.orc_degrid_f32.argtypes = [_P, _I32, _I32, _P, _P, _P, _P, _P, _I64, _I32]
         L.orc_grid_f64.argtypes = [_P, _I64, _I32, _P, _P, _P, _P, _P, _I32]
         L.orc_degrid_f64.argtypes = [_P, _I32, _I32, _P, _P, _P, _P, _P, _I64]
+        L.orc_cur_geometry.argtypes = [_I32, _P]
+        L.orc_cur_init_uvw.argtypes = [_I32, _P, _P, _P, _P]
+        L.orc_cur_init_c.argtypes = [_I32, _P, _P, _P]
+        L.orc_cur_init_offsets.argtypes = [_I32, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.orc_cur_sort_by_plane.argtypes = [_I64, _I32, _P, _P, _P, _P]
+        L.orc_cur_grid_f32.argtypes = [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _I32, _I32]
+        L.orc_cur_degrid_f32.argtypes = [_P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P, _I32]
         _lib = L
     return _lib
 
@@ -207,3 +214,82 @@ def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     b = np.asarray(b).astype(np.complex128).ravel()
     nb = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+# -------------------------------------------------------------------------------------------------
+# The variable-support path of current/tConvolveMPI (tconvolve_oracle_current.c)
+# -------------------------------------------------------------------------------------------------
+@dataclass(frozen=True)
+class CurGeometry:
+    run_type: int
+    w_size: int
+    over_sample: int
+    support: int
+    g_size: int
+    n_baselines: int
+    n_samples: int
+    w_cell_size: float
+    uv_cell_size: float
+    c_len: int
+    s_max: int
+
+
+def cur_geometry(run_type: int) -> CurGeometry:
+    """current/tConvolveMPI/Benchmark.cc:64-158 (run types 0 continuum, 1 spectral, 2 nearest
+    neighbour, 3 7x7 kernels, 4 87x87 kernels)."""
+    out = np.zeros(10, np.float64)
+    if lib().orc_cur_geometry(run_type, _p(out)) != 0:
+        raise ValueError(f"unknown run type {run_type}")
+    return CurGeometry(run_type, int(out[0]), int(out[1]), int(out[2]), int(out[3]), int(out[4]),
+                       int(out[5]), float(out[6]), float(out[7]), int(out[8]), int(out[9]))
+
+
+def cur_init_uvw(run_type: int, state: int = 1):
+    """current/tConvolveMPI/Benchmark.cc:246-262; returns u, v, w and the generator state after."""
+    g = cur_geometry(run_type)
+    u, v, w = (np.empty(g.n_samples, np.float64) for _ in range(3))
+    st = np.array([state], np.uint64)
+    lib().orc_cur_init_uvw(run_type, _p(st), _p(u), _p(v), _p(w))
+    return u, v, w, int(st[0])
+
+
+def cur_init_c(run_type: int):
+    """current/tConvolveMPI/Benchmark.cc:487-583: (C complex64, sSize per plane, cOffset0)."""
+    g = cur_geometry(run_type)
+    s_size = np.empty(g.w_size, np.int32)
+    off0 = np.empty(g.w_size, np.int32)
+    c = np.empty(g.c_len, np.complex64)
+    lib().orc_cur_init_c(run_type, _p(s_size), _p(off0), _p(c))
+    return c, s_size, off0
+
+
+def cur_init_offsets(run_type: int, u, v, w, s_size, off0):
+    """current/tConvolveMPI/Benchmark.cc:599-650: iu, iv, wPlane, cOffset."""
+    n = u.size
+    iu, iv, wp, co = (np.empty(n, np.int32) for _ in range(4))
+    lib().orc_cur_init_offsets(run_type, n, _p(u), _p(v), _p(w), _p(s_size), _p(off0), _p(iu), _p(iv),
+                               _p(wp), _p(co))
+    return iu, iv, wp, co
+
+
+def cur_sort_by_plane(w_size: int, iu, iv, wp, co):
+    """setSort(1), current/tConvolveMPI/Benchmark.cc:287-306: offsets stably ordered by w-plane."""
+    iu, iv, wp, co = (np.ascontiguousarray(a, np.int32).copy() for a in (iu, iv, wp, co))
+    lib().orc_cur_sort_by_plane(iu.size, w_size, _p(iu), _p(iv), _p(wp), _p(co))
+    return iu, iv, wp, co
+
+
+def cur_grid_f32(data, iu, iv, wp, co, s_size, c, grid, g_size: int, threads: int = 1):
+    """current/tConvolveMPI/Benchmark.cc:373-411, reference order; grid accumulated in place."""
+    data = np.ascontiguousarray(data, np.complex64)
+    lib().orc_cur_grid_f32(_p(data), data.size, _p(iu), _p(iv), _p(wp), _p(co), _p(s_size), _p(c), _p(grid),
+                           g_size, threads)
+    return grid
+
+
+def cur_degrid_f32(grid, g_size: int, iu, iv, wp, co, s_size, c, threads: int = 1):
+    """current/tConvolveMPI/Benchmark.cc:414-452."""
+    out = np.empty(iu.size, np.complex64)
+    lib().orc_cur_degrid_f32(_p(grid), g_size, iu.size, _p(iu), _p(iv), _p(wp), _p(co), _p(s_size), _p(c),
+                             _p(out), threads)
+    return out
