@@ -51,6 +51,7 @@ struct GridArgs {
     const JobDesc* __restrict__ jobs;
     const u32* __restrict__ tinfo;  // per tile: column | row << 11 | job << 22
     float2* partial;                // partial tiles of split cells (gridding), tile after tile
+    const unsigned short* __restrict__ ssz;  // per-sample footprint width (variable-width plans)
 };
 
 // A work unit: a cell's samples [first, first + count) of the sorted order, and the partial tile
@@ -160,7 +161,9 @@ __device__ __forceinline__ void cursor_next(ChunkCursor& c, u32 i1, const uint4*
     }
 }
 
-template <class Tab, int kS, int kR>
+// kVar: every sample has its own footprint width (its w-plane's, a.ssz) instead of one width
+// for the plan (variable-support tables, current/tConvolveMPI/Benchmark.cc:373-411).
+template <class Tab, int kS, int kR, bool kVar = false>
 __global__ void __launch_bounds__(kTileThreads, grid_min_blocks<Tab, kR>())
 grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
                  const int* __restrict__ iu, const int* __restrict__ iv,
@@ -170,16 +173,20 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
     constexpr int kTH = tile_height(kR);
     __shared__ float4 sm_rec[2][kTileChunk];  // (data.re, data.im, first column, first row)
     __shared__ int sm_coff[2][kTileChunk];
+    __shared__ int sm_w[kVar ? 2 : 1][kVar ? kTileChunk : 1];  // per-sample widths
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
+    const int s0 = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
     const u32 i1 = group_ustart[a.group + 1];
     auto stage = [&](const ChunkCursor& c, int buf) {
         if (int(threadIdx.x) < c.m) {
             const u32 k = order[c.start + c.base + threadIdx.x];
             const float2 d = data[k];
+            const int sk = kVar ? int(a.ssz[k]) : s0;
             sm_rec[buf][threadIdx.x] = make_float4(d.x * a.c_scale, d.y * a.c_scale,
-                                                   __int_as_float(iu[k] - a.support), __int_as_float(iv[k]));
+                                                   __int_as_float(iu[k] - (kVar ? sk / 2 : a.support)),
+                                                   __int_as_float(iv[k]));
             sm_coff[buf][threadIdx.x] = coff[k];
+            if (kVar) sm_w[kVar ? buf : 0][kVar ? threadIdx.x : 0] = sk;
         }
     };
     ChunkCursor cur;
@@ -201,6 +208,7 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
         const int gy0 = ty * kTH + (warp / (kTileW / 32)) * kR;
         for (int j = 0; j < cur.m; ++j) {
             const float4 q = sm_rec[buf][j];
+            const int s = kVar ? sm_w[kVar ? buf : 0][kVar ? j : 0] : s0;
             const int fx = __float_as_int(q.z), fy = __float_as_int(q.w);
             const int dy0 = gy0 - fy;  // footprint row of this warp's first row
             if (dy0 >= s || dy0 + kR <= 0) continue;      // warp-uniform
@@ -268,7 +276,7 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
 // with shuffles, and the CTA adds its 8 warp partials in warp order into the sample's slot for
 // this tile.  A final pass
 // (slot_reduce_kernel) adds each sample's tile slots in tile order: no atomics, deterministic.
-template <class Tab, int kS, int kR>
+template <class Tab, int kS, int kR, bool kVar = false>
 __global__ void __launch_bounds__(kTileThreads, degrid_min_blocks<Tab, kR>())
 degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                    const int* __restrict__ iu, const int* __restrict__ iv,
@@ -279,8 +287,9 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
     constexpr int kTH = tile_height(kR);
     __shared__ int4 sm_rec[kTileChunk];              // (sample, first column, first row, cOffset)
     __shared__ float2 sm_part[kTileChunk][kTileWarps];
+    __shared__ int sm_w[kVar ? kTileChunk : 1];      // per-sample widths
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
+    const int s0 = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
     const u32 i1 = group_ustart[a.group + 1];
     for (u32 it = group_ustart[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
         const uint4 u = units[it];  // the units of a split cell each read the tile; no partials
@@ -303,7 +312,9 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
             __syncthreads();
             if (threadIdx.x < m) {
                 const u32 k = order[start + base + threadIdx.x];
-                sm_rec[threadIdx.x] = make_int4(int(k), iu[k] - a.support, iv[k], coff[k]);
+                const int sk = kVar ? int(a.ssz[k]) : s0;
+                sm_rec[threadIdx.x] = make_int4(int(k), iu[k] - (kVar ? sk / 2 : a.support), iv[k], coff[k]);
+                if (kVar) sm_w[kVar ? threadIdx.x : 0] = sk;
             }
             __syncthreads();
             // four samples at a time: each lane's partial dot products of the four, then one
@@ -316,6 +327,7 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                     const int j = jg + e;
                     if (j >= m) continue;  // warp-uniform
                     const int4 q = sm_rec[j];
+                    const int s = kVar ? sm_w[kVar ? j : 0] : s0;
                     const int fx = q.y, fy = q.z;
                     const int dy0 = gy0 - fy;
                     if (dy0 >= s || dy0 + kR <= 0 || fx > bx0 + 31 || fx + s <= bx0) continue;  // warp-uniform
@@ -370,6 +382,7 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                     v.x += sm_part[threadIdx.x][w].x;
                     v.y += sm_part[threadIdx.x][w].y;
                 }
+                const int s = kVar ? sm_w[kVar ? threadIdx.x : 0] : s0;
                 const int sx0 = q.y / kTileW, sx1 = (q.y + s - 1) / kTileW, sy0 = q.z / kTH;
                 const int slot = (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0);
                 slots[(unsigned long long)(u32(q.x)) * max_tiles + slot] = v;

@@ -41,19 +41,20 @@ GridArgs make_args(const tcv_plan* p, int grp, float c_scale, float2* grid)
     a.jobs = p->jobs;
     a.tinfo = p->tinfo;
     a.partial = p->partial;
+    a.ssz = p->ssz;
     return a;
 }
 
 // One persistent launch per plane group, in group order on the stream: launches of one stream
 // run one after another, so a tile's read-modify-write never races with another group's.
-template <class Tab, int kR>
+template <class Tab, int kR, bool kVar = false>
 tcv_status launch(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
                   cudaStream_t st, int c_type)
 {
     const PlanGeom& g = p->g;
     if (g.n == 0) return TCV_OK;
-    const void* spec = jit_tile_kernel(0, c_type, g.s, kR);
-    const void* generic = reinterpret_cast<const void*>(&grid_tile_kernel<Tab, 0, kR>);
+    const void* spec = kVar ? nullptr : jit_tile_kernel(0, c_type, g.s, kR);
+    const void* generic = reinterpret_cast<const void*>(&grid_tile_kernel<Tab, 0, kR, kVar>);
     const void* kernel = spec ? spec : generic;
     const int ctas = resident_of(kernel);
     const typename Tab::elem* tab = static_cast<const typename Tab::elem*>(c);
@@ -73,14 +74,14 @@ tcv_status launch(const tcv_plan* p, const float2* data, const void* c, float c_
     return TCV_OK;
 }
 
-template <class Tab, int kR>
+template <class Tab, int kR, bool kVar = false>
 tcv_status launch_adjoint(const tcv_plan* p, const float2* grid, const void* c, float c_scale, float2* out,
                           cudaStream_t st, int c_type)
 {
     const PlanGeom& g = p->g;
     if (g.n == 0) return TCV_OK;
-    const void* spec = jit_tile_kernel(1, c_type, g.s, kR);
-    const void* generic = reinterpret_cast<const void*>(&degrid_tile_kernel<Tab, 0, kR>);
+    const void* spec = kVar ? nullptr : jit_tile_kernel(1, c_type, g.s, kR);
+    const void* generic = reinterpret_cast<const void*>(&degrid_tile_kernel<Tab, 0, kR, kVar>);
     const void* kernel = spec ? spec : generic;
     const int ctas = resident_of(kernel);
     const typename Tab::elem* tab = static_cast<const typename Tab::elem*>(c);
@@ -101,6 +102,12 @@ template <class Tab>
 tcv_status grid_rows(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
                      cudaStream_t st, int c_type)
 {
+    if (p->g.var) {  // per-sample widths: complex tables (the w-term is complex), 64 x 64 tiles
+        if constexpr (!Tab::kReal) {
+            if (p->g.rows == 16) return launch<Tab, 16, true>(p, data, c, c_scale, grid, st, c_type);
+        }
+        return TCV_ERR_UNSUPPORTED;
+    }
     switch (p->g.rows) {
         case 8: return launch<Tab, 8>(p, data, c, c_scale, grid, st, c_type);
         case 16: return launch<Tab, 16>(p, data, c, c_scale, grid, st, c_type);
@@ -113,6 +120,12 @@ template <class Tab>
 tcv_status degrid_rows(const tcv_plan* p, const float2* grid, const void* c, float c_scale, float2* out,
                        cudaStream_t st, int c_type)
 {
+    if (p->g.var) {
+        if constexpr (!Tab::kReal) {
+            if (p->g.rows == 16) return launch_adjoint<Tab, 16, true>(p, grid, c, c_scale, out, st, c_type);
+        }
+        return TCV_ERR_UNSUPPORTED;
+    }
     switch (p->g.rows) {
         case 8: return launch_adjoint<Tab, 8>(p, grid, c, c_scale, out, st, c_type);
         case 16: return launch_adjoint<Tab, 16>(p, grid, c, c_scale, out, st, c_type);

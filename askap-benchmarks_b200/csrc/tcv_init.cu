@@ -12,26 +12,7 @@
 namespace tcv {
 namespace {
 
-constexpr uint64_t kLcgA = 1103515245ull;
-constexpr uint64_t kLcgC = 12345ull;
 constexpr double kMaxInt = 2147483647.0;
-
-// x -> A x + C after m steps of x -> a x + c (mod 2^64), by binary powering of the affine map.
-__device__ __forceinline__ void lcg_jump(uint64_t m, uint64_t& A, uint64_t& C)
-{
-    uint64_t a = kLcgA, c = kLcgC;
-    A = 1;
-    C = 0;
-    while (m) {
-        if (m & 1) {
-            C = a * C + c;
-            A = a * A;
-        }
-        c = a * c + c;
-        a = a * a;
-        m >>= 1;
-    }
-}
 
 __device__ __forceinline__ double lcg_coord(uint64_t& state, double baseline, double half)
 {

@@ -56,6 +56,9 @@ struct PlanGeom {
     int degrid_mode;    // 0 staged (TMA), 1 direct from global
     int degrid_parts;   // warps sharing one sample's footprint in the staged kernel
     bool key64;         // 64-bit sort keys
+    // variable-width plans (one footprint width per w-plane; s and support are the widest)
+    bool var;
+    int n_planes;
 };
 
 }  // namespace tcv
@@ -102,6 +105,12 @@ struct tcv_plan {
     bool binned;
     std::vector<tcv::JobDesc> host_jobs;  // the job table (kept alive for its asynchronous copy)
     std::vector<uint32_t> host_job_start;
+    // variable-width plans
+    const int32_t* wplane;         // per-sample w-plane (device, the caller's)
+    int32_t* plane_s;              // footprint width per plane (device)
+    int32_t* plane_grp;            // plane group per plane (device)
+    uint16_t* ssz;                 // per-sample footprint width (device)
+    std::vector<int32_t> host_plane_s, host_plane_grp;
 };
 
 namespace tcv {
@@ -153,6 +162,27 @@ int64_t paired_copy_stride(int64_t c_len, int s);
 size_t paired_table_bytes(int64_t c_len, int s, int c_type);
 tcv_status pair_table(const void* in, int64_t c_len, int s, int c_type, void* out, cudaStream_t st);
 tcv_status pad_table(const void* in, int64_t c_len, int s, int c_type, void* out, cudaStream_t st);
+
+// The reference's K&R generator x -> a x + c (mod 2^64) (attic/tConvolveMPI/Benchmark.cc:53-58,
+// current/tConvolveMPI/Benchmark.cc:53-58): A, C of the map after m steps, by binary powering
+// of the affine map, so that sample i's draws start from A * state0 + C.
+constexpr uint64_t kLcgA = 1103515245ull;
+constexpr uint64_t kLcgC = 12345ull;
+__host__ __device__ inline void lcg_jump(uint64_t m, uint64_t& A, uint64_t& C)
+{
+    uint64_t a = kLcgA, c = kLcgC;
+    A = 1;
+    C = 0;
+    while (m) {
+        if (m & 1) {
+            C = a * C + c;
+            A = a * A;
+        }
+        c = a * c + c;
+        a = a * a;
+        m >>= 1;
+    }
+}
 
 inline tcv_status cuda_status(cudaError_t e)
 {

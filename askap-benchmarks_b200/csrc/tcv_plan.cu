@@ -30,6 +30,7 @@
 #include <thrust/iterator/transform_iterator.h>
 
 #include <algorithm>
+#include <climits>
 #include <new>
 
 namespace tcv {
@@ -60,22 +61,40 @@ __device__ __forceinline__ int job_of(const uint32_t* __restrict__ job_start, in
     return lo;
 }
 
+// Variable-width plans: the sample's w-plane gives its footprint width (plane_s) and its plane
+// group (plane_grp); the width is recorded per sample (ssz) for the tile kernels.
+struct VarPlanes {
+    const int32_t* __restrict__ wplane;
+    const int32_t* __restrict__ plane_s;
+    const int32_t* __restrict__ plane_grp;
+    uint16_t* ssz;
+};
+
 template <typename K>
 __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* __restrict__ iv,
                                  const int32_t* __restrict__ coff, PlanGeom g, const JobDesc* __restrict__ jobs,
                                  const uint32_t* __restrict__ job_start, K* keys, uint32_t* vals, K* akeys,
                                  uint32_t* avals, uint32_t* tile_count, uint32_t* atile_count, uint16_t* ntl,
-                                 unsigned long long* rejected)
+                                 unsigned long long* rejected, VarPlanes var)
 {
     const int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (d >= g.n) return;
     const int job = g.n_jobs > 1 ? job_of(job_start, g.n_jobs, uint32_t(d)) : 0;
     const JobDesc jd = jobs[job];
-    const int64_t fx = (int64_t)iu[d] - g.support;
+    int64_t s = g.s, support = g.support;
+    int plane = 0;
+    bool plane_ok = true;
+    if (g.var) {
+        plane = var.wplane[d];
+        plane_ok = plane >= 0 && plane < g.n_planes;
+        s = plane_ok ? var.plane_s[plane] : 1;
+        support = s / 2;
+        var.ssz[d] = uint16_t(s);
+    }
+    const int64_t fx = (int64_t)iu[d] - support;
     const int64_t fy = iv[d];
     const int64_t co = coff[d];
-    const int64_t s = g.s;
-    const bool ok = fx >= 0 && fx + s <= jd.g_size && fy >= 0 && fy + s <= jd.g_size && co >= 0 &&
+    const bool ok = plane_ok && fx >= 0 && fx + s <= jd.g_size && fy >= 0 && fy + s <= jd.g_size && co >= 0 &&
                     co + s * s <= g.c_len;
     K* kp = keys + d * g.max_tiles;
     uint32_t* vp = vals + d * g.max_tiles;
@@ -93,7 +112,7 @@ __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* 
         }
         return;
     }
-    const uint32_t grp = uint32_t(co / (s * s) / g.kid_group);
+    const uint32_t grp = g.var ? uint32_t(var.plane_grp[plane]) : uint32_t(co / (s * s) / g.kid_group);
     const uint32_t cell0 = grp * uint32_t(g.ntiles) + jd.tile_base;
     const int tx0 = int(fx / g.tw), tx1 = int((fx + s - 1) / g.tw);
     const int ty0 = int(fy / g.th), ty1 = int((fy + s - 1) / g.th);
@@ -298,9 +317,10 @@ tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_
     TCV_CUDA(cudaMemsetAsync(p->rejected, 0, sizeof(unsigned long long), st));
     TCV_CUDA(cudaMemsetAsync(p->status, 0, sizeof(unsigned int), st));
     if (g.n > 0) {
+        const VarPlanes var{p->wplane, p->plane_s, p->plane_grp, p->ssz};
         plan_keys_kernel<K><<<unsigned((g.n + 255) / 256), 256, 0, st>>>(
             iu, iv, coff, g, p->jobs, p->job_start, static_cast<K*>(p->keys[0]), p->vals[0],
-            static_cast<K*>(p->akeys[0]), p->avals[0], p->tile_count, p->atile_count, p->ntl, p->rejected);
+            static_cast<K*>(p->akeys[0]), p->avals[0], p->tile_count, p->atile_count, p->ntl, p->rejected, var);
         TCV_CUDA(cudaGetLastError());
         cub::DoubleBuffer<K> kb(static_cast<K*>(p->keys[0]), static_cast<K*>(p->keys[1]));
         cub::DoubleBuffer<uint32_t> vb(p->vals[0], p->vals[1]);
@@ -370,6 +390,11 @@ tcv_status plan_create(tcv_plan* p, void* d_work, size_t work_bytes, cudaStream_
     p->job_start = static_cast<uint32_t*>(take(size_t(g.n_jobs + 1) * 4));
     p->tinfo = static_cast<uint32_t*>(take(size_t(g.ntiles) * 4));
     p->ntl = static_cast<uint16_t*>(take(size_t(g.n) * 2));
+    if (g.var) {
+        p->ssz = static_cast<uint16_t*>(take(size_t(g.n) * 2));
+        p->plane_s = static_cast<int32_t*>(take(size_t(g.n_planes) * 4));
+        p->plane_grp = static_cast<int32_t*>(take(size_t(g.n_planes) * 4));
+    }
     p->keys[0] = take(np * ks);
     p->keys[1] = take(np * ks);
     p->vals[0] = static_cast<uint32_t*>(take(np * 4));
@@ -427,6 +452,11 @@ tcv_status plan_create(tcv_plan* p, void* d_work, size_t work_bytes, cudaStream_
     }
     tile_info_kernel<<<unsigned((g.ntiles + 255) / 256), 256, 0, st>>>(p->jobs, g.n_jobs, uint32_t(g.ntiles), p->tinfo);
     TCV_CUDA(cudaGetLastError());
+    if (g.var) {  // the plane widths and groups (host vectors owned by the plan)
+        TCV_CUDA(cudaMemcpyAsync(p->plane_s, p->host_plane_s.data(), size_t(g.n_planes) * 4, cudaMemcpyHostToDevice, st));
+        TCV_CUDA(cudaMemcpyAsync(p->plane_grp, p->host_plane_grp.data(), size_t(g.n_planes) * 4,
+                                 cudaMemcpyHostToDevice, st));
+    }
     return TCV_OK;
 }
 
@@ -530,6 +560,7 @@ size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out)
     size_t b = 0;
     b += align_up(size_t(g.n_jobs) * sizeof(JobDesc)) + align_up(size_t(g.n_jobs + 1) * 4);
     b += align_up(size_t(g.ntiles) * 4) + align_up(size_t(g.n) * 2);
+    if (g.var) b += align_up(size_t(g.n) * 2) + 2 * align_up(size_t(g.n_planes) * 4);
     b += 2 * align_up(np * ks) + 2 * align_up(np * 4);
     b += 2 * align_up(an * ks) + 2 * align_up(an * 4);
     const size_t cells = grid_cells(g), acells = anchor_cells(g);
@@ -544,6 +575,39 @@ size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out)
     b += align_up(np * sizeof(float2));
     b += align_up(cb);
     return b;
+}
+
+// Geometry of a variable-width plan: the widest plane sets the tile reach; whole planes are
+// grouped in order until a group's slice of the table passes group_mib (complex64).
+PlanGeom make_geom_var(int64_t n, const int32_t* s_size, const int32_t* c_off0, int n_planes, int g_size,
+                       int64_t c_len, const tcv_tuning* t, std::vector<int32_t>& plane_grp)
+{
+    int s_max = 1;
+    for (int k = 0; k < n_planes; ++k) s_max = std::max(s_max, int(s_size[k]));
+    PlanGeom g = make_geom(n, s_max / 2, &g_size, 1, c_len, t, false);
+    g.var = true;
+    g.n_planes = n_planes;
+    plane_grp.assign(size_t(n_planes), 0);
+    const int64_t budget = g.group_mib > 0 ? (int64_t(g.group_mib) << 20) : INT64_MAX;
+    int grp = 0;
+    int64_t used = 0;
+    for (int k = 0; k < n_planes; ++k) {
+        const int64_t end = k + 1 < n_planes ? c_off0[k + 1] : c_len;
+        const int64_t bytes = (end - c_off0[k]) * 8;
+        if (used > 0 && used + bytes > budget) {
+            ++grp;
+            used = 0;
+        }
+        used += bytes;
+        plane_grp[size_t(k)] = grp;
+    }
+    g.n_groups = grp + 1;
+    g.kid_group = 0;
+    g.group_bits = bits_for(uint64_t(g.n_groups - 1));
+    g.tile_bits = bits_for(uint64_t(g.n_groups) * uint64_t(g.ntiles) - 1);
+    g.key_bits = g.tile_bits + 1;
+    g.key64 = g.key_bits > 32;
+    return g;
 }
 
 tcv_status plan_bin(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff, cudaStream_t st)
@@ -569,6 +633,29 @@ tcv_status plan_init(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, cons
     *p = tcv_plan{};
     p->g = make_geom(n, support, &g_size, 1, c_len, t, true);
     if (!geom_supported(p->g)) return TCV_ERR_UNSUPPORTED;
+    const tcv_status s = plan_create(p, d_work, work_bytes, st);
+    if (s != TCV_OK) return s;
+    return plan_bin(p, d_iu, d_iv, d_coff, st);
+}
+
+// Fill *p with a variable-width one-job plan (per-sample widths from the w-planes) built in d_work.
+tcv_status plan_init_var(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff,
+                         const int32_t* d_wplane, int64_t n, const int32_t* s_size, const int32_t* c_off0,
+                         int n_planes, int g_size, int64_t c_len, void* d_work, size_t work_bytes, cudaStream_t st,
+                         const tcv_tuning* t)
+{
+    if (!p || n < 0 || g_size < 1 || c_len < 1 || n_planes < 1 || !s_size || !c_off0 || !valid_tuning(t))
+        return TCV_ERR_ARG;
+    if (n > 0 && (!d_iu || !d_iv || !d_coff || !d_wplane)) return TCV_ERR_ARG;
+    for (int k = 0; k < n_planes; ++k)
+        if (s_size[k] < 1 || s_size[k] % 2 == 0 || s_size[k] > 4095 || c_off0[k] < 0 || c_off0[k] > c_len)
+            return TCV_ERR_ARG;
+    if (!d_work) return TCV_ERR_ARG;
+    *p = tcv_plan{};
+    p->g = make_geom_var(n, s_size, c_off0, n_planes, g_size, c_len, t, p->host_plane_grp);
+    if (!geom_supported(p->g)) return TCV_ERR_UNSUPPORTED;
+    p->host_plane_s.assign(s_size, s_size + n_planes);
+    p->wplane = d_wplane;
     const tcv_status s = plan_create(p, d_work, work_bytes, st);
     if (s != TCV_OK) return s;
     return plan_bin(p, d_iu, d_iv, d_coff, st);
@@ -644,6 +731,33 @@ tcv_status tcv_batch_plan_create(tcv_plan** plan_out, const tcv_job* jobs, int n
     }
     p->host_job_start[size_t(n_jobs)] = first;
     s = plan_create(p, d_work, work_bytes, static_cast<cudaStream_t>(stream));
+    if (s != TCV_OK) {
+        delete p;
+        return s;
+    }
+    *plan_out = p;
+    return TCV_OK;
+}
+
+size_t tcv_plan_workspace_bytes_var(int64_t n, const int32_t* s_size, const int32_t* c_off0, int n_planes,
+                                    int g_size, int64_t c_len, const tcv_tuning* tuning)
+{
+    if (n < 0 || !s_size || !c_off0 || n_planes < 1 || g_size < 1 || c_len < 1 || !valid_tuning(tuning)) return 0;
+    std::vector<int32_t> grp;
+    PlanGeom g = make_geom_var(n, s_size, c_off0, n_planes, g_size, c_len, tuning, grp);
+    return plan_bytes(g, nullptr);
+}
+
+tcv_status tcv_plan_build_var(tcv_plan** plan_out, const int32_t* d_iu, const int32_t* d_iv, const int32_t* d_coff,
+                              const int32_t* d_wplane, int64_t n, const int32_t* s_size, const int32_t* c_off0,
+                              int n_planes, int g_size, int64_t c_len, const tcv_tuning* tuning, void* d_work,
+                              size_t work_bytes, void* stream)
+{
+    if (!plan_out) return TCV_ERR_ARG;
+    tcv_plan* p = new (std::nothrow) tcv_plan{};
+    if (!p) return TCV_ERR_OOM;
+    const tcv_status s = plan_init_var(p, d_iu, d_iv, d_coff, d_wplane, n, s_size, c_off0, n_planes, g_size, c_len,
+                                       d_work, work_bytes, static_cast<cudaStream_t>(stream), tuning);
     if (s != TCV_OK) {
         delete p;
         return s;
@@ -741,7 +855,7 @@ tcv_status tcv_plan_grid(const tcv_plan* plan, const float* d_data, const void* 
     if (plan->batch ? d_grid != nullptr : d_grid == nullptr) return TCV_ERR_ARG;
     if (tcv_ctype_bytes(c_type) == 0) return TCV_ERR_ARG;
     if (!plan->binned) return TCV_ERR_STATE;
-    const bool plain_tiles = !plan->batch && plan->g.rows == 16;  // what the other kernel families need
+    const bool plain_tiles = !plan->batch && !plan->g.var && plan->g.rows == 16;  // what the other families need
     if (c_type & TCV_C_PADDED) {
         if (!plain_tiles) return TCV_ERR_UNSUPPORTED;
         return launch_grid_pipe(plan, reinterpret_cast<const float2*>(d_data), d_c, c_type & 0xff, c_scale,
@@ -763,7 +877,7 @@ tcv_status tcv_plan_degrid(const tcv_plan* plan, const float* d_grid, const void
     if (plan->batch ? d_grid != nullptr : d_grid == nullptr) return TCV_ERR_ARG;
     if (tcv_ctype_bytes(c_type) == 0) return TCV_ERR_ARG;
     if (!plan->binned) return TCV_ERR_STATE;
-    const bool plain_tiles = !plan->batch && plan->g.rows == 16;
+    const bool plain_tiles = !plan->batch && !plan->g.var && plan->g.rows == 16;
     if (c_type & TCV_C_PADDED) {
         if (!plain_tiles) return TCV_ERR_UNSUPPORTED;
         if (plan->g.n == 0) return TCV_OK;
@@ -776,7 +890,7 @@ tcv_status tcv_plan_degrid(const tcv_plan* plan, const float* d_grid, const void
         return launch_degrid_pair(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type & 0xff, c_scale,
                                   reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
     }
-    if (plan->degrid_variant == TCV_DEGRID_TILES || plan->batch) {
+    if (plan->degrid_variant == TCV_DEGRID_TILES || plan->batch || plan->g.var) {
         if (plan->g.n == 0) return TCV_OK;
         return launch_degrid_tiles(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type, c_scale,
                                    reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));

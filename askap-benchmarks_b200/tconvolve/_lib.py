@@ -99,6 +99,15 @@ class TcvRequestInfo(ctypes.Structure):
 
 REQ_GRID, REQ_DEGRID = 0, 1
 
+
+class TcvCurGeometry(ctypes.Structure):
+    _fields_ = [
+        ("run_type", ctypes.c_int32), ("w_size", ctypes.c_int32), ("over_sample", ctypes.c_int32),
+        ("support", ctypes.c_int32), ("g_size", ctypes.c_int32), ("n_baselines", ctypes.c_int32),
+        ("n_samples", ctypes.c_int64), ("c_len", ctypes.c_int64), ("s_min", ctypes.c_int32),
+        ("s_max", ctypes.c_int32), ("w_cell_size", ctypes.c_double), ("uv_cell_size", ctypes.c_double),
+    ]
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I64 = ctypes.c_int64
@@ -150,6 +159,40 @@ SIGNATURES = {
     "tcv_server_submit": (_I, [_P, _P, _P]),
     "tcv_server_wait": (_I, [_P, ctypes.c_uint64, _D, _P]),
     "tcv_server_stats": (_I, [_P, _P, _P, _P, _P]),
+    "tcv_cur_geometry_of": (_I, [_I, _P]),
+    "tcv_cur_planes": (_I, [_I, _P, _P]),
+    "tcv_cur_init_uvw_raw": (_I, [_I, ctypes.c_uint64, _P, _P, _P, _P, _P]),
+    "tcv_cur_init_c_raw": (_I, [_I, _P, _P]),
+    "tcv_cur_init_offsets_raw": (_I, [_I, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P]),
+    "tcv_cur_required_rate": (None, [_P]),
+    "tcv_cur_create": (_I, [_I, _PP]),
+    "tcv_cur_destroy": (None, [_P]),
+    "tcv_cur_last_error": (ctypes.c_char_p, [_P]),
+    "tcv_cur_set_sort": (_I, [_P, _I]),
+    "tcv_cur_set_run_type": (_I, [_P, _I]),
+    "tcv_cur_get_run_type": (_I, [_P]),
+    "tcv_cur_set_ctype": (_I, [_P, _I]),
+    "tcv_cur_set_tuning": (_I, [_P, _P]),
+    "tcv_cur_init": (_I, [_P]),
+    "tcv_cur_run_grid": (_I, [_P]),
+    "tcv_cur_run_degrid": (_I, [_P]),
+    "tcv_cur_sync": (_I, [_P]),
+    "tcv_cur_get_stream": (_P, [_P]),
+    "tcv_cur_support": (_I, [_P]),
+    "tcv_cur_n_visibilities": (_I64, [_P]),
+    "tcv_cur_n_pixels": (_I64, [_P]),
+    "tcv_cur_generator_state": (ctypes.c_uint64, [_P]),
+    "tcv_cur_info": (_I, [_P, _P]),
+    "tcv_cur_set_data": (_I, [_P, _P, _I64]),
+    "tcv_cur_zero_grid": (_I, [_P]),
+    "tcv_cur_get_grid": (_I, [_P, _P]),
+    "tcv_cur_get_outdata": (_I, [_P, _P, _I64]),
+    "tcv_cur_get_c": (_I, [_P, _P, _I64]),
+    "tcv_cur_get_uvw": (_I, [_P, _P, _P, _P]),
+    "tcv_cur_get_offsets": (_I, [_P, _P, _P, _P, _P]),
+    "tcv_cur_get_planes": (_I, [_P, _P, _P]),
+    "tcv_plan_workspace_bytes_var": (_S, [_I64, _P, _P, _I, _I, _I64, _P]),
+    "tcv_plan_build_var": (_I, [_PP, _P, _P, _P, _P, _I64, _P, _P, _I, _I, _I64, _P, _P, _S, _P]),
     "tcv_jit_prepare": (_I, [_I, _I]),
     "tcv_jit_enable": (None, [_I]),
     "tcv_jit_info": (ctypes.c_char_p, []),

@@ -134,6 +134,35 @@ class Plan:
             pass
 
 
+class VarPlan(Plan):
+    """A variable-width plan (tcv_plan_build_var): every sample grids with the footprint width of
+    its w-plane, s_size[wplane[k]] (current/tConvolveMPI/Benchmark.cc:373-452); s_size and c_off0
+    are per-plane host arrays."""
+
+    def __init__(self, iu, iv, coff, wplane, s_size, c_off0, g_size: int, c_len: int, tuning=None, stream=None):
+        import numpy as np
+        import torch
+
+        from ._lib import TcvTuning
+
+        self.n = iu.numel()
+        self.g_size, self.c_len = g_size, c_len
+        s_size = np.ascontiguousarray(s_size, np.int32)
+        c_off0 = np.ascontiguousarray(c_off0, np.int32)
+        t = TcvTuning(*(tuple(tuning) + (0, 0, 0, 0))[:4]) if tuning is not None else None
+        tp = ctypes.byref(t) if t is not None else None
+        sp, op = ctypes.c_void_p(s_size.ctypes.data), ctypes.c_void_p(c_off0.ctypes.data)
+        nbytes = lib().tcv_plan_workspace_bytes_var(self.n, sp, op, s_size.size, g_size, c_len, tp)
+        if nbytes == 0:
+            raise _lib.TcvError(1, "tcv_plan_workspace_bytes_var")
+        self.work = torch.empty(nbytes, dtype=torch.uint8, device=iu.device)
+        self._keep = (iu, iv, coff, wplane, s_size, c_off0)
+        self.handle = ctypes.c_void_p()
+        check(lib().tcv_plan_build_var(ctypes.byref(self.handle), _ptr(iu), _ptr(iv), _ptr(coff), _ptr(wplane), self.n,
+                                       sp, op, s_size.size, g_size, c_len, tp, _ptr(self.work), nbytes,
+                                       _stream(stream)), "tcv_plan_build_var")
+
+
 def grid_raw(data, support, c, c_type, c_scale, coff, iu, iv, grid, g_size, stream=None):
     """One call: plan + gridding (tcv_grid_raw), workspace allocated by torch."""
     import torch

@@ -312,6 +312,21 @@ tcv_status tcv_plan_build_tuned(tcv_plan **plan_out, const int32_t *d_iu, const 
                                 int64_t c_len, const tcv_tuning *tuning, void *d_work,
                                 size_t work_bytes, void *stream);
 
+/* Variable-width plans (the current/tConvolveMPI path, current/tConvolveMPI/Benchmark.cc:373-452):
+ * every sample grids with the footprint width of its w-plane, s_size[d_wplane[k]] (odd), at
+ * columns iu-s/2 .. and rows iv .. iv+s-1; the table holds the planes back to back from
+ * c_off0[plane].  s_size and c_off0 are host arrays of n_planes.  Complex table forms only
+ * (c64, cbf16, cf16: the w-term is complex); tuning as above, tile rows must be 16.  The plan
+ * keeps d_wplane for re-binning with tcv_plan_bin. */
+size_t tcv_plan_workspace_bytes_var(int64_t n, const int32_t *s_size, const int32_t *c_off0,
+                                    int n_planes, int g_size, int64_t c_len,
+                                    const tcv_tuning *tuning);
+tcv_status tcv_plan_build_var(tcv_plan **plan_out, const int32_t *d_iu, const int32_t *d_iv,
+                              const int32_t *d_coff, const int32_t *d_wplane, int64_t n,
+                              const int32_t *s_size, const int32_t *c_off0, int n_planes,
+                              int g_size, int64_t c_len, const tcv_tuning *tuning, void *d_work,
+                              size_t work_bytes, void *stream);
+
 /* Tile kernels specialised on the footprint width.  The first launch of the tile kernels for a
  * (table form, support) builds copies with sSize = 2*support+1 a compile-time constant (NVRTC,
  * about a second, cached for the process); tcv_jit_prepare builds them ahead of time (set-up;
@@ -456,6 +471,72 @@ typedef struct tcv_device_buffers {
     int32_t c_type;   /* type code of c_active, TCV_C_PADDED set on the TMA path */
 } tcv_device_buffers;
 tcv_status tcv_get_device_buffers(tcv_ctx *ctx, tcv_device_buffers *out);
+
+/* ------------------------------------------------------------------------------------------
+ * The variable-support benchmark of current/tConvolveMPI: samples of a 12 h track of the
+ * 36-antenna array (two generator draws each: baseline, hour angle), per-plane kernel widths and
+ * complex W-projection kernels.  Run types (current/tConvolveMPI/Benchmark.cc:64-158): 0 continuum
+ * (483 planes, widths 7..121, 6440^2 grid), 1 spectral line (135 planes, widths 7..19, 1034^2),
+ * 2 nearest neighbour (1 x 1), 3 7 x 7 kernels, 4 87 x 87 kernels (4129^2, no w-projection).
+ * ---------------------------------------------------------------------------------------- */
+typedef struct tcv_cur_geometry {
+    int32_t run_type, w_size, over_sample, support, g_size, n_baselines;
+    int64_t n_samples, c_len; /* samples (one channel), table entries */
+    int32_t s_min, s_max;     /* narrowest and widest plane */
+    double w_cell_size, uv_cell_size;
+} tcv_cur_geometry;
+/* Host: the run type's constants, as the reference derives them. */
+tcv_status tcv_cur_geometry_of(int run_type, tcv_cur_geometry *out);
+/* Host: sSize and cOffset0 per plane (arrays of w_size). */
+tcv_status tcv_cur_planes(int run_type, int32_t *s_size, int32_t *c_off0);
+/* u, v, w of every sample from generator state state0 (1 for a fresh reference object);
+ * *state_after (may be NULL) receives the state after the 2 * n_samples draws.  Synchronises. */
+tcv_status tcv_cur_init_uvw_raw(int run_type, uint64_t state0, double *d_u, double *d_v, double *d_w,
+                                uint64_t *state_after, void *stream);
+/* The normalised complex64 table (c_len entries).  Synchronises. */
+tcv_status tcv_cur_init_c_raw(int run_type, float *d_c, void *stream);
+/* iu, iv, w-plane and cOffset per sample (d_s_size, d_c_off0: device copies of tcv_cur_planes). */
+tcv_status tcv_cur_init_offsets_raw(int run_type, const double *d_u, const double *d_v,
+                                    const double *d_w, int64_t n, const int32_t *d_s_size,
+                                    const int32_t *d_c_off0, int32_t *d_iu, int32_t *d_iv,
+                                    int32_t *d_wplane, int32_t *d_coff, void *stream);
+/* Benchmark::requiredRate (current/tConvolveMPI/Benchmark.cc:697-739): rates[0] continuum,
+ * rates[1] spectral line, pixels per second per process. */
+void tcv_cur_required_rate(float *rates);
+
+/* The Benchmark object of current/tConvolveMPI (current/tConvolveMPI/Benchmark.h:38-111) with its
+ * buffers on one GPU.  As in the reference, init() may be called again after setRunType on the
+ * same object, and the generator continues where the previous init() left it. */
+typedef struct tcv_cur_ctx tcv_cur_ctx;
+tcv_status tcv_cur_create(int device, tcv_cur_ctx **out);
+void tcv_cur_destroy(tcv_cur_ctx *ctx);
+const char *tcv_cur_last_error(const tcv_cur_ctx *ctx);
+tcv_status tcv_cur_set_sort(tcv_cur_ctx *ctx, int sort);           /* setSort: 1 = by w-plane */
+tcv_status tcv_cur_set_run_type(tcv_cur_ctx *ctx, int run_type);   /* setRunType */
+int tcv_cur_get_run_type(const tcv_cur_ctx *ctx);
+/* Table form of the passes: TCV_C_C64 (plain), TCV_C_CBF16 or TCV_C_CF16. */
+tcv_status tcv_cur_set_ctype(tcv_cur_ctx *ctx, int c_type);
+/* Plane-group slice and work units of the plan (tile_rows must be 0 or 16). */
+tcv_status tcv_cur_set_tuning(tcv_cur_ctx *ctx, const tcv_tuning *tuning);
+tcv_status tcv_cur_init(tcv_cur_ctx *ctx);       /* Benchmark::init */
+tcv_status tcv_cur_run_grid(tcv_cur_ctx *ctx);   /* Benchmark::runGrid: grid += ... */
+tcv_status tcv_cur_run_degrid(tcv_cur_ctx *ctx); /* Benchmark::runDegrid: outdata = ... */
+tcv_status tcv_cur_sync(tcv_cur_ctx *ctx);
+void *tcv_cur_get_stream(const tcv_cur_ctx *ctx);
+int tcv_cur_support(const tcv_cur_ctx *ctx);                /* getSupport */
+int64_t tcv_cur_n_visibilities(const tcv_cur_ctx *ctx);     /* nVisibilitiesGridded */
+int64_t tcv_cur_n_pixels(const tcv_cur_ctx *ctx);           /* nPixelsGridded */
+uint64_t tcv_cur_generator_state(const tcv_cur_ctx *ctx);
+tcv_status tcv_cur_info(const tcv_cur_ctx *ctx, tcv_cur_geometry *g);
+tcv_status tcv_cur_set_data(tcv_cur_ctx *ctx, const float *vis, int64_t n);
+tcv_status tcv_cur_zero_grid(tcv_cur_ctx *ctx);
+tcv_status tcv_cur_get_grid(tcv_cur_ctx *ctx, float *grid);
+tcv_status tcv_cur_get_outdata(tcv_cur_ctx *ctx, float *vis, int64_t n);
+tcv_status tcv_cur_get_c(tcv_cur_ctx *ctx, float *c, int64_t n_entries);
+tcv_status tcv_cur_get_uvw(tcv_cur_ctx *ctx, double *u, double *v, double *w);
+tcv_status tcv_cur_get_offsets(tcv_cur_ctx *ctx, int32_t *iu, int32_t *iv, int32_t *wplane,
+                               int32_t *coff);
+tcv_status tcv_cur_get_planes(const tcv_cur_ctx *ctx, int32_t *s_size, int32_t *c_off0);
 
 #ifdef __cplusplus
 }

@@ -57,6 +57,8 @@ def lib():
         L.orc_cur_sort_by_plane.argtypes = [_I64, _I32, _P, _P, _P, _P]
         L.orc_cur_grid_f32.argtypes = [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _I32, _I32]
         L.orc_cur_degrid_f32.argtypes = [_P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P, _I32]
+        L.orc_cur_degrid_f64.argtypes = [_P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P, _I32]
+        L.orc_cur_grid_f64.argtypes = [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _I32, _I32]
         _lib = L
     return _lib
 
@@ -293,3 +295,22 @@ def cur_degrid_f32(grid, g_size: int, iu, iv, wp, co, s_size, c, threads: int = 
     lib().orc_cur_degrid_f32(_p(grid), g_size, iu.size, _p(iu), _p(iv), _p(wp), _p(co), _p(s_size), _p(c),
                              _p(out), threads)
     return out
+
+
+def cur_degrid_f64(grid, g_size: int, iu, iv, wp, co, s_size, c, threads: int = 1):
+    """Degridding of the same float grid and table with double accumulation: the value the FP32
+    sums of current/tConvolveMPI/Benchmark.cc:414-452 approximate (complex128)."""
+    grid = np.ascontiguousarray(grid, np.complex64)
+    out = np.empty(iu.size, np.complex128)
+    lib().orc_cur_degrid_f64(_p(grid), g_size, iu.size, _p(iu), _p(iv), _p(wp), _p(co), _p(s_size), _p(c),
+                             _p(out), threads)
+    return out
+
+
+def cur_grid_f64(data, iu, iv, wp, co, s_size, c, g_size: int, threads: int = 1):
+    """Gridding of the float data and table with double accumulation (complex128 grid)."""
+    data = np.ascontiguousarray(data, np.complex64)
+    grid = np.zeros(g_size * g_size, np.complex128)
+    lib().orc_cur_grid_f64(_p(data), data.size, _p(iu), _p(iv), _p(wp), _p(co), _p(s_size), _p(c), _p(grid),
+                           g_size, threads)
+    return grid

@@ -398,3 +398,93 @@ void orc_cur_degrid_f32(const float *grid, int g_size, int64_t n, const int32_t 
     }
     for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
 }
+
+/* Degridding with double accumulation of the same float grid and table (the exact answer the
+ * FP32 sums of current/tConvolveMPI/Benchmark.cc:414-452 approximate); out: interleaved doubles. */
+static void *cur_degrid64_range(void *arg)
+{
+    const cur_job *jb = (const cur_job *)arg;
+    double *out = (double *)(void *)jb->out;
+    for (int64_t d = jb->d0; d < jb->d1; ++d) {
+        const int s = jb->s_size[jb->wplane[d]];
+        const int64_t gind0 = (int64_t)jb->iu[d] + (int64_t)jb->g_size * jb->iv[d] - s / 2;
+        double re = 0.0, im = 0.0;
+        for (int sv = 0; sv < s; ++sv) {
+            const float *g = jb->grid_in + 2 * (gind0 + (int64_t)jb->g_size * sv);
+            const float *cp = jb->c + 2 * ((int64_t)jb->coff[d] + (int64_t)s * sv);
+            for (int su = 0; su < s; ++su) {
+                re += (double)g[2 * su] * cp[2 * su] - (double)g[2 * su + 1] * cp[2 * su + 1];
+                im += (double)g[2 * su + 1] * cp[2 * su] + (double)g[2 * su] * cp[2 * su + 1];
+            }
+        }
+        out[2 * d] = re;
+        out[2 * d + 1] = im;
+    }
+    return NULL;
+}
+
+void orc_cur_degrid_f64(const float *grid, int g_size, int64_t n, const int32_t *iu, const int32_t *iv,
+                        const int32_t *wplane, const int32_t *coff, const int32_t *s_size, const float *c,
+                        double *out, int threads)
+{
+    if (threads < 1) threads = 1;
+    if (threads > 64) threads = 64;
+    pthread_t th[64];
+    cur_job jobs[64];
+    for (int t = 0; t < threads; ++t) {
+        cur_job jb = {NULL, c, grid, iu, iv, wplane, coff, s_size, NULL, (float *)(void *)out, n, n * t / threads,
+                      n * (t + 1) / threads, g_size, 0, 0};
+        jobs[t] = jb;
+        pthread_create(&th[t], NULL, cur_degrid64_range, &jobs[t]);
+    }
+    for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+}
+
+/* Gridding with double accumulation (grid: interleaved doubles) of the float data and table: the
+ * exact answer the FP32 sums of current/tConvolveMPI/Benchmark.cc:373-411 approximate.  Row
+ * bands per thread, as orc_cur_grid_f32. */
+typedef struct {
+    const float *data, *c;
+    const int32_t *iu, *iv, *wplane, *coff, *s_size;
+    double *grid;
+    int64_t n;
+    int g_size, row0, row1;
+} cur_job64;
+
+static void *cur_grid64_rows(void *arg)
+{
+    const cur_job64 *jb = (const cur_job64 *)arg;
+    for (int64_t d = 0; d < jb->n; ++d) {
+        const int s = jb->s_size[jb->wplane[d]];
+        const int64_t gind0 = (int64_t)jb->iu[d] + (int64_t)jb->g_size * jb->iv[d] - s / 2;
+        const double dre = jb->data[2 * d], dim = jb->data[2 * d + 1];
+        for (int sv = 0; sv < s; ++sv) {
+            const int row = jb->iv[d] + sv;
+            if (row < jb->row0 || row >= jb->row1) continue;
+            double *g = jb->grid + 2 * (gind0 + (int64_t)jb->g_size * sv);
+            const float *cp = jb->c + 2 * ((int64_t)jb->coff[d] + (int64_t)s * sv);
+            for (int su = 0; su < s; ++su) {
+                g[2 * su] += dre * cp[2 * su] - dim * cp[2 * su + 1];
+                g[2 * su + 1] += dim * cp[2 * su] + dre * cp[2 * su + 1];
+            }
+        }
+    }
+    return NULL;
+}
+
+void orc_cur_grid_f64(const float *data, int64_t n, const int32_t *iu, const int32_t *iv, const int32_t *wplane,
+                      const int32_t *coff, const int32_t *s_size, const float *c, double *grid, int g_size,
+                      int threads)
+{
+    if (threads < 1) threads = 1;
+    if (threads > 64) threads = 64;
+    pthread_t th[64];
+    cur_job64 jobs[64];
+    for (int t = 0; t < threads; ++t) {
+        cur_job64 jb = {data, c, iu, iv, wplane, coff, s_size, grid, n, g_size,
+                        (int)((int64_t)g_size * t / threads), (int)((int64_t)g_size * (t + 1) / threads)};
+        jobs[t] = jb;
+        pthread_create(&th[t], NULL, cur_grid64_rows, &jobs[t]);
+    }
+    for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+}

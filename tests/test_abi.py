@@ -197,3 +197,34 @@ def test_server_argument_validation(tcv):
     if not torch.cuda.is_available():
         # a valid configuration needs the GPU: no CPU fallback
         assert L.tcv_server_create(ctypes.byref(cfg), ctypes.byref(srv)) == 4  # TCV_ERR_CUDA
+
+
+def test_current_geometry_matches_oracle(tcv, orc):
+    """The library's host-side geometry of the variable-support run types equals the oracle's
+    (itself pinned to the reference), and the plane tables match the reference's (sha256)."""
+    import json
+
+    from conftest import GOLDEN_DIR, sha
+    from tconvolve._lib import TcvCurGeometry
+
+    L = tcv.lib()
+    with open(os.path.join(GOLDEN_DIR, "current.json")) as f:
+        gold = json.load(f)["runs"]
+    for rt in range(5):
+        g = TcvCurGeometry()
+        assert L.tcv_cur_geometry_of(rt, ctypes.byref(g)) == 0
+        o = orc.cur_geometry(rt)
+        assert (g.w_size, g.over_sample, g.support, g.g_size, g.n_baselines, g.n_samples, g.c_len, g.s_max) == \
+            (o.w_size, o.over_sample, o.support, o.g_size, o.n_baselines, o.n_samples, o.c_len, o.s_max)
+        assert g.w_cell_size == o.w_cell_size and g.uv_cell_size == o.uv_cell_size
+        import numpy as np
+        s = np.empty(g.w_size, np.int32)
+        off = np.empty(g.w_size, np.int32)
+        assert L.tcv_cur_planes(rt, s.ctypes.data_as(ctypes.c_void_p), off.ctypes.data_as(ctypes.c_void_p)) == 0
+        assert sha(s) == gold[f"rt{rt}"]["sha256"]["ssize"] and sha(off) == gold[f"rt{rt}"]["sha256"]["coff0"]
+    assert L.tcv_cur_geometry_of(5, ctypes.byref(TcvCurGeometry())) == 1
+    rates = (ctypes.c_float * 2)()
+    L.tcv_cur_required_rate(rates)
+    # current/tConvolveMPI/Benchmark.cc:697-739 evaluated by hand
+    assert rates[0] == np.float32(10 * 5443200 * 10 * 3 * 3 * 400 / 5250.0)
+    assert rates[1] == np.float32(10 * 3758400 * 4 * 3 * 78 * 100 / 5500.0)
