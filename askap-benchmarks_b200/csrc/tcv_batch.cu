@@ -69,6 +69,12 @@ struct DevBuf {
 
 }  // namespace
 
+void tcv::tune_report_set(const std::vector<std::pair<tcv_tuning, float>>& report)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_report = report;
+}
+
 extern "C" {
 
 tcv_status tcv_graph_capture(tcv_graph** graph_out, tcv_plan* plan, int passes, const int32_t* d_iu,

@@ -14,6 +14,7 @@
 
 #include <cub/device/device_radix_sort.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -628,11 +629,105 @@ tcv_status tcv_cur_set_ctype(tcv_cur_ctx* c, int c_type)
 
 tcv_status tcv_cur_set_tuning(tcv_cur_ctx* c, const tcv_tuning* t)
 {
-    if (!c || !t || (t->tile_rows != 0 && t->tile_rows != 16) || t->group_mib < -1 || t->split < 0 ||
-        t->degrid_split < 0)
+    if (!c || !t || (t->tile_rows != 0 && t->tile_rows != 8 && t->tile_rows != 16) || t->group_mib < -1 ||
+        t->split < 0 || t->degrid_split < 0)
         return TCV_ERR_ARG;
-    c->tuning = tcv_tuning{16, t->group_mib ? t->group_mib : 32, t->split, t->degrid_split};
+    c->tuning = tcv_tuning{t->tile_rows ? t->tile_rows : 16, t->group_mib ? t->group_mib : 32, t->split, t->degrid_split};
     return c->initialized ? cur_build_plan(c) : TCV_OK;
+}
+
+tcv_status tcv_cur_tune(tcv_cur_ctx* c, int reps, tcv_tuning* best_out, float* best_ms_out)
+{
+    if (!c || reps < 1) return TCV_ERR_ARG;
+    if (!c->initialized) return cur_fail(c, TCV_ERR_STATE, "tune before init");
+    reps = std::min(reps, 50);
+    const size_t g2 = size_t(c->p.g_size) * c->p.g_size;
+    float2 *grid = nullptr, *out = nullptr;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaError_t e = cudaMalloc(&grid, g2 * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&out, size_t(std::max<int64_t>(c->n, 1)) * 8);
+    for (int k = 0; k < 3 && e == cudaSuccess; ++k) e = cudaEventCreate(&ev[k]);
+    std::vector<std::pair<tcv_tuning, float>> report;
+    tcv_tuning best = c->tuning;
+    float best_ms = -1.f;
+    tcv_status s = cuda_status(e);
+    // one candidate: build its plan, then (reps + 1) x (grid pass, degrid pass), the first untimed
+    auto time_one = [&](const tcv_tuning& t) -> tcv_status {
+        c->tuning = t;
+        tcv_status r = cur_build_plan(c);
+        if (r != TCV_OK) return r;
+        std::vector<float> ms;
+        for (int k = 0; k <= reps && r == TCV_OK; ++k) {
+            r = cuda_status(cudaMemsetAsync(grid, 0, g2 * 8, c->stream));
+            if (r == TCV_OK) r = cuda_status(cudaEventRecord(ev[0], c->stream));
+            if (r == TCV_OK)
+                r = tcv_plan_grid(c->plan, reinterpret_cast<const float*>(c->data), cur_table(c), c->c_type,
+                                  c->c_scale, reinterpret_cast<float*>(grid), c->stream);
+            if (r == TCV_OK)
+                r = tcv_plan_degrid(c->plan, reinterpret_cast<const float*>(grid), cur_table(c), c->c_type,
+                                    c->c_scale, reinterpret_cast<float*>(out), c->stream);
+            if (r == TCV_OK) r = cuda_status(cudaEventRecord(ev[1], c->stream));
+            if (r == TCV_OK) r = cuda_status(cudaEventSynchronize(ev[1]));
+            float m = 0.f;
+            if (r == TCV_OK) r = cuda_status(cudaEventElapsedTime(&m, ev[0], ev[1]));
+            if (k > 0) ms.push_back(m);
+        }
+        if (r != TCV_OK) return r;
+        std::sort(ms.begin(), ms.end());
+        const float med = ms[ms.size() / 2];
+        report.emplace_back(t, med);
+        if (best_ms < 0.f || med < best_ms) {
+            best_ms = med;
+            best = t;
+        }
+        return TCV_OK;
+    };
+    // stage 1: tile height x plane-group slice (slices that give the same grouping timed once)
+    if (s == TCV_OK) {
+        std::vector<std::pair<int, int>> seen;  // (rows, number of plane groups)
+        for (int rows : {16, 8})
+            for (int mib : {32, 128, -1}) {
+                const tcv_tuning t{rows, mib, 0, 0};
+                int groups = 1;
+                const int64_t budget = mib > 0 ? (int64_t(mib) << 20) : INT64_MAX;
+                int64_t used = 0;
+                for (int k = 0; k < c->p.w_size; ++k) {
+                    const int64_t end = k + 1 < c->p.w_size ? c->c_off0[size_t(k) + 1] : c->c_len;
+                    const int64_t bytes = (end - c->c_off0[size_t(k)]) * 8;
+                    if (used > 0 && used + bytes > budget) {
+                        ++groups;
+                        used = 0;
+                    }
+                    used += bytes;
+                }
+                const std::pair<int, int> id(rows, groups);
+                if (std::find(seen.begin(), seen.end(), id) != seen.end()) continue;
+                seen.push_back(id);
+                if ((s = time_one(t)) != TCV_OK) break;
+            }
+    }
+    if (s == TCV_OK) {  // stage 2: gridding work units
+        const tcv_tuning base = best;
+        for (int split : {256, 128, 64})  // the partial-tile bound grows as 1 / split
+            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, split, 0})) != TCV_OK) break;
+    }
+    if (s == TCV_OK) {  // stage 3: degridding work units
+        const tcv_tuning base = best;
+        for (int split : {128, 64, 32, 16})
+            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, base.split, split})) != TCV_OK) break;
+    }
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    if (grid) cudaFree(grid);
+    if (out) cudaFree(out);
+    if (s != TCV_OK) return cur_fail(c, s, "tuning candidate");
+    tune_report_set(report);
+    c->tuning = best;
+    CUR_TRY(c, cur_build_plan(c));
+    if (best_out) *best_out = best;
+    if (best_ms_out) *best_ms_out = best_ms;
+    return TCV_OK;
 }
 
 tcv_status tcv_cur_init(tcv_cur_ctx* c)

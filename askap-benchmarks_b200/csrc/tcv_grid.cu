@@ -102,9 +102,10 @@ template <class Tab>
 tcv_status grid_rows(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
                      cudaStream_t st, int c_type)
 {
-    if (p->g.var) {  // per-sample widths: complex tables (the w-term is complex), 64 x 64 tiles
+    if (p->g.var) {  // per-sample widths: complex tables (the w-term is complex), 64 x 64 or 64 x 32 tiles
         if constexpr (!Tab::kReal) {
             if (p->g.rows == 16) return launch<Tab, 16, true>(p, data, c, c_scale, grid, st, c_type);
+            if (p->g.rows == 8) return launch<Tab, 8, true>(p, data, c, c_scale, grid, st, c_type);
         }
         return TCV_ERR_UNSUPPORTED;
     }
@@ -123,6 +124,7 @@ tcv_status degrid_rows(const tcv_plan* p, const float2* grid, const void* c, flo
     if (p->g.var) {
         if constexpr (!Tab::kReal) {
             if (p->g.rows == 16) return launch_adjoint<Tab, 16, true>(p, grid, c, c_scale, out, st, c_type);
+            if (p->g.rows == 8) return launch_adjoint<Tab, 8, true>(p, grid, c, c_scale, out, st, c_type);
         }
         return TCV_ERR_UNSUPPORTED;
     }

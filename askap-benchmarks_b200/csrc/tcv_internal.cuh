@@ -6,6 +6,7 @@
 #include <cuda_fp16.h>
 #include <cstdint>
 #include <cstddef>
+#include <utility>
 #include <vector>
 
 #include "tconvolve.h"
@@ -139,6 +140,8 @@ tcv_status launch_degrid(const tcv_plan* p, const float2* grid, const void* c, i
 const void* jit_tile_kernel(int kind, int c_type, int s, int rows);
 // build both specialised tile kernels of (form, sSize, rows) ahead of a capture or a timing
 void jit_prepare(int c_type, int s, int rows);
+// Record the candidates and median times of the last tuning run (read by tcv_autotune_report).
+void tune_report_set(const std::vector<std::pair<tcv_tuning, float>>& report);
 
 // degridding on the gridding plan (tcv_grid.cu), and the per-sample slot sum it ends with
 tcv_status launch_degrid_tiles(const tcv_plan* p, const float2* grid, const void* c, int c_type,

@@ -173,6 +173,7 @@ SIGNATURES = {
     "tcv_cur_get_run_type": (_I, [_P]),
     "tcv_cur_set_ctype": (_I, [_P, _I]),
     "tcv_cur_set_tuning": (_I, [_P, _P]),
+    "tcv_cur_tune": (_I, [_P, _I, _P, _P]),
     "tcv_cur_init": (_I, [_P]),
     "tcv_cur_run_grid": (_I, [_P]),
     "tcv_cur_run_degrid": (_I, [_P]),
@@ -273,3 +274,13 @@ def check(status: int, what: str, ctx=None) -> None:
             msg = lib().tcv_last_error(ctx)
             extra = f" ({msg.decode()})" if msg else ""
         raise TcvError(status, what + extra)
+
+
+def autotune_report(cap: int = 64):
+    """Candidates and median ms of the last tuning run (tcv_autotune or tcv_cur_tune):
+    [((tile_rows, group_mib, split, degrid_split), ms), ...]."""
+    cands = (TcvTuning * cap)()
+    times = (ctypes.c_float * cap)()
+    n = ctypes.c_int()
+    check(lib().tcv_autotune_report(cands, times, cap, ctypes.byref(n)), "tcv_autotune_report")
+    return [(cands[i].as_tuple(), float(times[i])) for i in range(min(n.value, cap))]

@@ -11,7 +11,7 @@ from __future__ import annotations
 import ctypes
 
 from . import _lib
-from ._lib import TcvJob, TcvTuning, check, lib
+from ._lib import TcvJob, TcvTuning, autotune_report, check, lib
 from .raw import _ptr, _stream
 
 
@@ -141,13 +141,7 @@ def autotune(sizes, iu, iv, coff, data, c, c_type: int, support: int, c_scale: f
     check(lib().tcv_autotune(jobs, len(sizes), _ptr(iu), _ptr(iv), _ptr(coff), _ptr(data), _ptr(c), c_type,
                              c_scale, table_len(c, c_type), support, reps, ctypes.byref(best), ctypes.byref(ms),
                              _stream(stream)), "tcv_autotune")
-    cap = 64
-    cands = (TcvTuning * cap)()
-    times = (ctypes.c_float * cap)()
-    n = ctypes.c_int()
-    check(lib().tcv_autotune_report(cands, times, cap, ctypes.byref(n)), "tcv_autotune_report")
-    report = [(cands[i].as_tuple(), float(times[i])) for i in range(min(n.value, cap))]
-    return best.as_tuple(), float(ms.value), report
+    return best.as_tuple(), float(ms.value), autotune_report()
 
 
 def make_problem(sizes, w_size: int = 33, cell_size: float = 5.0, baseline: int = 2000, vis_seed: int = 0,

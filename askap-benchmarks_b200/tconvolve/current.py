@@ -45,6 +45,7 @@ def required_rate():
 class Benchmark:
     def __init__(self, device: int = 0):
         self._ctx = ctypes.c_void_p()
+        self._tuning = (16, 32, 0, 0)
         check(lib().tcv_cur_create(device, ctypes.byref(self._ctx)), "tcv_cur_create")
 
     def close(self):
@@ -108,9 +109,27 @@ class Benchmark:
             c_type = _lib.CTYPE_BY_NAME[c_type]
         check(lib().tcv_cur_set_ctype(self._ctx, int(c_type)), "tcv_cur_set_ctype")
 
-    def set_tuning(self, group_mib: int = 32, split: int = 0, degrid_split: int = 0):
-        t = TcvTuning(16, int(group_mib), int(split), int(degrid_split))
+    def set_tuning(self, group_mib: int = 32, split: int = 0, degrid_split: int = 0, tile_rows: int = 16):
+        """Plane-group slice, work-unit sizes and tile height (rows per warp, 8 or 16) of the plan."""
+        t = TcvTuning(int(tile_rows), int(group_mib), int(split), int(degrid_split))
         check(lib().tcv_cur_set_tuning(self._ctx, ctypes.byref(t)), "tcv_cur_set_tuning")
+        self._tuning = t.as_tuple()
+
+    def tuning(self):
+        """The plan's (tile_rows, group_mib, split, degrid_split)."""
+        return self._tuning
+
+    def tune(self, reps: int = 3):
+        """Autotune the plan on the initialised problem (tcv_cur_tune): keeps the fastest tuning
+        and returns it with its median ms per gridding + degridding pass, and the candidates
+        timed as [((rows, group_mib, split, degrid_split), ms), ...]."""
+        t = TcvTuning()
+        ms = ctypes.c_float()
+        st = lib().tcv_cur_tune(self._ctx, int(reps), ctypes.byref(t), ctypes.byref(ms))
+        if st != _lib.TCV_OK:
+            raise _lib.TcvError(st, "tcv_cur_tune (" + lib().tcv_cur_last_error(self._ctx).decode() + ")")
+        self._tuning = t.as_tuple()
+        return t.as_tuple(), float(ms.value), _lib.autotune_report()
 
     def geometry(self) -> TcvCurGeometry:
         g = TcvCurGeometry()

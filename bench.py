@@ -39,6 +39,7 @@ ALG_BYTES = {"grid": 24, "degrid": 16}  # per update: C 8 + grid read 8 (+ grid 
 FALLBACK_HBM_GBS = 6650.0
 L2_FLUSH_BYTES = 512 << 20
 REF_DRIVER = os.path.join(REPO, "oracle", "_ref", "c2", "ref_driver")
+REF_DRIVER_CURRENT = os.path.join(REPO, "oracle", "_ref", "current", "ref_driver_current")
 
 
 def parse_args():
@@ -62,6 +63,8 @@ def parse_args():
     p.add_argument("--no-batched", action="store_true", help="skip the 64-job batched measurement")
     p.add_argument("--no-serving", action="store_true", help="skip the serving (Poisson arrivals) measurement")
     p.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window per serving rate")
+    p.add_argument("--no-current", action="store_true",
+                   help="skip the variable-support (current/tConvolveMPI) continuum and spectral measurement")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=4.0, help="target wall time of the CPU sample")
     return p.parse_args()
@@ -90,6 +93,22 @@ def run_reference_cpu(threads: int, per_thread: int, steps: int, warmup: int):
             rates.append(2 * u / (g + d))
             step_s.append(g + d)
     return rates, step_s
+
+
+def run_reference_cpu_current(run_type: int, threads: int, steps: int, max_samples: int):
+    """The reference's current/tConvolveMPI Benchmark (oracle/_ref/current) on the host cores: one
+    object per thread (as one per MPI rank), each over the first max_samples samples."""
+    if not os.path.exists(REF_DRIVER_CURRENT):
+        raise RuntimeError(f"reference build missing: {REF_DRIVER_CURRENT}")
+    out = subprocess.run([REF_DRIVER_CURRENT, "time", str(run_type), str(threads), str(steps), str(max_samples)],
+                         check=True, capture_output=True, text=True, timeout=600).stdout
+    rates = []
+    for line in out.splitlines():
+        if line.startswith("step "):
+            f = line.split()
+            g, d, px = float(f[3]), float(f[5]), float(f[7])
+            rates.append({"grid_px_s": px / g, "degrid_px_s": px / d, "updates_per_s": 2 * px / (g + d)})
+    return rates
 
 
 def cpu_sample_size(threads: int, seconds: float) -> int:
@@ -408,8 +427,8 @@ def b200_arm(args):
                                     else "degrid_staged_kernel")}[(dom, args.path)]
 
     # the other workloads run after the headline's context is released
-    batched = serving = None
-    if not (args.no_batched and args.no_serving):
+    batched = serving = current = None
+    if not (args.no_batched and args.no_serving and args.no_current):
         b.close()
         torch.cuda.empty_cache()
     if not args.no_batched:
@@ -417,6 +436,9 @@ def b200_arm(args):
         torch.cuda.empty_cache()
     if not args.no_serving:
         serving = serving_section(args, local)
+    if not args.no_current:
+        current = current_section(args, torch, world)
+        torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -455,6 +477,7 @@ def b200_arm(args):
             "plain_form": plain,
             "batched": batched,
             "serving": serving,
+            "current": current,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * (8 + 4 * 3),
                     "d2h_bytes_per_step": n * 8, "ms_per_step": e2e_mean},
             "gpu_launches": launches_per_step * args.steps if launches_per_step else None,
@@ -466,7 +489,7 @@ def b200_arm(args):
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    if args.no_batched and args.no_serving:
+    if args.no_batched and args.no_serving and args.no_current:
         b.close()  # not released above
     if world > 1:
         dist.destroy_process_group()
@@ -576,6 +599,87 @@ def serving_section(args, device):
             "form": args.form if args.form in ("r32", "c64", "rbf16", "cbf16") else "r32",
             "hbm_budget_bytes": int(150e9), "bytes_held": st["bytes_held"], "slots": 2, "max_batch": 32,
             "latency": "submission to result-ready (server clock)", "rates": rates}
+
+
+def current_section(args, torch, world):
+    """The variable-support benchmark of current/tConvolveMPI (tConvolveMPI.cc:85-186): the
+    continuum run (6440^2 grid, 483 w-planes, kernels 7^2..121^2) and then the spectral-line run
+    (1034^2, 135 planes, 7^2..19^2) on one Benchmark object, unit visibilities as in the reference.
+    A step is runGrid + runDegrid; updates are nPixelsGridded per pass.  Each run is measured with
+    the default plan and with the plan tcv_cur_tune picks; the reference's own code is timed on the
+    host cores beside it (bounded sample)."""
+    from tconvolve.current import RUN_TYPES, Benchmark, required_rate
+
+    b = Benchmark()
+    b.setSort(0)
+    stream = torch.cuda.ExternalStream(b.stream) if b.stream else torch.cuda.current_stream()
+    res = {"workload": "current/tConvolveMPI: continuum then spectral line on one object (the generator "
+                       "continues), data 1+0i, wide-field 36-antenna track",
+           "step": "runGrid + runDegrid", "required_rate_px_s": dict(zip(("continuum", "spectral"), required_rate())),
+           "runs": {}}
+
+    def timed(k):
+        for _ in range(3):
+            b.runGrid()
+            b.runDegrid()
+        b.sync()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * k + 1)]
+        ev[0].record(stream)
+        for i in range(k):
+            b.runGrid()
+            ev[2 * i + 1].record(stream)
+            b.runDegrid()
+            ev[2 * i + 2].record(stream)
+        b.sync()
+        torch.cuda.synchronize()
+        g = [ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(k)]
+        d = [ev[2 * i + 1].elapsed_time(ev[2 * i + 2]) for i in range(k)]
+        gm, dm = statistics.median(g), statistics.median(d)
+        if world > 1:
+            from tconvolve import replicas
+            gm, dm = replicas.max_over_ranks([gm, dm], device="cuda")
+        return gm, dm
+
+    for rt in (0, 1):
+        b.setRunType(rt)
+        t0 = time.perf_counter()
+        b.init()
+        b.sync()
+        init_s = time.perf_counter() - t0
+        px = b.nPixelsGridded()
+        g = b.geometry()
+        entry = {"gSize": g.g_size, "wSize": g.w_size, "support": g.support, "samples": b.nVisibilitiesGridded(),
+                 "pixels_per_pass": px, "init_s": init_s}
+        gm, dm = timed(5)
+        entry["default"] = {"tuning": list(b.tuning()), "grid_ms": gm, "degrid_ms": dm,
+                            "value": world * 2 * px / ((gm + dm) * 1e-3)}
+        t0 = time.perf_counter()
+        best, _, report = b.tune(reps=3)
+        tune_s = time.perf_counter() - t0
+        gm, dm = timed(5)
+        entry["tuned"] = {"tuning": list(best), "autotune_s": tune_s, "grid_ms": gm, "degrid_ms": dm,
+                          "grid_px_s": px / (gm * 1e-3), "degrid_px_s": px / (dm * 1e-3),
+                          "value": world * 2 * px / ((gm + dm) * 1e-3), "unit": UNIT,
+                          "candidates": [[list(t), m] for t, m in report]}
+        if not args.no_cpu_baseline and world == 1:
+            threads = host_threads() if rt == 1 else min(host_threads(), 8)
+            sample = 400_000 if rt == 0 else 0  # continuum: a prefix; spectral: every sample
+            try:
+                r = run_reference_cpu_current(rt, threads, 2, sample)
+                best_r = max(r, key=lambda x: x["updates_per_s"])
+                what = f"first {sample} samples" if sample else "all samples"
+                entry["cpu_reference"] = dict(best_r, cores=threads, kind="reference",
+                                              sample=f"{threads} objects (one per thread) x {what}, "
+                                                     f"runGrid + runDegrid of current/tConvolveMPI/Benchmark.cc, "
+                                                     f"best of 2")
+            except (RuntimeError, subprocess.CalledProcessError, subprocess.TimeoutExpired, OSError) as e:
+                entry["cpu_reference"] = {"value": None, "sample": f"unavailable: {e}"}
+        res["runs"][RUN_TYPES[rt]] = entry
+    b.close()
+    return res
 
 
 def count_step_kernels(torch, step):

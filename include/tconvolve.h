@@ -316,7 +316,7 @@ tcv_status tcv_plan_build_tuned(tcv_plan **plan_out, const int32_t *d_iu, const 
  * every sample grids with the footprint width of its w-plane, s_size[d_wplane[k]] (odd), at
  * columns iu-s/2 .. and rows iv .. iv+s-1; the table holds the planes back to back from
  * c_off0[plane].  s_size and c_off0 are host arrays of n_planes.  Complex table forms only
- * (c64, cbf16, cf16: the w-term is complex); tuning as above, tile rows must be 16.  The plan
+ * (c64, cbf16, cf16: the w-term is complex); tuning as above, tile rows 8 or 16.  The plan
  * keeps d_wplane for re-binning with tcv_plan_bin. */
 size_t tcv_plan_workspace_bytes_var(int64_t n, const int32_t *s_size, const int32_t *c_off0,
                                     int n_planes, int g_size, int64_t c_len,
@@ -516,8 +516,14 @@ tcv_status tcv_cur_set_run_type(tcv_cur_ctx *ctx, int run_type);   /* setRunType
 int tcv_cur_get_run_type(const tcv_cur_ctx *ctx);
 /* Table form of the passes: TCV_C_C64 (plain), TCV_C_CBF16 or TCV_C_CF16. */
 tcv_status tcv_cur_set_ctype(tcv_cur_ctx *ctx, int c_type);
-/* Plane-group slice and work units of the plan (tile_rows must be 0 or 16). */
+/* Tile height, plane-group slice and work units of the plan (tile_rows 0 = 16, or 8). */
 tcv_status tcv_cur_set_tuning(tcv_cur_ctx *ctx, const tcv_tuning *tuning);
+/* Time one gridding and one degridding pass of the initialised problem per candidate tuning
+ * (median of reps, into scratch buffers: the context's grid and samples are left untouched) and
+ * keep the fastest: tile height x plane groups, then gridding work units, then degridding work
+ * units.  The candidates and their times are readable with tcv_autotune_report.  Set-up path:
+ * allocates and synchronises. */
+tcv_status tcv_cur_tune(tcv_cur_ctx *ctx, int reps, tcv_tuning *best_out, float *best_ms_out);
 tcv_status tcv_cur_init(tcv_cur_ctx *ctx);       /* Benchmark::init */
 tcv_status tcv_cur_run_grid(tcv_cur_ctx *ctx);   /* Benchmark::runGrid: grid += ... */
 tcv_status tcv_cur_run_degrid(tcv_cur_ctx *ctx); /* Benchmark::runDegrid: outdata = ... */

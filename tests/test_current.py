@@ -181,17 +181,11 @@ def test_current_reduced_forms(tcv, orc, cuda_ok, form, bound):
     b.close()
 
 
-@pytest.mark.parametrize("tuning", [(32, 0, 0), (8, 0, 64), (8, 64, 64), (-1, 256, 128)])
-def test_current_tunings_and_determinism(tcv, orc, cuda_ok, tuning):
-    """Plane groups and work units change the summation order only: every tuning within its bar
-    (module docstring), each bit-identical when rerun."""
-    from tconvolve.current import Benchmark
-
-    b = Benchmark()
-    b.setRunType(1)
-    b.init()
-    b.set_tuning(*tuning)
+def _check_tuned(b, orc):
+    """Grid + degrid twice (bit-identical), then the bars of the module docstring for the plan's
+    tuning: cells whole -> the reference's order; split cells -> against FP64."""
     iu, iv, wp, co = b.offsets()
+    b.zero_grid()
     b.runGrid()
     b.runDegrid()
     b.sync()
@@ -204,13 +198,50 @@ def test_current_tunings_and_determinism(tcv, orc, cuda_ok, tuning):
     c, grid_ref, out_ref = _oracle_run(orc, 1, iu, iv, wp, co)
     s_size, _ = b.planes()
     g = b.geometry()
-    if tuning[1] == 0:  # gridding cells whole: the reference's order at every point
+    split = b.tuning()[2]
+    if split == 0:  # gridding cells whole: the reference's order at every point
         assert orc.rel_l2(g1, grid_ref) <= REL_L2_FP32
     else:
         g64 = orc.cur_grid_f64(np.ones(iu.size, np.complex64), iu, iv, wp, co, s_size, c, g.g_size, threads=16)
         assert orc.rel_l2(g1, g64) <= 1.5 * orc.rel_l2(grid_ref, g64) + 1e-7
     o64 = orc.cur_degrid_f64(g1, g.g_size, iu, iv, wp, co, s_size, c, threads=16)
     assert orc.rel_l2(o1, o64) <= 1e-6
-    if tuning[1] == 0:
+    if split == 0:
         assert orc.rel_l2(o1, out_ref) <= REL_L2_FP32
+
+
+@pytest.mark.parametrize("tuning", [(32, 0, 0, 16), (8, 0, 64, 16), (8, 64, 64, 16), (-1, 256, 128, 16),
+                                    (32, 0, 0, 8), (-1, 128, 64, 8), (32, 256, 8, 8)])
+def test_current_tunings_and_determinism(tcv, orc, cuda_ok, tuning):
+    """Plane groups, work units and tile heights change the summation order only: every tuning
+    within its bar (module docstring), each bit-identical when rerun."""
+    from tconvolve.current import Benchmark
+
+    b = Benchmark()
+    b.setRunType(1)
+    b.init()
+    b.set_tuning(*tuning)
+    assert b.tuning() == (tuning[3],) + tuning[:3]
+    _check_tuned(b, orc)
+    b.close()
+
+
+def test_current_autotune(tcv, orc, cuda_ok):
+    """tcv_cur_tune keeps the fastest of the candidates it timed, leaves the object's grid alone,
+    and the tuned plan meets the bars of its tuning."""
+    from tconvolve.current import Benchmark
+
+    b = Benchmark()
+    b.setRunType(1)
+    b.init()
+    b.runGrid()
+    b.sync()
+    before = b.grid()
+    best, ms, report = b.tune(reps=2)
+    assert np.array_equal(b.grid(), before), "the tuner wrote into the object's grid"
+    assert best == b.tuning() and ms > 0
+    assert len(report) >= 9 and best in [t for t, _ in report]
+    assert ms == min(m for _, m in report)
+    assert {t[0] for t, _ in report} == {8, 16}
+    _check_tuned(b, orc)
     b.close()
