@@ -645,6 +645,7 @@ def current_section(args, torch, world):
 
     for rt in (0, 1):
         b.setRunType(rt)
+        b.set_tuning()  # the default plan first (a tuning stays with the object across init calls)
         t0 = time.perf_counter()
         b.init()
         b.sync()
