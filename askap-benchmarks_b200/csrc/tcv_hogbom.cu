@@ -1,0 +1,347 @@
+// tcv_hogbom.cu -- Hogbom CLEAN (the minor cycle) on the device.
+//
+// Reference: current/tHogbomCleanOMP/HogbomGolden.cc:47-141 (HogbomGolden::deconvolve, findPeak,
+// subtractPSF) and the same steps inside current/tMajorACC/tMajorACC.cc:689-877 (deconvolve).  Each
+// iteration takes the pixel of largest |residual| (the first such index, as the reference's strict
+// '>' scan in index order does), adds gain * peak to the model there, and subtracts
+// (gain * peak) * psf, shifted so that the PSF's own peak lands on that pixel, over the overlap of
+// the two images.  The arithmetic is the reference's, rounding by rounding: t = gain * peak,
+// u = t * psf, r = r - u, each rounded to float (no contraction into fused multiply-adds), so the
+// model and the residual are bit-identical to the reference's.
+//
+// The reference computes the PSF row as y - (ry - px) (its diffy uses the PSF peak's x,
+// HogbomGolden.cc:108); that is kept.  Where it points outside the PSF (only when the PSF peak is
+// off the diagonal) the reference reads out of bounds; here those rows are skipped and counted.
+//
+// B200 layout: one launch per iteration, no host round trip.  A launch subtracts the PSF over its
+// blocks' slices of the image and scans the updated values for the next peak in the same pass, so
+// an iteration reads the residual once, reads the PSF's overlap once and writes the overlap once.
+// Each block leaves one candidate, a 64-bit key (|value| bits << 32 | ~index: the largest key is
+// the largest magnitude at the smallest index) with its signed value; the last block to finish
+// (an atomic ticket, no waiting) reduces the candidates to the winner that the next launch reads.
+// The stop test (|peak| < threshold) is taken on the device: later launches see the flag and return.
+#include "tcv_internal.cuh"
+
+#include <algorithm>
+#include <cstdint>
+
+namespace tcv {
+namespace {
+
+constexpr int kHogThreads = 256;
+constexpr int kHogMaxBlocks = 592;  // 4 x 148
+
+// device state of one deconvolution (start of the caller's workspace; zeroed by the host)
+struct HogState {
+    unsigned long long win_key[3];  // winners: [0], [1] by iteration parity, [2] the PSF's
+    float win_val[3];
+    unsigned int arrived;           // blocks finished in the current launch
+    int stopped;                    // 1 + the iteration whose |peak| fell below the threshold; 0 = running
+    int done;                       // iterations carried out
+    unsigned int psf_pos;           // PSF peak index
+    unsigned long long skipped_rows;  // PSF rows outside the PSF (reference out-of-bounds reads)
+};
+
+struct HogArgs {
+    const float* psf;
+    float* residual;
+    float* model;
+    unsigned long long* keys;  // one candidate per block
+    float* vals;
+    HogState* state;
+    float* hist_val;         // per iteration: peak value (may be null)
+    unsigned int* hist_pos;  // per iteration: peak index (may be null)
+    int width, psf_width, nblocks;
+    long long n;  // width * width
+    float gain, threshold;
+};
+
+__device__ __forceinline__ unsigned long long peak_key(float v, unsigned int idx)
+{
+    return (static_cast<unsigned long long>(__float_as_uint(fabsf(v))) << 32) | static_cast<unsigned int>(~idx);
+}
+
+__device__ __forceinline__ unsigned int key_index(unsigned long long k) { return ~static_cast<unsigned int>(k); }
+
+// Block-wide maximum of (key, value); the winner is returned to every thread.
+__device__ unsigned long long block_max(unsigned long long k, float& v)
+{
+    __shared__ unsigned long long sk[kHogThreads / 32];
+    __shared__ float sv[kHogThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long ko = __shfl_down_sync(0xffffffffu, k, o);
+        const float vo = __shfl_down_sync(0xffffffffu, v, o);
+        if (ko > k) {
+            k = ko;
+            v = vo;
+        }
+    }
+    const int w = threadIdx.x >> 5;
+    __syncthreads();  // earlier readers of sk/sv are done
+    if ((threadIdx.x & 31) == 0) {
+        sk[w] = k;
+        sv[w] = v;
+    }
+    __syncthreads();
+    k = sk[0];
+    v = sv[0];
+    for (int i = 1; i < kHogThreads / 32; ++i)
+        if (sk[i] > k) {
+            k = sk[i];
+            v = sv[i];
+        }
+    return k;
+}
+
+// Leave this block's candidate; the last block of the launch reduces all of them into
+// state->win_key/win_val[slot] (and for the PSF slot, the PSF peak position).
+__device__ void finish_scan(unsigned long long best, float bv, unsigned long long* keys, float* vals, int nblocks,
+                            HogState* st, int slot)
+{
+    best = block_max(best, bv);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        keys[blockIdx.x] = best;
+        vals[blockIdx.x] = bv;
+        __threadfence();
+        last = atomicAdd(&st->arrived, 1u) == unsigned(nblocks - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    unsigned long long k = 0;
+    float v = 0.f;
+    for (int i = threadIdx.x; i < nblocks; i += kHogThreads) {
+        const unsigned long long ki = __ldcg(keys + i);
+        if (ki > k) {
+            k = ki;
+            v = __ldcg(vals + i);
+        }
+    }
+    k = block_max(k, v);
+    if (threadIdx.x == 0) {
+        const bool zero = (k >> 32) == 0;  // an all-zero image: the reference keeps maxPos = 0, maxVal = 0
+        st->win_key[slot] = zero ? static_cast<unsigned long long>(~0u) : k;
+        st->win_val[slot] = zero ? 0.f : v;
+        if (slot == 2) st->psf_pos = zero ? 0u : key_index(k);
+        st->arrived = 0;
+    }
+}
+
+// Scan an image (copying it to copy_to when given) for its peak.
+__global__ void __launch_bounds__(kHogThreads) hog_scan_kernel(const float* __restrict__ img, float* __restrict__ copy_to,
+                                                               long long n, int nblocks, unsigned long long* keys,
+                                                               float* vals, HogState* st, int slot)
+{
+    const long long per = (n + nblocks - 1) / nblocks;
+    const long long lo = per * blockIdx.x, hi = min(n, lo + per);
+    unsigned long long best = 0;
+    float bv = 0.f;
+    for (long long i = lo + threadIdx.x; i < hi; i += kHogThreads) {
+        const float v = img[i];
+        if (copy_to) copy_to[i] = v;
+        const unsigned long long k = peak_key(v, static_cast<unsigned int>(i));
+        if (k > best) {
+            best = k;
+            bv = v;
+        }
+    }
+    finish_scan(best, bv, keys, vals, nblocks, st, slot);
+}
+
+__device__ __forceinline__ void take(float r, long long i, unsigned long long& best, float& bv)
+{
+    const unsigned long long k = peak_key(r, static_cast<unsigned int>(i));
+    if (k > best) {
+        best = k;
+        bv = r;
+    }
+}
+
+// One iteration: the previous scan's peak, the model update, the PSF subtraction over this block's
+// slice and the scan of the updated slice.  kVec: width a multiple of 4 and the residual 16-byte
+// aligned (float4 residual I/O).
+template <bool kVec>
+__global__ void __launch_bounds__(kHogThreads) hog_iter_kernel(HogArgs a, int it)
+{
+    HogState* st = a.state;
+    if (st->stopped) return;  // an earlier launch stopped the loop
+    const int par = it & 1;
+    const unsigned long long pk = st->win_key[par];
+    const unsigned int ppos = key_index(pk);
+    const float peak = st->win_val[par];
+    if (fabsf(peak) < a.threshold) {  // HogbomGolden.cc:86-89
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->stopped = it + 1;
+        return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // model[absPeakPos] += absPeakVal * g_gain (HogbomGolden.cc:93)
+        a.model[ppos] = __fadd_rn(a.model[ppos], __fmul_rn(peak, a.gain));
+        if (a.hist_val) a.hist_val[it] = peak;
+        if (a.hist_pos) a.hist_pos[it] = ppos;
+        st->done = it + 1;
+    }
+    // subtractPSF (HogbomGolden.cc:99-124)
+    const int W = a.width, P = a.psf_width;
+    const int rx = int(ppos % unsigned(W)), ry = int(ppos / unsigned(W));
+    const int px = int(st->psf_pos % unsigned(P)), py = int(st->psf_pos / unsigned(P));
+    const int diffx = rx - px, diffy = ry - px;  // diffy uses px, as the reference does
+    const int startx = max(0, rx - px), starty = max(0, ry - py);
+    const int stopx = min(W - 1, rx + (P - px - 1)), stopy = min(W - 1, ry + (P - py - 1));
+    const float t = __fmul_rn(a.gain, peak);
+
+    const long long per = ((a.n + a.nblocks - 1) / a.nblocks + 3) & ~3LL;
+    const long long lo = per * blockIdx.x, hi = min(a.n, lo + per);
+    unsigned long long best = 0;
+    float bv = 0.f;
+    unsigned long long skipped = 0;
+    if (kVec) {
+        for (long long i = lo + 4 * threadIdx.x; i < hi; i += 4 * kHogThreads) {
+            const unsigned ui = unsigned(i);  // n < 2^32
+            const int y = int(ui / unsigned(W)), x0 = int(ui - unsigned(y) * unsigned(W));
+            float4 r = __ldcg(reinterpret_cast<const float4*>(a.residual + i));
+            const int prow = y - diffy;
+            const bool row_in = y >= starty && y <= stopy;
+            const bool prow_ok = prow >= 0 && prow < P;
+            if (row_in && prow_ok && x0 + 3 >= startx && x0 <= stopx) {
+                const long long pbase = (long long)prow * P - diffx;  // + x: inside the PSF row for x in range
+                float* rv = reinterpret_cast<float*>(&r);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int x = x0 + j;
+                    if (x >= startx && x <= stopx) rv[j] = __fsub_rn(rv[j], __fmul_rn(t, __ldg(a.psf + (pbase + x))));
+                }
+                __stcg(reinterpret_cast<float4*>(a.residual + i), r);
+            } else if (row_in && !prow_ok && x0 == 0) {
+                ++skipped;
+            }
+            take(r.x, i, best, bv);
+            take(r.y, i + 1, best, bv);
+            take(r.z, i + 2, best, bv);
+            take(r.w, i + 3, best, bv);
+        }
+    } else {
+        for (long long i = lo + threadIdx.x; i < hi; i += kHogThreads) {
+            const unsigned ui = unsigned(i);
+            const int y = int(ui / unsigned(W)), x = int(ui - unsigned(y) * unsigned(W));
+            float r = a.residual[i];
+            const int prow = y - diffy;
+            if (y >= starty && y <= stopy && x >= startx && x <= stopx) {
+                if (prow >= 0 && prow < P) {
+                    r = __fsub_rn(r, __fmul_rn(t, a.psf[(long long)prow * P + (x - diffx)]));
+                    a.residual[i] = r;
+                } else if (x == startx) {
+                    ++skipped;
+                }
+            }
+            take(r, i, best, bv);
+        }
+    }
+    if (skipped) atomicAdd(&st->skipped_rows, skipped);
+    finish_scan(best, bv, a.keys, a.vals, a.nblocks, st, par ^ 1);
+}
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+int hog_blocks(long long n)
+{
+    const long long want = (n + 4095) / 4096;  // at least ~4096 pixels per block
+    return int(std::max<long long>(1, std::min<long long>(kHogMaxBlocks, want)));
+}
+
+}  // namespace
+}  // namespace tcv
+
+using namespace tcv;
+
+extern "C" {
+
+size_t tcv_hogbom_workspace_bytes(int width)
+{
+    if (width < 1) return 0;
+    return align256(sizeof(HogState)) + align256(size_t(kHogMaxBlocks) * 8) + align256(size_t(kHogMaxBlocks) * 4);
+}
+
+tcv_status tcv_hogbom_deconvolve(const float* d_dirty, int width, const float* d_psf, int psf_width, float* d_model,
+                                 float* d_residual, int niters, float gain, float threshold, float* d_hist_val,
+                                 uint32_t* d_hist_pos, void* d_work, size_t work_bytes, void* stream)
+{
+    if (!d_dirty || !d_psf || !d_model || !d_residual || !d_work || width < 1 || psf_width < 1 || niters < 0)
+        return TCV_ERR_ARG;
+    if (uint64_t(width) * uint64_t(width) >= 0xffffffffull || uint64_t(psf_width) * uint64_t(psf_width) >= 0xffffffffull)
+        return TCV_ERR_UNSUPPORTED;
+    if (work_bytes < tcv_hogbom_workspace_bytes(width)) return TCV_ERR_WORKSPACE;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    char* w = static_cast<char*>(d_work);
+    HogArgs a{};
+    a.state = reinterpret_cast<HogState*>(w);
+    a.keys = reinterpret_cast<unsigned long long*>(w + align256(sizeof(HogState)));
+    a.vals = reinterpret_cast<float*>(w + align256(sizeof(HogState)) + align256(size_t(kHogMaxBlocks) * 8));
+    a.psf = d_psf;
+    a.residual = d_residual;
+    a.model = d_model;
+    a.hist_val = d_hist_val;
+    a.hist_pos = d_hist_pos;
+    a.width = width;
+    a.psf_width = psf_width;
+    a.n = (long long)width * width;
+    a.nblocks = hog_blocks(a.n);
+    a.gain = gain;
+    a.threshold = threshold;
+    TCV_CUDA(cudaMemsetAsync(a.state, 0, sizeof(HogState), st));
+    // the PSF's peak (HogbomGolden.cc:73-76), then residual = dirty with the first scan (:70)
+    const long long np = (long long)psf_width * psf_width;
+    const int pb = hog_blocks(np);
+    hog_scan_kernel<<<pb, kHogThreads, 0, st>>>(d_psf, nullptr, np, pb, a.keys, a.vals, a.state, 2);
+    TCV_CUDA(cudaGetLastError());
+    hog_scan_kernel<<<a.nblocks, kHogThreads, 0, st>>>(d_dirty, d_residual, a.n, a.nblocks, a.keys, a.vals, a.state, 0);
+    TCV_CUDA(cudaGetLastError());
+    const bool vec = width % 4 == 0 && reinterpret_cast<uintptr_t>(d_residual) % 16 == 0;
+    for (int it = 0; it < niters; ++it) {
+        if (vec)
+            hog_iter_kernel<true><<<a.nblocks, kHogThreads, 0, st>>>(a, it);
+        else
+            hog_iter_kernel<false><<<a.nblocks, kHogThreads, 0, st>>>(a, it);
+    }
+    TCV_CUDA(cudaGetLastError());
+    return TCV_OK;
+}
+
+tcv_status tcv_hogbom_result(const void* d_work, int* iters_done, int* stopped_at, int64_t* skipped_rows,
+                             int64_t* psf_peak_pos, void* stream)
+{
+    if (!d_work) return TCV_ERR_ARG;
+    HogState h{};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    TCV_CUDA(cudaMemcpyAsync(&h, d_work, sizeof(h), cudaMemcpyDeviceToHost, st));
+    TCV_CUDA(cudaStreamSynchronize(st));
+    if (iters_done) *iters_done = h.done;
+    if (stopped_at) *stopped_at = h.stopped - 1;
+    if (skipped_rows) *skipped_rows = int64_t(h.skipped_rows);
+    if (psf_peak_pos) *psf_peak_pos = int64_t(h.psf_pos);
+    return TCV_OK;
+}
+
+tcv_status tcv_find_peak(const float* d_image, int64_t n, float* val_out, int64_t* pos_out, void* d_work,
+                         size_t work_bytes, void* stream)
+{
+    if (!d_image || n < 1 || !d_work || n >= int64_t(0xffffffffll)) return TCV_ERR_ARG;
+    if (work_bytes < tcv_hogbom_workspace_bytes(1)) return TCV_ERR_WORKSPACE;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    char* w = static_cast<char*>(d_work);
+    HogState* state = reinterpret_cast<HogState*>(w);
+    unsigned long long* keys = reinterpret_cast<unsigned long long*>(w + align256(sizeof(HogState)));
+    float* vals = reinterpret_cast<float*>(w + align256(sizeof(HogState)) + align256(size_t(kHogMaxBlocks) * 8));
+    TCV_CUDA(cudaMemsetAsync(state, 0, sizeof(HogState), st));
+    const int nb = hog_blocks(n);
+    hog_scan_kernel<<<nb, kHogThreads, 0, st>>>(d_image, nullptr, n, nb, keys, vals, state, 0);
+    TCV_CUDA(cudaGetLastError());
+    HogState h{};
+    TCV_CUDA(cudaMemcpyAsync(&h, state, sizeof(h), cudaMemcpyDeviceToHost, st));
+    TCV_CUDA(cudaStreamSynchronize(st));
+    if (val_out) *val_out = h.win_val[0];
+    if (pos_out) *pos_out = int64_t(~static_cast<unsigned int>(h.win_key[0]));
+    return TCV_OK;
+}
+
+}  // extern "C"

@@ -174,6 +174,10 @@ SIGNATURES = {
     "tcv_cur_set_ctype": (_I, [_P, _I]),
     "tcv_cur_set_tuning": (_I, [_P, _P]),
     "tcv_cur_tune": (_I, [_P, _I, _P, _P]),
+    "tcv_hogbom_workspace_bytes": (_S, [_I]),
+    "tcv_hogbom_deconvolve": (_I, [_P, _I, _P, _I, _P, _P, _I, _F, _F, _P, _P, _P, _S, _P]),
+    "tcv_hogbom_result": (_I, [_P, _P, _P, _P, _P, _P]),
+    "tcv_find_peak": (_I, [_P, _I64, _P, _P, _P, _S, _P]),
     "tcv_cur_init": (_I, [_P]),
     "tcv_cur_run_grid": (_I, [_P]),
     "tcv_cur_run_degrid": (_I, [_P]),

@@ -86,3 +86,62 @@ def batch_sizes(n_jobs: int = 64, seed: int = 0, n_min: float = 1e4, n_max: floa
     n = np.exp(rng.uniform(math.log(n_min), math.log(n_max), n_jobs)).astype(np.int64)
     g = rng.choice(np.asarray(g_sizes, dtype=np.int64), n_jobs)
     return [(int(a), int(b)) for a, b in zip(n, g)]
+
+
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    """SplitMix64 finaliser on uint64 counters (exact integer arithmetic, same bits everywhere)."""
+    with np.errstate(over="ignore"):
+        z = x + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def synthetic_psf(width: int, scale: float | None = None) -> np.ndarray:
+    """A point-spread function of width x width float32 pixels with its peak, 1.0, at
+    (width/2, width/2) and a negative sidelobe ring decaying as 1/r^2: psf(r) = (1 - r^2 / 2s^2) /
+    (1 + r^2 / s^2)^2 with s = width / 64 (at least 2).  Rational arithmetic in float64 only (no
+    transcendental functions), so the same bits on every host.  It stands in for the reference's
+    psf_<width>.img inputs of current/tHogbomCleanOMP, which are not in its tree."""
+    s = float(scale) if scale else max(2.0, width / 64.0)
+    c = width // 2
+    d = np.arange(width, dtype=np.float64) - c
+    r2 = d[:, None] ** 2 + d[None, :] ** 2
+    s2 = s * s
+    q = 1.0 + r2 / s2
+    return ((1.0 - r2 / (2.0 * s2)) / (q * q)).astype(np.float32)
+
+
+def synthetic_dirty(width: int, n_sources: int = 20, noise: float = 1e-3, seed: int = 0,
+                    psf_scale: float | None = None) -> np.ndarray:
+    """A dirty image of width x width float32 pixels: n_sources point sources, each the
+    synthetic_psf shape centred on its pixel with amplitude in [0.1, 1), plus uniform noise in
+    [-noise/2, noise/2).  Positions and amplitudes come from the reference's K&R generator
+    (state seed + 1, three draws per source: x, y, amplitude), positions in the inner 80% of the
+    image; the noise from SplitMix64 of the pixel index and seed.  Float64 rational arithmetic,
+    rounded to float32 once."""
+    s = float(psf_scale) if psf_scale else max(2.0, width / 64.0)
+    s2 = s * s
+    state = seed + 1
+    maxint = 2147483647
+
+    def draw():
+        nonlocal state
+        state = (state * 1103515245 + 12345) & 0xFFFFFFFFFFFFFFFF
+        return ((state // 65536) & 0xFFFFFFFF) % maxint
+
+    img = np.zeros((width, width), np.float64)
+    d = np.arange(width, dtype=np.float64)
+    lo, span = int(0.1 * width), max(1, int(0.8 * width))
+    for _ in range(n_sources):
+        x = lo + int(span * (draw() / maxint))
+        y = lo + int(span * (draw() / maxint))
+        a = 0.1 + 0.9 * (draw() / maxint)
+        r2 = (d[:, None] - y) ** 2 + (d[None, :] - x) ** 2
+        q = 1.0 + r2 / s2
+        img += a * (1.0 - r2 / (2.0 * s2)) / (q * q)
+    if noise:
+        idx = np.arange(width * width, dtype=np.uint64) + np.uint64(seed) * np.uint64(0x100000000)
+        u = (_splitmix64(idx) >> np.uint64(11)).astype(np.float64) / float(1 << 53)
+        img += (noise * (u - 0.5)).reshape(width, width)
+    return img.astype(np.float32)

@@ -544,6 +544,35 @@ tcv_status tcv_cur_get_offsets(tcv_cur_ctx *ctx, int32_t *iu, int32_t *iv, int32
                                int32_t *coff);
 tcv_status tcv_cur_get_planes(const tcv_cur_ctx *ctx, int32_t *s_size, int32_t *c_off0);
 
+/* ------------------------------------------------------------------------------------------
+ * Hogbom CLEAN, the minor cycle (current/tHogbomCleanOMP/HogbomGolden.cc:47-141,
+ * attic/tHogbomCleanCuda/HogbomCuda.cu:81-202; the same steps in current/tMajorACC/tMajorACC.cc:689-877).
+ * Images are float, row-major, square: the dirty image and the residual width x width, the PSF
+ * psf_width x psf_width.  Results are bit-identical to the reference's (its float roundings, no
+ * fused multiply-adds).  The reference's PSF row index y - (ry - px) is kept; where it falls outside
+ * the PSF (PSF peak off the diagonal) the reference reads out of bounds, here the row is skipped
+ * and counted (tcv_hogbom_result).
+ * ---------------------------------------------------------------------------------------- */
+size_t tcv_hogbom_workspace_bytes(int width);
+/* residual = dirty, then niters iterations (fewer once |peak| < threshold, HogbomGolden.cc:86-89;
+ * threshold 0 never stops, as tMajorACC's loop): model[peak] += peak * gain; residual -= (gain *
+ * peak) * shifted psf.  The model is accumulated into (the reference zeroes it first).  d_hist_val /
+ * d_hist_pos (device, niters entries, may be NULL) receive each iteration's peak value and index.
+ * Asynchronous on the stream: all iterations are issued without waiting; d_work must stay
+ * allocated until they finish. */
+tcv_status tcv_hogbom_deconvolve(const float *d_dirty, int width, const float *d_psf, int psf_width,
+                                 float *d_model, float *d_residual, int niters, float gain,
+                                 float threshold, float *d_hist_val, uint32_t *d_hist_pos,
+                                 void *d_work, size_t work_bytes, void *stream);
+/* After tcv_hogbom_deconvolve (synchronises): iterations done, the iteration that met the
+ * threshold (-1 if none), PSF rows skipped, the PSF peak index.  Any output may be NULL. */
+tcv_status tcv_hogbom_result(const void *d_work, int *iters_done, int *stopped_at,
+                             int64_t *skipped_rows, int64_t *psf_peak_pos, void *stream);
+/* findPeak (HogbomGolden.cc:127-139): the value of largest magnitude and its first index
+ * (0 and 0 for an all-zero image).  Synchronises; d_work as for tcv_hogbom_deconvolve. */
+tcv_status tcv_find_peak(const float *d_image, int64_t n, float *val_out, int64_t *pos_out,
+                         void *d_work, size_t work_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,12 @@ def lib():
         L.orc_cur_degrid_f32.argtypes = [_P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P, _I32]
         L.orc_cur_degrid_f64.argtypes = [_P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P, _I32]
         L.orc_cur_grid_f64.argtypes = [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _I32, _I32]
+        L.orc_find_peak.argtypes = [_P, _I64, _P, _P]
+        L.orc_subtract_psf.argtypes = [_P, _I32, _P, _I32, _I64, _I64, ctypes.c_float, ctypes.c_float]
+        L.orc_subtract_psf.restype = _I64
+        L.orc_hogbom.argtypes = [_P, _I32, _P, _I32, _P, _P, _I32, ctypes.c_float, ctypes.c_float, _P, _P, _P,
+                                 _P, _P]
+        L.orc_hogbom.restype = _I32
         _lib = L
     return _lib
 
@@ -314,3 +320,37 @@ def cur_grid_f64(data, iu, iv, wp, co, s_size, c, g_size: int, threads: int = 1)
     lib().orc_cur_grid_f64(_p(data), data.size, _p(iu), _p(iv), _p(wp), _p(co), _p(s_size), _p(c), _p(grid),
                            g_size, threads)
     return grid
+
+
+# ---- Hogbom CLEAN (tconvolve_oracle_hogbom.c; current/tHogbomCleanOMP/HogbomGolden.cc:47-141) ----
+def find_peak(image: np.ndarray):
+    """findPeak (HogbomGolden.cc:127-139): (value, first index) of the largest |value|."""
+    img = np.ascontiguousarray(image, dtype=np.float32).ravel()
+    v = ctypes.c_float()
+    p = ctypes.c_int64()
+    lib().orc_find_peak(_p(img), img.size, ctypes.byref(v), ctypes.byref(p))
+    return float(v.value), int(p.value)
+
+
+def hogbom(dirty: np.ndarray, psf: np.ndarray, niters: int, gain: float = 0.1, threshold: float = 0.0,
+           model: np.ndarray | None = None):
+    """HogbomGolden::deconvolve (HogbomGolden.cc:62-97) on square float images.  Returns a dict
+    with model, residual, iterations done, stop iteration (-1), per-iteration peaks and the PSF
+    rows skipped (reference out-of-bounds reads)."""
+    d = np.ascontiguousarray(dirty, dtype=np.float32)
+    p = np.ascontiguousarray(psf, dtype=np.float32)
+    w, pw = int(round(np.sqrt(d.size))), int(round(np.sqrt(p.size)))
+    assert w * w == d.size and pw * pw == p.size
+    m = np.zeros(d.size, np.float32) if model is None else np.ascontiguousarray(model, dtype=np.float32).ravel().copy()
+    r = np.empty(d.size, np.float32)
+    hv = np.zeros(max(niters, 1), np.float32)
+    hp = np.zeros(max(niters, 1), np.int64)
+    stopped = ctypes.c_int()
+    skipped = ctypes.c_int64()
+    ppos = ctypes.c_int64()
+    done = lib().orc_hogbom(_p(d), w, _p(p), pw, _p(m), _p(r), int(niters), ctypes.c_float(gain),
+                            ctypes.c_float(threshold), _p(hv), _p(hp), ctypes.byref(stopped), ctypes.byref(skipped),
+                            ctypes.byref(ppos))
+    return {"model": m, "residual": r, "done": int(done), "stopped_at": int(stopped.value),
+            "hist_val": hv[:done], "hist_pos": hp[:done], "skipped_rows": int(skipped.value),
+            "psf_peak_pos": int(ppos.value)}
