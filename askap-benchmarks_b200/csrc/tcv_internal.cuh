@@ -140,6 +140,11 @@ tcv_status launch_degrid(const tcv_plan* p, const float2* grid, const void* c, i
 const void* jit_tile_kernel(int kind, int c_type, int s, int rows);
 // build both specialised tile kernels of (form, sSize, rows) ahead of a capture or a timing
 void jit_prepare(int c_type, int s, int rows);
+// FFT steps (tcv_fft.cu): fftExec in place; the inverse transform of a grid fused with fftFix into
+// a float image (and/or a complex one); the forward transform of a real image into a grid.
+tcv_status fft_exec(float2* d_grid, int n, bool forward, cudaStream_t st);
+tcv_status image_from_grid(float2* d_grid, int n, float scale, float* d_image, float2* d_image_c, cudaStream_t st);
+tcv_status grid_from_image(const float* d_image, int n, float2* d_grid, cudaStream_t st);
 // Record the candidates and median times of the last tuning run (read by tcv_autotune_report).
 void tune_report_set(const std::vector<std::pair<tcv_tuning, float>>& report);
 
@@ -195,6 +200,12 @@ inline tcv_status cuda_status(cudaError_t e)
 }
 
 }  // namespace tcv
+
+#define TCV_CHECK(call)                    \
+    do {                                   \
+        const tcv_status _s = (call);      \
+        if (_s != TCV_OK) return _s;       \
+    } while (0)
 
 #define TCV_CUDA(call)                                         \
     do {                                                       \

@@ -278,12 +278,6 @@ size_t cub_temp_bytes(const PlanGeom& g)
     return std::max(std::max(std::max(a, b), std::max(c, d)), std::max(e, f));
 }
 
-#define TCV_CHECK(call)                    \
-    do {                                   \
-        const tcv_status _s = (call);      \
-        if (_s != TCV_OK) return _s;       \
-    } while (0)
-
 // the unit list of one unit size over the plan's non-empty cells, with its per-group ranges
 tcv_status build_units(tcv_plan* p, int split, uint32_t* nunits, uint32_t* ustart, uint32_t* pstart, uint4* units,
                        uint32_t* group_ustart, cudaStream_t st)

@@ -100,6 +100,20 @@ class TcvRequestInfo(ctypes.Structure):
 REQ_GRID, REQ_DEGRID = 0, 1
 
 
+class TcvMajorConfig(ctypes.Structure):
+    _fields_ = [
+        ("n_samples", ctypes.c_int64), ("w_size", ctypes.c_int32), ("n_chan", ctypes.c_int32),
+        ("cell_size", ctypes.c_double), ("g_size", ctypes.c_int32), ("baseline", ctypes.c_int32),
+        ("n_major", ctypes.c_int32), ("n_minor", ctypes.c_int32), ("gain", ctypes.c_float),
+        ("n_sources", ctypes.c_int32), ("device", ctypes.c_int32), ("keep_stages", ctypes.c_int32),
+        ("tuning", TcvTuning),
+    ]
+
+
+MAJOR_STAGES = ("psf_grid", "psf_ifft", "grid", "ifft", "hogbom", "fft", "degrid", "subtract")
+IMG_PSF, IMG_DIRTY, IMG_RESIDUAL, IMG_MODEL = 0, 1, 2, 3
+
+
 class TcvCurGeometry(ctypes.Structure):
     _fields_ = [
         ("run_type", ctypes.c_int32), ("w_size", ctypes.c_int32), ("over_sample", ctypes.c_int32),
@@ -178,6 +192,24 @@ SIGNATURES = {
     "tcv_hogbom_deconvolve": (_I, [_P, _I, _P, _I, _P, _P, _I, _F, _F, _P, _P, _P, _S, _P]),
     "tcv_hogbom_result": (_I, [_P, _P, _P, _P, _P, _P]),
     "tcv_find_peak": (_I, [_P, _I64, _P, _P, _P, _S, _P]),
+    "tcv_fft_exec": (_I, [_P, _I, _I, _P]),
+    "tcv_fft_fix": (_I, [_P, _I64, _F, _P]),
+    "tcv_image_from_grid": (_I, [_P, _I, _F, _P, _P]),
+    "tcv_grid_from_image": (_I, [_P, _I, _P, _P]),
+    "tcv_major_config_default": (None, [_P]),
+    "tcv_major_create": (_I, [_P, _P]),
+    "tcv_major_destroy": (None, [_P]),
+    "tcv_major_last_error": (ctypes.c_char_p, [_P]),
+    "tcv_major_get_stream": (_P, [_P]),
+    "tcv_major_init": (_I, [_P]),
+    "tcv_major_run_cycle": (_I, [_P]),
+    "tcv_major_sync": (_I, [_P]),
+    "tcv_major_stage_ms": (_I, [_P, _P, _P]),
+    "tcv_major_info": (_I, [_P, _P, _P, _P, _P]),
+    "tcv_major_get_image": (_I, [_P, _I, _P]),
+    "tcv_major_get_grid": (_I, [_P, _I, _P]),
+    "tcv_major_get_vis": (_I, [_P, _I, _P]),
+    "tcv_major_get_offsets": (_I, [_P, _P, _P, _P]),
     "tcv_cur_init": (_I, [_P]),
     "tcv_cur_run_grid": (_I, [_P]),
     "tcv_cur_run_degrid": (_I, [_P]),

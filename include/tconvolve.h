@@ -573,6 +573,70 @@ tcv_status tcv_hogbom_result(const void *d_work, int *iters_done, int *stopped_a
 tcv_status tcv_find_peak(const float *d_image, int64_t n, float *val_out, int64_t *pos_out,
                          void *d_work, size_t work_bytes, void *stream);
 
+/* ------------------------------------------------------------------------------------------
+ * FFT steps either side of gridding (current/tMajorACC/tMajorACC.cc:487-640).  Grids are square
+ * complex64 of even size g_size (odd sizes: TCV_ERR_UNSUPPORTED, as the reference refuses them).
+ * ---------------------------------------------------------------------------------------- */
+/* fftExec / fftExecGPU: in place, rotate by half the size in both axes, unnormalised 2-D C2C
+ * transform (forward: exp(-i..), else exp(+i..)), rotate back.  Single precision (cuFFT). */
+tcv_status tcv_fft_exec(float *d_grid, int g_size, int forward, void *stream);
+/* fftFix / fftFixGPU: grid[i] = (Re grid[i] * scale, 0) for n complex values. */
+tcv_status tcv_fft_fix(float *d_grid, int64_t n, float scale, void *stream);
+/* The dirty-image step fused: d_image (float, g_size^2) = Re(fftExec(d_grid, backward)) * scale;
+ * d_grid is used as scratch (overwritten). */
+tcv_status tcv_image_from_grid(float *d_grid, int g_size, float scale, float *d_image, void *stream);
+/* The model-to-grid step fused: d_grid = fftExec(complex(d_image), forward). */
+tcv_status tcv_grid_from_image(const float *d_image, int g_size, float *d_grid, void *stream);
+
+/* ------------------------------------------------------------------------------------------
+ * The imaging major cycle of current/tMajorACC (tMajorACC.cc:889-1635) on one GPU: set-up as
+ * there (samples, the delta convolution table of its initC, offsets, a 100-source sky and its
+ * degridded visibilities), then per cycle: grid the PSF (first cycle), grid the data, inverse FFT
+ * to the dirty image, Hogbom CLEAN (n_minor iterations, gain, no threshold), forward FFT of the
+ * model, degrid, subtract the model visibilities from the data.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct tcv_major_config {
+    int64_t n_samples; /* 160000 */
+    int w_size;        /* 33 */
+    int n_chan;        /* 1 */
+    double cell_size;  /* 5 wavelengths */
+    int g_size;        /* 4096 (even) */
+    int baseline;      /* 2000 m */
+    int n_major;       /* 5 (the driver's loop count; tcv_major_run_cycle runs one) */
+    int n_minor;       /* 100 */
+    float gain;        /* 0.1 */
+    int n_sources;     /* 100 */
+    int device;
+    int keep_stages;   /* 1: keep copies of the PSF and data uv grids (tcv_major_get_grid 0, 1) */
+    tcv_tuning tuning; /* of the binning plan */
+} tcv_major_config;
+enum {
+    TCV_MAJOR_PSF_GRID = 0, TCV_MAJOR_PSF_IFFT = 1, TCV_MAJOR_GRID = 2, TCV_MAJOR_IFFT = 3,
+    TCV_MAJOR_HOGBOM = 4, TCV_MAJOR_FFT = 5, TCV_MAJOR_DEGRID = 6, TCV_MAJOR_SUBTRACT = 7,
+    TCV_MAJOR_STAGES = 8
+};
+enum { TCV_IMG_PSF = 0, TCV_IMG_DIRTY = 1, TCV_IMG_RESIDUAL = 2, TCV_IMG_MODEL = 3 };
+typedef struct tcv_major_ctx tcv_major_ctx;
+void tcv_major_config_default(tcv_major_config *cfg);
+tcv_status tcv_major_create(const tcv_major_config *cfg, tcv_major_ctx **out);
+void tcv_major_destroy(tcv_major_ctx *ctx);
+const char *tcv_major_last_error(const tcv_major_ctx *ctx);
+void *tcv_major_get_stream(const tcv_major_ctx *ctx);
+tcv_status tcv_major_init(tcv_major_ctx *ctx);      /* set-up; synchronises */
+tcv_status tcv_major_run_cycle(tcv_major_ctx *ctx); /* one major cycle, asynchronous */
+tcv_status tcv_major_sync(tcv_major_ctx *ctx);
+/* Device time per stage summed over the cycles run (ms[TCV_MAJOR_STAGES]); synchronises. */
+tcv_status tcv_major_stage_ms(tcv_major_ctx *ctx, double *ms, int *cycles);
+tcv_status tcv_major_info(const tcv_major_ctx *ctx, int *support, int64_t *n_vis, int64_t *c_len,
+                          float *scale);
+/* Copies to host: images (TCV_IMG_*, float g_size^2), grids (0 PSF uv grid, 1 data uv grid, both
+ * with keep_stages; 2 the model grid of the last cycle; complex64 g_size^2), visibilities
+ * (0 the data, 1 the last model visibilities; complex64), offsets. */
+tcv_status tcv_major_get_image(tcv_major_ctx *ctx, int which, float *out);
+tcv_status tcv_major_get_grid(tcv_major_ctx *ctx, int which, float *out);
+tcv_status tcv_major_get_vis(tcv_major_ctx *ctx, int which, float *out);
+tcv_status tcv_major_get_offsets(tcv_major_ctx *ctx, int32_t *iu, int32_t *iv, int32_t *coff);
+
 #ifdef __cplusplus
 }
 #endif

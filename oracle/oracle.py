@@ -354,3 +354,95 @@ def hogbom(dirty: np.ndarray, psf: np.ndarray, niters: int, gain: float = 0.1, t
     return {"model": m, "residual": r, "done": int(done), "stopped_at": int(stopped.value),
             "hist_val": hv[:done], "hist_pos": hp[:done], "skipped_rows": int(skipped.value),
             "psf_peak_pos": int(ppos.value)}
+
+
+# ---- the imaging major cycle (current/tMajorACC/tMajorACC.cc:487-640, 889-1635) ----
+# Restated with the gridding, degridding and Hogbom functions above (C, float) and numpy's
+# double-precision FFT for fftExec (the reference calls single-precision FFTW or cuFFT there; its
+# own check of one against the other is |difference| * psfScale <= 1e-5 per pixel, :1460-1580).
+# tMajorACC needs FFTW, OpenACC and the PGI compiler, none of which is here: it is not built, so
+# this restatement is checked piecewise (gridding, degridding and Hogbom are the pinned functions
+# above; the set-up draws are the attic generator's) and its FFT against the definition.
+
+def lcg_after(draws: int, state: int = 1) -> int:
+    """The K&R generator's state after `draws` steps (attic/tConvolveMPI/Benchmark.cc:53-58)."""
+    a, c, m = 1103515245, 12345, 1 << 64
+    A, C = 1, 0
+    while draws:
+        if draws & 1:
+            A, C = (a * A) % m, (a * C + c) % m
+        a, c = (a * a) % m, (a * c + c) % m
+        draws >>= 1
+    return (A * state + C) % m
+
+
+def fft_exec(grid: np.ndarray, g_size: int, forward: bool) -> np.ndarray:
+    """fftExec (tMajorACC.cc:487-545): half-size rotation, unnormalised 2-D transform (forward
+    exp(-i..), backward exp(+i..)), rotation back; in double, returned as complex64."""
+    x = np.fft.fftshift(np.asarray(grid, np.complex128).reshape(g_size, g_size))
+    y = np.fft.fft2(x) if forward else np.fft.ifft2(x, norm="forward")
+    return np.fft.fftshift(y).astype(np.complex64).ravel()
+
+
+def fft_fix(grid: np.ndarray, scale: float) -> np.ndarray:
+    """fftFix (tMajorACC.cc:620-626): Re * scale in float; returned as the float real image."""
+    return (np.real(grid).astype(np.float32) * np.float32(scale)).astype(np.float32)
+
+
+def major_setup(n_samples: int = 160000, w_size: int = 33, n_chan: int = 1, cell_size: float = 5.0,
+                g_size: int = 4096, baseline: int = 2000, n_sources: int = 100, threads: int = 16):
+    """tMajorACC's set-up (:930-1035): samples, the delta table of its initC (:349-434), offsets,
+    the true sky of n_sources points and its degridded visibilities."""
+    cfg = Config(n_samples, w_size, n_chan, g_size, cell_size, baseline, 0)
+    u, v, w = init_uvw(cfg)
+    support, os_, wcs = c_geometry(cfg)
+    s = 2 * support + 1
+    c = np.zeros(s * s * os_ * os_ * w_size, np.complex64)
+    c[::s * s] = 1.0  # C[cind] = 1 at i == 0 && j == 0; the float normalisation factor is exactly 1
+    iu, iv, co = init_offsets(cfg, u, v, w, wcs, support, os_)
+    state = lcg_after(3 * n_samples)
+    maxint = 2147483647
+
+    def draw():
+        nonlocal state
+        state = (state * 1103515245 + 12345) % (1 << 64)
+        return ((state // 65536) & 0xFFFFFFFF) % maxint
+
+    true = np.zeros(g_size * g_size, np.complex64)
+    for _ in range(n_sources):
+        l = int(g_size * float(draw()) / float(maxint))
+        m = int(g_size * float(draw()) / float(maxint))
+        true[m * g_size + l] += np.float32(draw()) / np.float32(2147483648.0)
+    true_uv = fft_exec(true, g_size, True)
+    vis = degrid_f32(true_uv, g_size, support, c, co, iu, iv, threads)
+    n = n_samples * n_chan
+    scale = float(np.float32(1.0 / float(np.float32(n))))
+    return {"cfg": cfg, "support": support, "C": c, "iu": iu, "iv": iv, "coff": co, "vis": vis, "scale": scale,
+            "true": true}
+
+
+def major_cycle(st: dict, data: np.ndarray, psf_image: np.ndarray | None, n_minor: int = 100, gain: float = 0.1,
+                threads: int = 16) -> dict:
+    """One major cycle of tMajorACC's CPU path (:1096-1236): grid (the PSF too when psf_image is
+    None), inverse FFT + fix, Hogbom (no threshold), forward FFT of the model, degrid, subtract.
+    Returns every stage's output and the updated data."""
+    g = st["cfg"].g_size
+    sup, c, iu, iv, co, scale = st["support"], st["C"], st["iu"], st["iv"], st["coff"], st["scale"]
+    out = {}
+    if psf_image is None:
+        uv_psf = np.zeros(g * g, np.complex64)
+        grid_f32(np.ones(iu.size, np.complex64), sup, c, co, iu, iv, uv_psf, g, threads)
+        out["uv_psf"] = uv_psf
+        psf_image = fft_fix(fft_exec(uv_psf, g, False), scale)
+    out["psf"] = psf_image
+    uv = np.zeros(g * g, np.complex64)
+    grid_f32(data, sup, c, co, iu, iv, uv, g, threads)
+    out["uv_data"] = uv
+    dirty = fft_fix(fft_exec(uv, g, False), scale)
+    out["dirty"] = dirty
+    h = hogbom(dirty, psf_image, n_minor, gain, 0.0)
+    out["residual"], out["model"] = h["residual"], h["model"]
+    out["model_grid"] = fft_exec(h["model"].astype(np.complex64), g, True)
+    out["model_vis"] = degrid_f32(out["model_grid"], g, sup, c, co, iu, iv, threads)
+    out["data"] = (data - out["model_vis"]).astype(np.complex64)
+    return out
