@@ -86,3 +86,57 @@ class Hogbom:
         if residual is not None:
             residual.reshape(-1)[:] = out
         return out
+
+
+def main(argv=None) -> int:
+    """tHogbomCleanOMP's driver (current/tHogbomCleanOMP/tHogbomCleanOMP.cc:81-124) on the GPU:
+    raw float32 dirty and PSF images (--dirty/--psf, the reference's .img format) or synthetic ones
+    (--width), the reference's parameters unless overridden, and its report lines."""
+    import argparse
+
+    import torch
+
+    from .workload import synthetic_dirty, synthetic_psf
+
+    ap = argparse.ArgumentParser(prog="python -m tconvolve.hogbom")
+    ap.add_argument("--dirty")
+    ap.add_argument("--psf")
+    ap.add_argument("--width", type=int, default=4096, help="synthetic images of this size when no files are given")
+    ap.add_argument("--niters", type=int, default=NITERS)
+    ap.add_argument("--gain", type=float, default=GAIN)
+    ap.add_argument("--threshold", type=float, default=THRESHOLD)
+    ap.add_argument("--repeat", type=int, default=1)
+    a = ap.parse_args(argv)
+    if a.dirty and a.psf:
+        dirty, psf = np.fromfile(a.dirty, np.float32), np.fromfile(a.psf, np.float32)
+    else:
+        dirty, psf = synthetic_dirty(a.width, 20, 1e-3, seed=7).ravel(), synthetic_psf(a.width).ravel()
+    dim, pdim = int(round(np.sqrt(dirty.size))), int(round(np.sqrt(psf.size)))
+    if dim * dim != dirty.size or pdim * pdim != psf.size:
+        print("Error: Image is not square")
+        return 1
+    print(f"Iterations = {a.niters}")
+    print(f"Image dimensions = {dim}x{dim}")
+    d, p = torch.from_numpy(dirty).cuda(), torch.from_numpy(psf).cuda()
+    m, r = torch.zeros_like(d), torch.empty_like(d)
+    ws = Workspace(dim)
+    print("+++++ Forward processing (B200) +++++")
+    for _ in range(a.repeat):
+        m.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        deconvolve_device(d, dim, p, pdim, m, r, a.niters, a.gain, a.threshold, work=ws)
+        e1.record()
+        torch.cuda.synchronize()
+        s = e0.elapsed_time(e1) * 1e-3
+        done = ws.result()["done"]
+        print(f"    Time {s} (s) ")
+        print(f"    Time per cycle {s / max(done, 1) * 1000} (ms)")
+        print(f"    Cleaning rate  {done / s} (iterations per second)")
+    print("Done")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

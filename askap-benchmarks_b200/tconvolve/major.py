@@ -127,3 +127,60 @@ def image_from_grid(grid, g_size: int, scale: float, image, stream=None):
 def grid_from_image(image, g_size: int, grid, stream=None):
     """grid (complex64) = fftExec(complex(image), forward)."""
     check(lib().tcv_grid_from_image(_ptr(image), int(g_size), _ptr(grid), _stream(stream)), "tcv_grid_from_image")
+
+
+def main(argv=None) -> int:
+    """tMajorACC's driver (current/tMajorACC/tMajorACC.cc:889-1635) on the GPU with its options
+    (-n samples, -w planes, -c channels, -f cell-size factor) and its timing report."""
+    import argparse
+
+    ap = argparse.ArgumentParser(prog="python -m tconvolve.major")
+    ap.add_argument("-n", type=int, default=160000)
+    ap.add_argument("-w", type=int, default=33)
+    ap.add_argument("-c", type=int, default=1)
+    ap.add_argument("-f", type=float, default=1.0)
+    ap.add_argument("--g-size", type=int, default=4096)
+    ap.add_argument("--major", type=int, default=5)
+    ap.add_argument("--minor", type=int, default=100)
+    a = ap.parse_args(argv)
+    print(f"nSamples = {a.n}\nnChan = {a.c}\nwSize = {a.w}\ncellSize = {5.0 * a.f}")
+    m = MajorCycle(n_samples=a.n, w_size=a.w, n_chan=a.c, cell_size=5.0 * a.f, g_size=a.g_size, n_major=a.major,
+                   n_minor=a.minor)
+    m.init()
+    for it in range(a.major):
+        print(f"cycle {it}")
+        m.run_cycle()
+    m.sync()
+    ms, n = m.stage_ms()
+    info = m.info()
+    s = 2 * info["support"] + 1
+    nv = info["n_vis"]
+    griddings = nv * s * s
+    print("\n+++++ B200 times +++++\n")
+
+    def rates(title, t):
+        print(title)
+        print(f"    Time per major cycle {t} (s) ")
+        print(f"    Time per visibility sample {1e6 * t / nv} (us) ")
+        print(f"    Time per gridding   {1e9 * t / griddings} (ns) ")
+        print(f"    Gridding rate   {griddings / 1e6 / t} (million grid points per second)")
+
+    rates("Gridding PSF", ms["psf_grid"] * 1e-3)
+    rates("Gridding data", ms["grid"] * 1e-3 / n)
+    print(f"Inverse FFTs\n    Time per major cycle {ms['ifft'] * 1e-3 / n} (s) ")
+    t = ms["hogbom"] * 1e-3 / n
+    print(f"Hogbom clean\n    Time per major cycle {t} (s) \n    Time per minor cycle {t / a.minor * 1000} (ms)")
+    print(f"    Cleaning rate  {a.minor / t} (iterations per second)")
+    print(f"Forward FFT\n    Time per major cycle {ms['fft'] * 1e-3 / n} (s) ")
+    t = ms["degrid"] * 1e-3 / n
+    print("Degridding data")
+    print(f"    Time per major cycle {t} (s) ")
+    print(f"    Time per visibility sample {1e6 * t / nv} (us) ")
+    print(f"    Time per degridding   {1e9 * t / griddings} (ns) ")
+    print(f"    Degridding rate   {griddings / 1e6 / t} (million grid points per second)")
+    m.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -27,6 +27,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "askap-benchmarks_b200"))
 
@@ -40,6 +42,7 @@ FALLBACK_HBM_GBS = 6650.0
 L2_FLUSH_BYTES = 512 << 20
 REF_DRIVER = os.path.join(REPO, "oracle", "_ref", "c2", "ref_driver")
 REF_DRIVER_CURRENT = os.path.join(REPO, "oracle", "_ref", "current", "ref_driver_current")
+REF_DRIVER_HOGBOM = os.path.join(REPO, "oracle", "_ref", "hogbom", "ref_driver_hogbom")
 
 
 def parse_args():
@@ -63,6 +66,8 @@ def parse_args():
     p.add_argument("--no-batched", action="store_true", help="skip the 64-job batched measurement")
     p.add_argument("--no-serving", action="store_true", help="skip the serving (Poisson arrivals) measurement")
     p.add_argument("--serve-seconds", type=float, default=2.0, help="arrival window per serving rate")
+    p.add_argument("--no-hogbom", action="store_true", help="skip the Hogbom CLEAN (minor cycle) measurement")
+    p.add_argument("--no-major", action="store_true", help="skip the imaging major cycle measurement")
     p.add_argument("--no-current", action="store_true",
                    help="skip the variable-support (current/tConvolveMPI) continuum and spectral measurement")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -427,8 +432,8 @@ def b200_arm(args):
                                     else "degrid_staged_kernel")}[(dom, args.path)]
 
     # the other workloads run after the headline's context is released
-    batched = serving = current = None
-    if not (args.no_batched and args.no_serving and args.no_current):
+    batched = serving = current = hogbom = major = None
+    if not (args.no_batched and args.no_serving and args.no_current and args.no_hogbom and args.no_major):
         b.close()
         torch.cuda.empty_cache()
     if not args.no_batched:
@@ -438,6 +443,12 @@ def b200_arm(args):
         serving = serving_section(args, local)
     if not args.no_current:
         current = current_section(args, torch, world)
+        torch.cuda.empty_cache()
+    if not args.no_hogbom and world == 1:
+        hogbom = hogbom_section(args, torch)
+        torch.cuda.empty_cache()
+    if not args.no_major and world == 1:
+        major = major_section(args, torch)
         torch.cuda.empty_cache()
 
     cpu = None
@@ -478,6 +489,8 @@ def b200_arm(args):
             "batched": batched,
             "serving": serving,
             "current": current,
+            "hogbom": hogbom,
+            "major": major,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * (8 + 4 * 3),
                     "d2h_bytes_per_step": n * 8, "ms_per_step": e2e_mean},
             "gpu_launches": launches_per_step * args.steps if launches_per_step else None,
@@ -489,7 +502,7 @@ def b200_arm(args):
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    if args.no_batched and args.no_serving and args.no_current:
+    if args.no_batched and args.no_serving and args.no_current and args.no_hogbom and args.no_major:
         b.close()  # not released above
     if world > 1:
         dist.destroy_process_group()
@@ -681,6 +694,136 @@ def current_section(args, torch, world):
         res["runs"][RUN_TYPES[rt]] = entry
     b.close()
     return res
+
+
+def hogbom_section(args, torch):
+    """Hogbom CLEAN as current/tHogbomCleanOMP runs it (Parameters.h: 1000 iterations, gain 0.1,
+    threshold 1e-5) on synthetic 4096^2 and 1024^2 dirty images and PSFs (tconvolve.workload; the
+    reference's data/*.img inputs are not in its tree).  Metric: iterations per second (the
+    reference's "Cleaning rate").  Algorithmic bytes per iteration: the residual read once
+    (4 B/pixel) plus the PSF overlap read and the residual overlap written (8 B/pixel of overlap)."""
+    from tconvolve.hogbom import Workspace, deconvolve_device
+    from tconvolve.workload import synthetic_dirty, synthetic_psf
+
+    res = {"workload": "synthetic dirty image (20 point sources x PSF + 1e-3 uniform noise) and PSF, "
+                       "1000 iterations, gain 0.1, threshold 1e-5", "sizes": {}}
+    peak, peak_kind = measured_hbm_peak()
+    for w in (4096, 1024):
+        dirty, psf = synthetic_dirty(w, 20, 1e-3, seed=7), synthetic_psf(w)
+        d = torch.from_numpy(dirty.ravel()).cuda()
+        p = torch.from_numpy(psf.ravel()).cuda()
+        m = torch.zeros_like(d)
+        r = torch.empty_like(d)
+        hv = torch.zeros(1000, dtype=torch.float32, device="cuda")
+        hp = torch.zeros(1000, dtype=torch.int32, device="cuda")
+        ws = Workspace(w)
+        times = []
+        for rep in range(4):  # the first run is the warm-up
+            m.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            deconvolve_device(d, w, p, w, m, r, 1000, 0.1, 1e-5, hist=(hv, hp), work=ws)
+            e1.record()
+            torch.cuda.synchronize()
+            if rep:
+                times.append(e0.elapsed_time(e1))
+        out = ws.result()
+        ms = statistics.median(times)
+        pos = hp[:out["done"]].cpu().numpy().astype(np.int64)
+        rx, ry, c = pos % w, pos // w, w // 2  # PSF peak at the centre: overlap = (w - |rx - c|)(w - |ry - c|)
+        overlap = ((w - np.abs(rx - c)) * (w - np.abs(ry - c))).astype(np.float64)
+        alg_bytes = 4.0 * w * w * out["done"] + 8.0 * overlap.sum()
+        achieved = alg_bytes / (ms * 1e-3) / 1e9
+        res["sizes"][str(w)] = {"iterations": out["done"], "ms": ms, "us_per_iteration": 1e3 * ms / out["done"],
+                                "iterations_per_s": out["done"] / (ms * 1e-3),
+                                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                             "frac": achieved / peak, "peak_source": peak_kind,
+                                             "alg_bytes_per_iteration": alg_bytes / out["done"]}}
+        del d, p, m, r
+    if not args.no_cpu_baseline:
+        res["cpu_reference"] = hogbom_cpu_reference()
+    return res
+
+
+def hogbom_cpu_reference():
+    """The reference's HogbomGolden (current/tHogbomCleanOMP/HogbomGolden.cc, compiled from its
+    source) on the 1024^2 synthetic images: one core, 1000 iterations."""
+    import tempfile
+
+    from tconvolve.workload import synthetic_dirty, synthetic_psf
+
+    if not os.path.exists(REF_DRIVER_HOGBOM):
+        return {"value": None, "sample": f"unavailable: reference build missing: {REF_DRIVER_HOGBOM}"}
+    with tempfile.TemporaryDirectory() as td:
+        paths = [os.path.join(td, n) for n in ("dirty.img", "psf.img", "model.out", "residual.out")]
+        synthetic_dirty(1024, 20, 1e-3, seed=7).tofile(paths[0])
+        synthetic_psf(1024).tofile(paths[1])
+        t0 = time.perf_counter()
+        subprocess.run([REF_DRIVER_HOGBOM] + paths, check=True, capture_output=True, timeout=600)
+        s = time.perf_counter() - t0
+    return {"value": 1000 / s, "unit": "iterations/s", "cores": 1, "kind": "reference",
+            "sample": "1024^2 synthetic images, 1000 iterations of HogbomGolden::deconvolve (wall time of the "
+                      "driver, image reads included)"}
+
+
+def major_section(args, torch):
+    """The imaging major cycle of current/tMajorACC with its own constants (160000 samples, 33
+    w-planes, 4096^2, cell 5 wavelengths, 100 sources, 100 minor iterations): 5 cycles, device time
+    per stage as the reference's timers.  A first object is run once to warm up (the first
+    gridding launch compiles the tile kernels for the footprint width)."""
+    from tconvolve.major import MajorCycle
+
+    warm = MajorCycle()
+    warm.init()
+    warm.run_cycle()
+    warm.sync()
+    warm.close()
+    torch.cuda.empty_cache()
+    m = MajorCycle()
+    t0 = time.perf_counter()
+    m.init()
+    init_s = time.perf_counter() - t0
+    cycles = m.config.n_major
+    for _ in range(cycles):
+        m.run_cycle()
+    m.sync()
+    ms, n = m.stage_ms()
+    info = m.info()
+    m.close()
+    s = 2 * info["support"] + 1
+    updates = info["n_vis"] * s * s
+    per_cycle = {k: v / n for k, v in ms.items() if k not in ("psf_grid", "psf_ifft")}
+    cycle_ms = sum(ms.values()) / n
+    res = {"workload": "tMajorACC: 160000 samples, wSize 33, 4096^2, support 64, 100 sources, 5 major x 100 minor",
+           "cycles": n, "init_s": init_s, "ms_per_cycle": cycle_ms, "stage_ms_per_cycle": per_cycle,
+           "psf_ms": {"psf_grid": ms["psf_grid"], "psf_ifft": ms["psf_ifft"]},
+           "grid_updates_per_s": updates / (per_cycle["grid"] * 1e-3),
+           "degrid_updates_per_s": updates / (per_cycle["degrid"] * 1e-3),
+           "minor_iterations_per_s": m.config.n_minor / (per_cycle["hogbom"] * 1e-3)}
+    if not args.no_cpu_baseline:
+        res["cpu_port"] = major_cpu_port()
+    return res
+
+
+def major_cpu_port():
+    """One major cycle of the oracle's restatement of tMajorACC's CPU path at full size (its
+    gridding and degridding in C on all host threads, numpy's FFT, the C Hogbom on one core).
+    tMajorACC itself needs FFTW, OpenACC and the PGI compiler and is not built here."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as orc
+
+    threads = host_threads()
+    t0 = time.perf_counter()
+    st = orc.major_setup(threads=threads)
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    orc.major_cycle(st, st["vis"], None, 100, threads=threads)
+    s = time.perf_counter() - t0
+    return {"value": s * 1e3, "unit": "ms per major cycle (first cycle, PSF included)", "cores": threads,
+            "kind": "port", "setup_s": setup_s,
+            "sample": "one full-size major cycle of the oracle restatement (C gridding/degridding on all threads, "
+                      "numpy FFT, C Hogbom)"}
 
 
 def count_step_kernels(torch, step):
