@@ -29,7 +29,7 @@ namespace tcv {
 namespace {
 
 constexpr int kHogThreads = 256;
-constexpr int kHogMaxBlocks = 592;  // 4 x 148
+constexpr int kHogMaxBlocks = 888;  // 6 x 148 (six 256-thread CTAs fit an SM at <= 40 registers)
 
 // device state of one deconvolution (start of the caller's workspace; zeroed by the host)
 struct HogState {
@@ -162,7 +162,7 @@ __device__ __forceinline__ void take(float r, long long i, unsigned long long& b
 // slice and the scan of the updated slice.  kVec: width a multiple of 4 and the residual 16-byte
 // aligned (float4 residual I/O).
 template <bool kVec>
-__global__ void __launch_bounds__(kHogThreads) hog_iter_kernel(HogArgs a, int it)
+__global__ void __launch_bounds__(kHogThreads, 6) hog_iter_kernel(HogArgs a, int it)
 {
     HogState* st = a.state;
     if (st->stopped) return;  // an earlier launch stopped the loop
@@ -196,29 +196,55 @@ __global__ void __launch_bounds__(kHogThreads) hog_iter_kernel(HogArgs a, int it
     float bv = 0.f;
     unsigned long long skipped = 0;
     if (kVec) {
-        for (long long i = lo + 4 * threadIdx.x; i < hi; i += 4 * kHogThreads) {
-            const unsigned ui = unsigned(i);  // n < 2^32
-            const int y = int(ui / unsigned(W)), x0 = int(ui - unsigned(y) * unsigned(W));
-            float4 r = __ldcg(reinterpret_cast<const float4*>(a.residual + i));
-            const int prow = y - diffy;
-            const bool row_in = y >= starty && y <= stopy;
-            const bool prow_ok = prow >= 0 && prow < P;
-            if (row_in && prow_ok && x0 + 3 >= startx && x0 <= stopx) {
-                const long long pbase = (long long)prow * P - diffx;  // + x: inside the PSF row for x in range
-                float* rv = reinterpret_cast<float*>(&r);
+        // two float4 per thread per step, every load issued before any store (memory in flight)
+        constexpr int U = 2;
+        for (long long base = lo + 4 * threadIdx.x; base < hi; base += 4 * kHogThreads * U) {
+            float4 r[U];
+            float pv[U][4];
+            bool sub[U];
+            int x0[U];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int x = x0 + j;
-                    if (x >= startx && x <= stopx) rv[j] = __fsub_rn(rv[j], __fmul_rn(t, __ldg(a.psf + (pbase + x))));
+            for (int u = 0; u < U; ++u) {
+                const long long i = base + 4LL * kHogThreads * u;
+                sub[u] = false;
+                x0[u] = 0;
+                r[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (i < hi) {
+                    const unsigned ui = unsigned(i);  // n < 2^32
+                    const int y = int(ui / unsigned(W));
+                    x0[u] = int(ui - unsigned(y) * unsigned(W));
+                    r[u] = __ldcg(reinterpret_cast<const float4*>(a.residual + i));
+                    const int prow = y - diffy;
+                    const bool row_in = y >= starty && y <= stopy;
+                    const bool prow_ok = prow >= 0 && prow < P;
+                    sub[u] = row_in && prow_ok && x0[u] + 3 >= startx && x0[u] <= stopx;
+                    if (row_in && !prow_ok && x0[u] == 0) ++skipped;
+                    const long long pbase = (long long)prow * P - diffx;  // + x: inside the PSF row for x in range
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int x = x0[u] + j;
+                        pv[u][j] = (sub[u] && x >= startx && x <= stopx) ? __ldg(a.psf + (pbase + x)) : 0.f;
+                    }
                 }
-                __stcg(reinterpret_cast<float4*>(a.residual + i), r);
-            } else if (row_in && !prow_ok && x0 == 0) {
-                ++skipped;
             }
-            take(r.x, i, best, bv);
-            take(r.y, i + 1, best, bv);
-            take(r.z, i + 2, best, bv);
-            take(r.w, i + 3, best, bv);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const long long i = base + 4LL * kHogThreads * u;
+                if (i >= hi) continue;
+                if (sub[u]) {
+                    float* rv = reinterpret_cast<float*>(&r[u]);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int x = x0[u] + j;
+                        if (x >= startx && x <= stopx) rv[j] = __fsub_rn(rv[j], __fmul_rn(t, pv[u][j]));
+                    }
+                    __stcg(reinterpret_cast<float4*>(a.residual + i), r[u]);
+                }
+                take(r[u].x, i, best, bv);
+                take(r[u].y, i + 1, best, bv);
+                take(r[u].z, i + 2, best, bv);
+                take(r[u].w, i + 3, best, bv);
+            }
         }
     } else {
         for (long long i = lo + threadIdx.x; i < hi; i += kHogThreads) {
