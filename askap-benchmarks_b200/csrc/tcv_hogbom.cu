@@ -29,7 +29,7 @@ namespace tcv {
 namespace {
 
 constexpr int kHogThreads = 256;
-constexpr int kHogMaxBlocks = 888;  // 6 x 148 (six 256-thread CTAs fit an SM at <= 40 registers)
+constexpr int kHogMaxBlocks = 592;  // 4 x 148: one wave of four 256-thread CTAs per SM
 
 // device state of one deconvolution (start of the caller's workspace; zeroed by the host)
 struct HogState {
@@ -55,11 +55,6 @@ struct HogArgs {
     long long n;  // width * width
     float gain, threshold;
 };
-
-__device__ __forceinline__ unsigned long long peak_key(float v, unsigned int idx)
-{
-    return (static_cast<unsigned long long>(__float_as_uint(fabsf(v))) << 32) | static_cast<unsigned int>(~idx);
-}
 
 __device__ __forceinline__ unsigned int key_index(unsigned long long k) { return ~static_cast<unsigned int>(k); }
 
@@ -135,34 +130,27 @@ __global__ void __launch_bounds__(kHogThreads) hog_scan_kernel(const float* __re
 {
     const long long per = (n + nblocks - 1) / nblocks;
     const long long lo = per * blockIdx.x, hi = min(n, lo + per);
-    unsigned long long best = 0;
-    float bv = 0.f;
+    float best_abs = -1.f, bv = 0.f;
+    unsigned int bi = 0;
     for (long long i = lo + threadIdx.x; i < hi; i += kHogThreads) {
         const float v = img[i];
         if (copy_to) copy_to[i] = v;
-        const unsigned long long k = peak_key(v, static_cast<unsigned int>(i));
-        if (k > best) {
-            best = k;
+        if (fabsf(v) > best_abs) {  // strict '>' in index order keeps the first index
+            best_abs = fabsf(v);
             bv = v;
+            bi = static_cast<unsigned int>(i);
         }
     }
+    const unsigned long long best =
+        best_abs < 0.f ? 0ull : (static_cast<unsigned long long>(__float_as_uint(best_abs)) << 32) | (~bi & 0xffffffffu);
     finish_scan(best, bv, keys, vals, nblocks, st, slot);
-}
-
-__device__ __forceinline__ void take(float r, long long i, unsigned long long& best, float& bv)
-{
-    const unsigned long long k = peak_key(r, static_cast<unsigned int>(i));
-    if (k > best) {
-        best = k;
-        bv = r;
-    }
 }
 
 // One iteration: the previous scan's peak, the model update, the PSF subtraction over this block's
 // slice and the scan of the updated slice.  kVec: width a multiple of 4 and the residual 16-byte
 // aligned (float4 residual I/O).
 template <bool kVec>
-__global__ void __launch_bounds__(kHogThreads, 6) hog_iter_kernel(HogArgs a, int it)
+__global__ void __launch_bounds__(kHogThreads, 4) hog_iter_kernel(HogArgs a, int it)
 {
     HogState* st = a.state;
     if (st->stopped) return;  // an earlier launch stopped the loop
@@ -190,65 +178,77 @@ __global__ void __launch_bounds__(kHogThreads, 6) hog_iter_kernel(HogArgs a, int
     const int stopx = min(W - 1, rx + (P - px - 1)), stopy = min(W - 1, ry + (P - py - 1));
     const float t = __fmul_rn(a.gain, peak);
 
-    const long long per = ((a.n + a.nblocks - 1) / a.nblocks + 3) & ~3LL;
-    const long long lo = per * blockIdx.x, hi = min(a.n, lo + per);
-    unsigned long long best = 0;
-    float bv = 0.f;
+    // running maximum of |value| in index order: strict '>' keeps the first index (findPeak's rule)
+    float best_abs = -1.f, bv = 0.f;
+    unsigned int bi = 0;
     unsigned long long skipped = 0;
+    auto track = [&](float v, unsigned int idx) {
+        const float av = fabsf(v);
+        if (av > best_abs) {
+            best_abs = av;
+            bv = v;
+            bi = idx;
+        }
+    };
     if (kVec) {
-        // two float4 per thread per step, every load issued before any store (memory in flight)
-        constexpr int U = 2;
-        for (long long base = lo + 4 * threadIdx.x; base < hi; base += 4 * kHogThreads * U) {
-            float4 r[U];
-            float pv[U][4];
-            bool sub[U];
-            int x0[U];
+        // whole rows per block; per row every thread loads its float4s (up to U) before any store
+        constexpr int U = 4;
+        const int rows_per = (W + a.nblocks - 1) / a.nblocks;
+        const int r0 = int(blockIdx.x) * rows_per, r1 = min(W, r0 + rows_per);
+        for (int y = r0; y < r1; ++y) {
+            const int prow = y - diffy;
+            const bool row_in = y >= starty && y <= stopy;
+            const bool prow_ok = prow >= 0 && prow < P;
+            const bool row_sub = row_in && prow_ok;
+            if (row_in && !prow_ok && threadIdx.x == 0) ++skipped;
+            float* rrow = a.residual + (long long)y * W;
+            const long long pbase = (long long)prow * P - diffx;  // + x: inside the PSF row for x in range
+            const unsigned int ibase = unsigned(y) * unsigned(W);
+            for (int xb = 4 * int(threadIdx.x); xb < W; xb += 4 * kHogThreads * U) {
+                float4 r[U];
+                float pv[U][4];
+                bool sub[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const long long i = base + 4LL * kHogThreads * u;
-                sub[u] = false;
-                x0[u] = 0;
-                r[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (i < hi) {
-                    const unsigned ui = unsigned(i);  // n < 2^32
-                    const int y = int(ui / unsigned(W));
-                    x0[u] = int(ui - unsigned(y) * unsigned(W));
-                    r[u] = __ldcg(reinterpret_cast<const float4*>(a.residual + i));
-                    const int prow = y - diffy;
-                    const bool row_in = y >= starty && y <= stopy;
-                    const bool prow_ok = prow >= 0 && prow < P;
-                    sub[u] = row_in && prow_ok && x0[u] + 3 >= startx && x0[u] <= stopx;
-                    if (row_in && !prow_ok && x0[u] == 0) ++skipped;
-                    const long long pbase = (long long)prow * P - diffx;  // + x: inside the PSF row for x in range
+                for (int u = 0; u < U; ++u) {
+                    const int x0 = xb + 4 * kHogThreads * u;
+                    sub[u] = false;
+                    r[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (x0 < W) {
+                        r[u] = __ldcg(reinterpret_cast<const float4*>(rrow + x0));
+                        sub[u] = row_sub && x0 + 3 >= startx && x0 <= stopx;
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int x = x0[u] + j;
-                        pv[u][j] = (sub[u] && x >= startx && x <= stopx) ? __ldg(a.psf + (pbase + x)) : 0.f;
+                        for (int j = 0; j < 4; ++j) {
+                            const int x = x0 + j;
+                            pv[u][j] = (sub[u] && x >= startx && x <= stopx) ? __ldg(a.psf + (pbase + x)) : 0.f;
+                        }
                     }
                 }
-            }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const long long i = base + 4LL * kHogThreads * u;
-                if (i >= hi) continue;
-                if (sub[u]) {
-                    float* rv = reinterpret_cast<float*>(&r[u]);
+                for (int u = 0; u < U; ++u) {
+                    const int x0 = xb + 4 * kHogThreads * u;
+                    if (x0 >= W) continue;
+                    if (sub[u]) {
+                        float* rv = reinterpret_cast<float*>(&r[u]);
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int x = x0[u] + j;
-                        if (x >= startx && x <= stopx) rv[j] = __fsub_rn(rv[j], __fmul_rn(t, pv[u][j]));
+                        for (int j = 0; j < 4; ++j) {
+                            const int x = x0 + j;
+                            if (x >= startx && x <= stopx) rv[j] = __fsub_rn(rv[j], __fmul_rn(t, pv[u][j]));
+                        }
+                        __stcg(reinterpret_cast<float4*>(rrow + x0), r[u]);
                     }
-                    __stcg(reinterpret_cast<float4*>(a.residual + i), r[u]);
+                    const unsigned int i0 = ibase + unsigned(x0);
+                    track(r[u].x, i0);
+                    track(r[u].y, i0 + 1);
+                    track(r[u].z, i0 + 2);
+                    track(r[u].w, i0 + 3);
                 }
-                take(r[u].x, i, best, bv);
-                take(r[u].y, i + 1, best, bv);
-                take(r[u].z, i + 2, best, bv);
-                take(r[u].w, i + 3, best, bv);
             }
         }
     } else {
+        const long long per = (a.n + a.nblocks - 1) / a.nblocks;
+        const long long lo = per * blockIdx.x, hi = min(a.n, lo + per);
         for (long long i = lo + threadIdx.x; i < hi; i += kHogThreads) {
-            const unsigned ui = unsigned(i);
+            const unsigned ui = unsigned(i);  // n < 2^32
             const int y = int(ui / unsigned(W)), x = int(ui - unsigned(y) * unsigned(W));
             float r = a.residual[i];
             const int prow = y - diffy;
@@ -260,9 +260,11 @@ __global__ void __launch_bounds__(kHogThreads, 6) hog_iter_kernel(HogArgs a, int
                     ++skipped;
                 }
             }
-            take(r, i, best, bv);
+            track(r, ui);
         }
     }
+    const unsigned long long best =
+        best_abs < 0.f ? 0ull : (static_cast<unsigned long long>(__float_as_uint(best_abs)) << 32) | (~bi & 0xffffffffu);
     if (skipped) atomicAdd(&st->skipped_rows, skipped);
     finish_scan(best, bv, a.keys, a.vals, a.nblocks, st, par ^ 1);
 }
