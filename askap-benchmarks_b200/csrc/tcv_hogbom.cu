@@ -40,6 +40,8 @@ struct HogState {
     int done;                       // iterations carried out
     unsigned int psf_pos;           // PSF peak index
     unsigned long long skipped_rows;  // PSF rows outside the PSF (reference out-of-bounds reads)
+    unsigned int gen;                 // persistent kernel: barrier generation
+    int error;                        // persistent kernel: a barrier wait gave up
 };
 
 struct HogArgs {
@@ -146,33 +148,17 @@ __global__ void __launch_bounds__(kHogThreads) hog_scan_kernel(const float* __re
     finish_scan(best, bv, keys, vals, nblocks, st, slot);
 }
 
-// One iteration: the previous scan's peak, the model update, the PSF subtraction over this block's
-// slice and the scan of the updated slice.  kVec: width a multiple of 4 and the residual 16-byte
-// aligned (float4 residual I/O).
+// subtractPSF (HogbomGolden.cc:99-124) over this CTA's share of the image, and the scan of the
+// updated values: returns the CTA-thread's candidate key (0 if it saw no pixel) and value.
+// kVec: width a multiple of 4 and the residual 16-byte aligned (float4 residual I/O).
 template <bool kVec>
-__global__ void __launch_bounds__(kHogThreads, 4) hog_iter_kernel(HogArgs a, int it)
+__device__ __forceinline__ unsigned long long iter_body(const HogArgs& a, unsigned int ppos, float peak,
+                                                        unsigned int psf_pos, float& bv_out,
+                                                        unsigned long long& skipped_out)
 {
-    HogState* st = a.state;
-    if (st->stopped) return;  // an earlier launch stopped the loop
-    const int par = it & 1;
-    const unsigned long long pk = st->win_key[par];
-    const unsigned int ppos = key_index(pk);
-    const float peak = st->win_val[par];
-    if (fabsf(peak) < a.threshold) {  // HogbomGolden.cc:86-89
-        if (blockIdx.x == 0 && threadIdx.x == 0) st->stopped = it + 1;
-        return;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        // model[absPeakPos] += absPeakVal * g_gain (HogbomGolden.cc:93)
-        a.model[ppos] = __fadd_rn(a.model[ppos], __fmul_rn(peak, a.gain));
-        if (a.hist_val) a.hist_val[it] = peak;
-        if (a.hist_pos) a.hist_pos[it] = ppos;
-        st->done = it + 1;
-    }
-    // subtractPSF (HogbomGolden.cc:99-124)
     const int W = a.width, P = a.psf_width;
     const int rx = int(ppos % unsigned(W)), ry = int(ppos / unsigned(W));
-    const int px = int(st->psf_pos % unsigned(P)), py = int(st->psf_pos / unsigned(P));
+    const int px = int(psf_pos % unsigned(P)), py = int(psf_pos / unsigned(P));
     const int diffx = rx - px, diffy = ry - px;  // diffy uses px, as the reference does
     const int startx = max(0, rx - px), starty = max(0, ry - py);
     const int stopx = min(W - 1, rx + (P - px - 1)), stopy = min(W - 1, ry + (P - py - 1));
@@ -265,11 +251,133 @@ __global__ void __launch_bounds__(kHogThreads, 4) hog_iter_kernel(HogArgs a, int
     }
     const unsigned long long best =
         best_abs < 0.f ? 0ull : (static_cast<unsigned long long>(__float_as_uint(best_abs)) << 32) | (~bi & 0xffffffffu);
+    bv_out = bv;
+    skipped_out = skipped;
+    return best;
+}
+
+// model[absPeakPos] += absPeakVal * g_gain (HogbomGolden.cc:93), by one thread
+__device__ __forceinline__ void model_update(const HogArgs& a, int it, unsigned int ppos, float peak)
+{
+    a.model[ppos] = __fadd_rn(a.model[ppos], __fmul_rn(peak, a.gain));
+    if (a.hist_val) a.hist_val[it] = peak;
+    if (a.hist_pos) a.hist_pos[it] = ppos;
+}
+
+// One launch per iteration: the previous scan's winner, the model update, the PSF subtraction and
+// the scan of this CTA's rows.
+template <bool kVec>
+__global__ void __launch_bounds__(kHogThreads, 4) hog_iter_kernel(HogArgs a, int it)
+{
+    HogState* st = a.state;
+    if (st->stopped) return;  // an earlier launch stopped the loop
+    const int par = it & 1;
+    const unsigned int ppos = key_index(st->win_key[par]);
+    const float peak = st->win_val[par];
+    if (fabsf(peak) < a.threshold) {  // HogbomGolden.cc:86-89
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->stopped = it + 1;
+        return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        model_update(a, it, ppos, peak);
+        st->done = it + 1;
+    }
+    float bv;
+    unsigned long long skipped;
+    const unsigned long long best = iter_body<kVec>(a, ppos, peak, st->psf_pos, bv, skipped);
     if (skipped) atomicAdd(&st->skipped_rows, skipped);
     finish_scan(best, bv, a.keys, a.vals, a.nblocks, st, par ^ 1);
 }
 
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// All iterations in one cooperative launch (every CTA resident): per iteration each CTA leaves its
+// candidate; the last to arrive reduces them, publishes the winner and advances the barrier
+// generation; the others wait for it, bounded by an iteration count and 2 s of %globaltimer, after
+// which they flag the error and return (the host reports TCV_ERR_TIMEOUT).
+template <bool kVec>
+__global__ void __launch_bounds__(kHogThreads, 4) hog_persist_kernel(HogArgs a, int niters)
+{
+    HogState* st = a.state;
+    const unsigned int psf_pos = st->psf_pos;
+    __shared__ bool last;
+    __shared__ int ok;
+    for (int it = 0; it < niters; ++it) {
+        const int par = it & 1;
+        const unsigned int ppos = key_index(__ldcg(&st->win_key[par]));
+        const float peak = __ldcg(&st->win_val[par]);
+        if (fabsf(peak) < a.threshold) {  // every CTA reads the same winner: all stop here
+            if (blockIdx.x == 0 && threadIdx.x == 0) st->stopped = it + 1;
+            return;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            model_update(a, it, ppos, peak);
+            st->done = it + 1;
+        }
+        float bv;
+        unsigned long long skipped;
+        unsigned long long best = iter_body<kVec>(a, ppos, peak, psf_pos, bv, skipped);
+        if (skipped) atomicAdd(&st->skipped_rows, skipped);
+        best = block_max(best, bv);
+        // barrier `it`: st->gen counts completed barriers, so it passes once gen > it
+        if (threadIdx.x == 0) {
+            a.keys[blockIdx.x] = best;
+            a.vals[blockIdx.x] = bv;
+            __threadfence();
+            last = atomicAdd(&st->arrived, 1u) == unsigned(a.nblocks - 1);
+        }
+        __syncthreads();
+        if (last) {
+            __threadfence();
+            unsigned long long k = 0;
+            float v = 0.f;
+            for (int i = threadIdx.x; i < a.nblocks; i += kHogThreads) {
+                const unsigned long long ki = __ldcg(a.keys + i);
+                if (ki > k) {
+                    k = ki;
+                    v = __ldcg(a.vals + i);
+                }
+            }
+            k = block_max(k, v);
+            if (threadIdx.x == 0) {
+                const bool zero = (k >> 32) == 0;
+                st->win_key[par ^ 1] = zero ? static_cast<unsigned long long>(~0u) : k;
+                st->win_val[par ^ 1] = zero ? 0.f : v;
+                st->arrived = 0;
+                __threadfence();
+                atomicExch(&st->gen, unsigned(it + 1));  // release
+                ok = 1;
+            }
+        } else if (threadIdx.x == 0) {
+            ok = 0;
+            const unsigned long long t0 = global_ns();
+            for (unsigned int spin = 0; spin < (1u << 24); ++spin) {
+                if (*reinterpret_cast<volatile unsigned int*>(&st->gen) > unsigned(it)) {
+                    ok = 1;
+                    break;
+                }
+                if (*reinterpret_cast<volatile int*>(&st->error)) break;
+                __nanosleep(32);
+                if ((spin & 1023u) == 1023u && global_ns() - t0 > 2000000000ull) break;
+            }
+            if (!ok) st->error = 1;
+            __threadfence();
+        }
+        __syncthreads();
+        if (!ok) return;
+    }
+}
+
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// residual + PSF bytes up to which the persistent kernel is chosen (they stay in the 126 MB L2)
+constexpr size_t kPersistBytes = size_t(48) << 20;
+int g_hog_strategy = TCV_HOGBOM_AUTO;
 
 int hog_blocks(long long n)
 {
@@ -325,6 +433,31 @@ tcv_status tcv_hogbom_deconvolve(const float* d_dirty, int width, const float* d
     hog_scan_kernel<<<a.nblocks, kHogThreads, 0, st>>>(d_dirty, d_residual, a.n, a.nblocks, a.keys, a.vals, a.state, 0);
     TCV_CUDA(cudaGetLastError());
     const bool vec = width % 4 == 0 && reinterpret_cast<uintptr_t>(d_residual) % 16 == 0;
+    // images whose residual and PSF sit in L2 run every iteration in one cooperative launch
+    const size_t resident = size_t(a.n) * 4 + size_t(np) * 4;
+    bool persist = g_hog_strategy == TCV_HOGBOM_PERSISTENT ||
+                   (g_hog_strategy == TCV_HOGBOM_AUTO && resident <= kPersistBytes);
+    int dev = 0, coop = 0, sms = 0, per_sm = 0;
+    if (persist) {
+        TCV_CUDA(cudaGetDevice(&dev));
+        TCV_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        TCV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (vec)
+            TCV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hog_persist_kernel<true>, kHogThreads, 0));
+        else
+            TCV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hog_persist_kernel<false>, kHogThreads, 0));
+        persist = coop && per_sm > 0;
+    }
+    if (persist && niters > 0) {
+        // two CTAs per SM at most (fewer candidates per barrier), never more than resident
+        a.nblocks = std::max(1, std::min({sms * std::min(per_sm, 2), hog_blocks(a.n), width}));
+        int n_it = niters;
+        void* args[] = {&a, &n_it};
+        TCV_CUDA(cudaLaunchCooperativeKernel(vec ? reinterpret_cast<const void*>(hog_persist_kernel<true>)
+                                                 : reinterpret_cast<const void*>(hog_persist_kernel<false>),
+                                             dim3(unsigned(a.nblocks)), dim3(kHogThreads), args, 0, st));
+        return TCV_OK;
+    }
     for (int it = 0; it < niters; ++it) {
         if (vec)
             hog_iter_kernel<true><<<a.nblocks, kHogThreads, 0, st>>>(a, it);
@@ -333,6 +466,11 @@ tcv_status tcv_hogbom_deconvolve(const float* d_dirty, int width, const float* d
     }
     TCV_CUDA(cudaGetLastError());
     return TCV_OK;
+}
+
+void tcv_hogbom_set_strategy(int strategy)
+{
+    if (strategy >= TCV_HOGBOM_AUTO && strategy <= TCV_HOGBOM_PERSISTENT) g_hog_strategy = strategy;
 }
 
 tcv_status tcv_hogbom_result(const void* d_work, int* iters_done, int* stopped_at, int64_t* skipped_rows,
@@ -347,7 +485,7 @@ tcv_status tcv_hogbom_result(const void* d_work, int* iters_done, int* stopped_a
     if (stopped_at) *stopped_at = h.stopped - 1;
     if (skipped_rows) *skipped_rows = int64_t(h.skipped_rows);
     if (psf_peak_pos) *psf_peak_pos = int64_t(h.psf_pos);
-    return TCV_OK;
+    return h.error ? TCV_ERR_TIMEOUT : TCV_OK;
 }
 
 tcv_status tcv_find_peak(const float* d_image, int64_t n, float* val_out, int64_t* pos_out, void* d_work,

@@ -180,3 +180,67 @@ class Benchmark:
         s, o = np.empty(g.w_size, np.int32), np.empty(g.w_size, np.int32)
         check(lib().tcv_cur_get_planes(self._ctx, _p(s), _p(o)), "tcv_cur_get_planes")
         return s, o
+
+
+def main(argv=None) -> int:
+    """current/tConvolveMPI's driver (current/tConvolveMPI/tConvolveMPI.cc:61-186) on one GPU:
+    the continuum then the spectral run on one object, runGrid and runDegrid each timed, and the
+    reference's report lines.  --tune picks the plan with tcv_cur_tune first (untimed);
+    --runs selects run types; --repeat times each pass that many times (the last is reported)."""
+    import argparse
+    import time
+
+    ap = argparse.ArgumentParser(prog="python -m tconvolve.current")
+    ap.add_argument("--runs", default="0,1", help="run types in order (0 continuum, 1 spectral, 2-4 tests)")
+    ap.add_argument("--sort", type=int, default=0)
+    ap.add_argument("--tune", action="store_true")
+    ap.add_argument("--repeat", type=int, default=1)
+    a = ap.parse_args(argv)
+    b = Benchmark()
+    b.setSort(a.sort)
+    for run in (int(r) for r in a.runs.split(",")):
+        b.setRunType(run)
+        print(f"+++++ Test {b.getRunType()} +++++")
+        b.init()
+        if a.tune:
+            best, ms, _ = b.tune()
+            print(f"    Tuned plan (rows, group MiB, split, degrid split) = {best}, {ms:.3f} ms per grid+degrid")
+        ngridvis = float(b.nVisibilitiesGridded())
+        ngridpix = float(b.nPixelsGridded())
+        label = {0: "Continuum", 1: "Spectral"}.get(run)
+        for kind in ("grid", "degrid"):
+            for _ in range(a.repeat):
+                b.sync()
+                t0 = time.perf_counter()
+                b.runGrid() if kind == "grid" else b.runDegrid()
+                b.sync()
+                t = time.perf_counter() - t0
+            if kind == "grid":
+                print("  Forward processing")
+                print("    Number of processes: 1")
+                print(f"    Time {t} (s) ")
+                print(f"    Time per visibility spectral sample {1e6 * t / ngridvis} (us) ")
+                print(f"    Time per gridding   {1e9 * t / ngridpix} (ns) ")
+                print(f"    Gridding rate (per process)   {(ngridvis / 1e6) / t} (Mvis/sec)")
+                print(f"    Gridding rate (per process)   {(ngridpix / 1e6) / t} (Mpix/sec)")
+                print(f"    Gridding rate (total)      {(ngridpix / 1e6) / t} (Mpix/sec)")
+                if label:
+                    print(f"    {label} gridding performance (per process):   {(ngridpix / 1e6) / t} (Mpix/sec)")
+            else:
+                print("  Reverse processing")
+                print("    Number of processes: 1")
+                print(f"    Time {t} (s) ")
+                print(f"    Time per visibility spectral sample {1e6 * t / ngridvis} (us) ")
+                print(f"    Time per degridding {1e9 * t / ngridpix} (ns) ")
+                print(f"    Degridding rate (per node) {(ngridvis / 1e6) / t} (Mvis/sec)")
+                print(f"    Degridding rate (per node) {(ngridpix / 1e6) / t} (Mpix/sec)")
+                print(f"    Degridding rate (total)    {(ngridpix / 1e6) / t} (Mpix/sec)")
+                if label:
+                    print(f"    {label} degridding performance (per process):   {(ngridpix / 1e6) / t} (Mpix/sec)")
+        print("Done")
+    b.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -564,8 +564,15 @@ tcv_status tcv_hogbom_deconvolve(const float *d_dirty, int width, const float *d
                                  float *d_model, float *d_residual, int niters, float gain,
                                  float threshold, float *d_hist_val, uint32_t *d_hist_pos,
                                  void *d_work, size_t work_bytes, void *stream);
+/* How tcv_hogbom_deconvolve issues the iterations (process-wide): AUTO (default) runs images
+ * whose residual and PSF fit in 48 MiB as one cooperative launch of all iterations (CTAs meet at a
+ * bounded grid barrier per iteration) and larger ones as one launch per iteration; the other two
+ * force either form.  Results are identical. */
+enum { TCV_HOGBOM_AUTO = 0, TCV_HOGBOM_PER_LAUNCH = 1, TCV_HOGBOM_PERSISTENT = 2 };
+void tcv_hogbom_set_strategy(int strategy);
 /* After tcv_hogbom_deconvolve (synchronises): iterations done, the iteration that met the
- * threshold (-1 if none), PSF rows skipped, the PSF peak index.  Any output may be NULL. */
+ * threshold (-1 if none), PSF rows skipped, the PSF peak index.  Any output may be NULL.
+ * TCV_ERR_TIMEOUT if a grid-barrier wait of the persistent form gave up (the loop stopped). */
 tcv_status tcv_hogbom_result(const void *d_work, int *iters_done, int *stopped_at,
                              int64_t *skipped_rows, int64_t *psf_peak_pos, void *stream);
 /* findPeak (HogbomGolden.cc:127-139): the value of largest magnitude and its first index

@@ -112,3 +112,25 @@ def test_hogbom_deterministic(tcv, cuda_ok):
     a = _device_run(dirty, 512, psf, 512, 300, 0.1, 0.0)
     b = _device_run(dirty, 512, psf, 512, 300, 0.1, 0.0)
     assert all(np.array_equal(x, y) for x, y in zip(a[:4], b[:4]))
+
+
+@pytest.mark.parametrize("width", [512, 100])
+def test_persistent_and_per_launch_forms_agree(tcv, orc, cuda_ok, width):
+    """The cooperative all-iterations launch and the launch-per-iteration form give the same bits
+    (and the oracle's), on a float4-aligned width and an odd one."""
+    from tconvolve._lib import lib
+    from tconvolve.workload import synthetic_dirty, synthetic_psf
+
+    dirty, psf = synthetic_dirty(width, 15, 1e-3, seed=13), synthetic_psf(width)
+    runs = []
+    try:
+        for strategy in (1, 2):  # TCV_HOGBOM_PER_LAUNCH, TCV_HOGBOM_PERSISTENT
+            lib().tcv_hogbom_set_strategy(strategy)
+            runs.append(_device_run(dirty, width, psf, width, 400, 0.1, 1e-5))
+    finally:
+        lib().tcv_hogbom_set_strategy(0)
+    (m1, r1, v1, p1, s1), (m2, r2, v2, p2, s2) = runs
+    assert s1 == s2
+    assert np.array_equal(m1, m2) and np.array_equal(r1, r2) and np.array_equal(p1, p2) and np.array_equal(v1, v2)
+    o = orc.hogbom(dirty, psf, 400, 0.1, 1e-5)
+    assert np.array_equal(m2, o["model"]) and np.array_equal(r2, o["residual"])
