@@ -194,6 +194,7 @@ def main(argv=None) -> int:
     ap.add_argument("--runs", default="0,1", help="run types in order (0 continuum, 1 spectral, 2-4 tests)")
     ap.add_argument("--sort", type=int, default=0)
     ap.add_argument("--tune", action="store_true")
+    ap.add_argument("--tuning", default=None, help="fixed plan: tile rows,group MiB,split,degrid split")
     ap.add_argument("--repeat", type=int, default=1)
     a = ap.parse_args(argv)
     b = Benchmark()
@@ -201,6 +202,9 @@ def main(argv=None) -> int:
     for run in (int(r) for r in a.runs.split(",")):
         b.setRunType(run)
         print(f"+++++ Test {b.getRunType()} +++++")
+        if a.tuning:
+            rows, mib, split, dsplit = (int(x) for x in a.tuning.split(","))
+            b.set_tuning(mib, split, dsplit, rows)
         b.init()
         if a.tune:
             best, ms, _ = b.tune()
