@@ -630,9 +630,10 @@ tcv_status tcv_cur_set_ctype(tcv_cur_ctx* c, int c_type)
 tcv_status tcv_cur_set_tuning(tcv_cur_ctx* c, const tcv_tuning* t)
 {
     if (!c || !t || (t->tile_rows != 0 && t->tile_rows != 8 && t->tile_rows != 16) || t->group_mib < -1 ||
-        t->split < 0 || t->degrid_split < 0)
+        t->split < 0 || t->degrid_split < 0 || (t->kernel != 0 && !(t->kernel == 1 && t->tile_rows == 8)))
         return TCV_ERR_ARG;
-    c->tuning = tcv_tuning{t->tile_rows ? t->tile_rows : 16, t->group_mib ? t->group_mib : 32, t->split, t->degrid_split};
+    c->tuning = tcv_tuning{t->tile_rows ? t->tile_rows : 16, t->group_mib ? t->group_mib : 32, t->split, t->degrid_split,
+                           t->kernel};
     return c->initialized ? cur_build_plan(c) : TCV_OK;
 }
 
@@ -682,12 +683,14 @@ tcv_status tcv_cur_tune(tcv_cur_ctx* c, int reps, tcv_tuning* best_out, float* b
         }
         return TCV_OK;
     };
-    // stage 1: tile height x plane-group slice (slices that give the same grouping timed once)
+    // stage 1: kernel family and tile height x plane-group slice (slices that give the same
+    // grouping timed once); kernel 1 = the sample-parallel kernels on 8-row tiles
     if (s == TCV_OK) {
-        std::vector<std::pair<int, int>> seen;  // (rows, number of plane groups)
-        for (int rows : {16, 8})
+        std::vector<std::pair<int, int>> seen;  // (rows, or -1 for the sample-parallel kernels; plane groups)
+        for (int variant : {16, 8, -1})
             for (int mib : {32, 128, -1}) {
-                const tcv_tuning t{rows, mib, 0, 0};
+                const int rows = variant < 0 ? 8 : variant;
+                const tcv_tuning t{rows, mib, 0, 0, variant < 0 ? 1 : 0};
                 int groups = 1;
                 const int64_t budget = mib > 0 ? (int64_t(mib) << 20) : INT64_MAX;
                 int64_t used = 0;
@@ -700,7 +703,7 @@ tcv_status tcv_cur_tune(tcv_cur_ctx* c, int reps, tcv_tuning* best_out, float* b
                     }
                     used += bytes;
                 }
-                const std::pair<int, int> id(rows, groups);
+                const std::pair<int, int> id(variant, groups);
                 if (std::find(seen.begin(), seen.end(), id) != seen.end()) continue;
                 seen.push_back(id);
                 if ((s = time_one(t)) != TCV_OK) break;
@@ -709,12 +712,13 @@ tcv_status tcv_cur_tune(tcv_cur_ctx* c, int reps, tcv_tuning* best_out, float* b
     if (s == TCV_OK) {  // stage 2: gridding work units
         const tcv_tuning base = best;
         for (int split : {256, 128, 64})  // the partial-tile bound grows as 1 / split
-            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, split, 0})) != TCV_OK) break;
+            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, split, 0, base.kernel})) != TCV_OK) break;
     }
     if (s == TCV_OK) {  // stage 3: degridding work units
         const tcv_tuning base = best;
         for (int split : {128, 64, 32, 16})
-            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, base.split, split})) != TCV_OK) break;
+            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, base.split, split, base.kernel})) != TCV_OK)
+                break;
     }
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (cudaEvent_t x : ev)

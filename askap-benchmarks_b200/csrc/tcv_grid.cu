@@ -98,17 +98,30 @@ tcv_status launch_adjoint(const tcv_plan* p, const float2* grid, const void* c, 
     return slot_reduce(p, c_scale, out, st);
 }
 
+}  // namespace
+
+tcv_status launch_fold8(const tcv_plan* p, const GridArgs& a, cudaStream_t st)
+{
+    fold_kernel<8><<<fold_ctas(), kTileThreads, 0, st>>>(p->items, p->group_start, p->nunits, p->pstart, a);
+    TCV_CUDA(cudaGetLastError());
+    return TCV_OK;
+}
+
+namespace {
+
 template <class Tab>
 tcv_status grid_rows(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
                      cudaStream_t st, int c_type)
 {
     if (p->g.var) {  // per-sample widths: complex tables (the w-term is complex), 64 x 64 or 64 x 32 tiles
         if constexpr (!Tab::kReal) {
+            if (p->g.dense) return launch_dense_grid<Tab>(p, data, c, c_scale, grid, st);
             if (p->g.rows == 16) return launch<Tab, 16, true>(p, data, c, c_scale, grid, st, c_type);
             if (p->g.rows == 8) return launch<Tab, 8, true>(p, data, c, c_scale, grid, st, c_type);
         }
         return TCV_ERR_UNSUPPORTED;
     }
+    if (p->g.dense) return TCV_ERR_UNSUPPORTED;  // sample-parallel kernels: variable-width plans only
     switch (p->g.rows) {
         case 8: return launch<Tab, 8>(p, data, c, c_scale, grid, st, c_type);
         case 16: return launch<Tab, 16>(p, data, c, c_scale, grid, st, c_type);
@@ -123,11 +136,13 @@ tcv_status degrid_rows(const tcv_plan* p, const float2* grid, const void* c, flo
 {
     if (p->g.var) {
         if constexpr (!Tab::kReal) {
+            if (p->g.dense) return launch_dense_degrid<Tab>(p, grid, c, c_scale, out, st);
             if (p->g.rows == 16) return launch_adjoint<Tab, 16, true>(p, grid, c, c_scale, out, st, c_type);
             if (p->g.rows == 8) return launch_adjoint<Tab, 8, true>(p, grid, c, c_scale, out, st, c_type);
         }
         return TCV_ERR_UNSUPPORTED;
     }
+    if (p->g.dense) return TCV_ERR_UNSUPPORTED;  // sample-parallel kernels: variable-width plans only
     switch (p->g.rows) {
         case 8: return launch_adjoint<Tab, 8>(p, grid, c, c_scale, out, st, c_type);
         case 16: return launch_adjoint<Tab, 16>(p, grid, c, c_scale, out, st, c_type);

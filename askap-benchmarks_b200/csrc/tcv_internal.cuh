@@ -46,6 +46,7 @@ struct PlanGeom {
     int rows, tw, th;
     int split;          // samples per gridding work unit of a split cell (0: cells are never split)
     int dsplit;         // the same for degridding
+    bool dense;         // variable-width plans: sample-parallel kernels (tcv_dense.cu)
     int ntx, nty;       // tiles per row / column of a one-job plan
     int64_t ntiles;     // tiles of all jobs
     int max_tiles;      // tiles one footprint can touch
@@ -145,6 +146,15 @@ void jit_prepare(int c_type, int s, int rows);
 tcv_status fft_exec(float2* d_grid, int n, bool forward, cudaStream_t st);
 tcv_status image_from_grid(float2* d_grid, int n, float scale, float* d_image, float2* d_image_c, cudaStream_t st);
 tcv_status grid_from_image(const float* d_image, int n, float2* d_grid, cudaStream_t st);
+// Sample-parallel kernels of variable-width plans on 64 x 32 tiles (tcv_dense.cu).
+template <class Tab>
+tcv_status launch_dense_grid(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
+                             cudaStream_t st);
+template <class Tab>
+tcv_status launch_dense_degrid(const tcv_plan* p, const float2* grid, const void* c, float c_scale, float2* out,
+                               cudaStream_t st);
+// fold_kernel<8> over one plane group of a plan (the partial tiles of its split cells)
+tcv_status launch_fold8(const tcv_plan* p, const GridArgs& a, cudaStream_t st);
 // Record the candidates and median times of the last tuning run (read by tcv_autotune_report).
 void tune_report_set(const std::vector<std::pair<tcv_tuning, float>>& report);
 

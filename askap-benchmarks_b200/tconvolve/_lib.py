@@ -67,10 +67,13 @@ class TcvJob(ctypes.Structure):
 
 class TcvTuning(ctypes.Structure):
     _fields_ = [("tile_rows", ctypes.c_int32), ("group_mib", ctypes.c_int32), ("split", ctypes.c_int32),
-                ("degrid_split", ctypes.c_int32)]
+                ("degrid_split", ctypes.c_int32), ("kernel", ctypes.c_int32)]
 
     def as_tuple(self):
-        return (int(self.tile_rows), int(self.group_mib), int(self.split), int(self.degrid_split))
+        """(tile_rows, group_mib, split, degrid_split), with a fifth entry, kernel, when it is not
+        the tile kernels (1: the sample-parallel kernels of variable-width plans)."""
+        t = (int(self.tile_rows), int(self.group_mib), int(self.split), int(self.degrid_split))
+        return t + (int(self.kernel),) if self.kernel else t
 
 
 class TcvServerConfig(ctypes.Structure):

@@ -109,9 +109,11 @@ class Benchmark:
             c_type = _lib.CTYPE_BY_NAME[c_type]
         check(lib().tcv_cur_set_ctype(self._ctx, int(c_type)), "tcv_cur_set_ctype")
 
-    def set_tuning(self, group_mib: int = 32, split: int = 0, degrid_split: int = 0, tile_rows: int = 16):
-        """Plane-group slice, work-unit sizes and tile height (rows per warp, 8 or 16) of the plan."""
-        t = TcvTuning(int(tile_rows), int(group_mib), int(split), int(degrid_split))
+    def set_tuning(self, group_mib: int = 32, split: int = 0, degrid_split: int = 0, tile_rows: int = 16,
+                   kernel: int = 0):
+        """Plane-group slice, work-unit sizes, tile height (rows per warp, 8 or 16) and kernel family
+        (0 tile kernels, 1 sample-parallel kernels, which need tile_rows 8) of the plan."""
+        t = TcvTuning(int(tile_rows), int(group_mib), int(split), int(degrid_split), int(kernel))
         check(lib().tcv_cur_set_tuning(self._ctx, ctypes.byref(t)), "tcv_cur_set_tuning")
         self._tuning = t.as_tuple()
 
@@ -194,7 +196,8 @@ def main(argv=None) -> int:
     ap.add_argument("--runs", default="0,1", help="run types in order (0 continuum, 1 spectral, 2-4 tests)")
     ap.add_argument("--sort", type=int, default=0)
     ap.add_argument("--tune", action="store_true")
-    ap.add_argument("--tuning", default=None, help="fixed plan: tile rows,group MiB,split,degrid split")
+    ap.add_argument("--tuning", default=None,
+                    help="fixed plan: tile rows,group MiB,split,degrid split[,kernel (1: sample-parallel)]")
     ap.add_argument("--repeat", type=int, default=1)
     a = ap.parse_args(argv)
     b = Benchmark()
@@ -203,8 +206,8 @@ def main(argv=None) -> int:
         b.setRunType(run)
         print(f"+++++ Test {b.getRunType()} +++++")
         if a.tuning:
-            rows, mib, split, dsplit = (int(x) for x in a.tuning.split(","))
-            b.set_tuning(mib, split, dsplit, rows)
+            v = [int(x) for x in a.tuning.split(",")]
+            b.set_tuning(v[1], v[2], v[3], v[0], v[4] if len(v) > 4 else 0)
         b.init()
         if a.tune:
             best, ms, _ = b.tune()

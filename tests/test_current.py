@@ -12,7 +12,8 @@ Bars (written here, used below):
     0.5% and 4 ulp);
   * grid and degridded samples, plain complex64 form, cells whole: relative L2 <= 1e-5
     (REL_L2_FP32) against the oracle (the reference's arithmetic and order, pinned bit-exact);
-  * with busy cells split into work units the FP32 sums are grouped differently; the reference's
+  * with busy cells split into work units, or with the sample-parallel kernels (which sum each
+    point per warp, then the warps in order), the FP32 sums are grouped differently; the reference's
     own FP32 grid is then the yardstick: the relative L2 distance of our grid from the FP64 grid
     at most 1.5 x the reference's (both ~8e-6 on the spectral problem with unit data, where
     thousands of samples pile on each point), and degridding within 1e-6 of the FP64 degridding
@@ -199,29 +200,33 @@ def _check_tuned(b, orc):
     s_size, _ = b.planes()
     g = b.geometry()
     split = b.tuning()[2]
-    if split == 0:  # gridding cells whole: the reference's order at every point
+    ref_order = split == 0 and len(b.tuning()) == 4  # tile kernels, cells whole
+    if ref_order:  # gridding cells whole: the reference's order at every point
         assert orc.rel_l2(g1, grid_ref) <= REL_L2_FP32
     else:
         g64 = orc.cur_grid_f64(np.ones(iu.size, np.complex64), iu, iv, wp, co, s_size, c, g.g_size, threads=16)
         assert orc.rel_l2(g1, g64) <= 1.5 * orc.rel_l2(grid_ref, g64) + 1e-7
     o64 = orc.cur_degrid_f64(g1, g.g_size, iu, iv, wp, co, s_size, c, threads=16)
     assert orc.rel_l2(o1, o64) <= 1e-6
-    if split == 0:
+    if ref_order:
         assert orc.rel_l2(o1, out_ref) <= REL_L2_FP32
 
 
 @pytest.mark.parametrize("tuning", [(32, 0, 0, 16), (8, 0, 64, 16), (8, 64, 64, 16), (-1, 256, 128, 16),
-                                    (32, 0, 0, 8), (-1, 128, 64, 8), (32, 256, 8, 8)])
+                                    (32, 0, 0, 8), (-1, 128, 64, 8), (32, 256, 8, 8),
+                                    (32, 0, 0, 8, 1), (-1, 256, 128, 8, 1), (8, 64, 16, 8, 1)])
 def test_current_tunings_and_determinism(tcv, orc, cuda_ok, tuning):
-    """Plane groups, work units and tile heights change the summation order only: every tuning
-    within its bar (module docstring), each bit-identical when rerun."""
+    """Plane groups, work units, tile heights and the sample-parallel kernels (fifth entry 1)
+    change the summation order only: every tuning within its bar (module docstring; the
+    sample-parallel kernels group each point's sum by warp, so they are judged as split cells
+    are), each bit-identical when rerun."""
     from tconvolve.current import Benchmark
 
     b = Benchmark()
     b.setRunType(1)
     b.init()
     b.set_tuning(*tuning)
-    assert b.tuning() == (tuning[3],) + tuning[:3]
+    assert b.tuning() == (tuning[3],) + tuning[:3] + tuning[4:]
     _check_tuned(b, orc)
     b.close()
 
