@@ -630,7 +630,7 @@ tcv_status tcv_cur_set_ctype(tcv_cur_ctx* c, int c_type)
 tcv_status tcv_cur_set_tuning(tcv_cur_ctx* c, const tcv_tuning* t)
 {
     if (!c || !t || (t->tile_rows != 0 && t->tile_rows != 8 && t->tile_rows != 16) || t->group_mib < -1 ||
-        t->split < 0 || t->degrid_split < 0 || (t->kernel != 0 && !(t->kernel == 1 && t->tile_rows == 8)))
+        t->split < 0 || t->degrid_split < 0 || (t->kernel != 0 && !(t->kernel >= 1 && t->kernel <= 3 && t->tile_rows == 8)))
         return TCV_ERR_ARG;
     c->tuning = tcv_tuning{t->tile_rows ? t->tile_rows : 16, t->group_mib ? t->group_mib : 32, t->split, t->degrid_split,
                            t->kernel};
@@ -683,14 +683,15 @@ tcv_status tcv_cur_tune(tcv_cur_ctx* c, int reps, tcv_tuning* best_out, float* b
         }
         return TCV_OK;
     };
-    // stage 1: kernel family and tile height x plane-group slice (slices that give the same
-    // grouping timed once); kernel 1 = the sample-parallel kernels on 8-row tiles
+    // stage 1: kernel families and tile height x plane-group slice (slices that give the same
+    // grouping timed once).  Variants: 64 x 64 and 64 x 32 tile kernels; on 64 x 32 tiles the
+    // sample-parallel degridding, and both passes sample-parallel (kernel bits 2 and 3).
     if (s == TCV_OK) {
-        std::vector<std::pair<int, int>> seen;  // (rows, or -1 for the sample-parallel kernels; plane groups)
-        for (int variant : {16, 8, -1})
+        std::vector<std::pair<int, int>> seen;  // (variant, number of plane groups)
+        for (int variant : {16, 8, -2, -3})
             for (int mib : {32, 128, -1}) {
                 const int rows = variant < 0 ? 8 : variant;
-                const tcv_tuning t{rows, mib, 0, 0, variant < 0 ? 1 : 0};
+                const tcv_tuning t{rows, mib, 0, 0, variant < 0 ? -variant : 0};
                 int groups = 1;
                 const int64_t budget = mib > 0 ? (int64_t(mib) << 20) : INT64_MAX;
                 int64_t used = 0;

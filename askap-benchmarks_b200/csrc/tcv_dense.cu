@@ -106,45 +106,53 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
                 const int w = R.c1 - R.c0;
                 if (w <= 0 || R.r1 <= R.r0) continue;  // no overlap (a binned sample always has one); warp-uniform
                 const int pbase = (fy - ty0) * kDTW + (fx - tx0);  // tile point of footprint (0, 0)
+                // U steps per iteration: every table load of the iteration is issued before any
+                // update of the warp's tile copy (memory in flight at 12 warps per SM)
+                constexpr int U = 4;
                 if (w <= 32) {
                     const int kk = L.k[w], qq = L.q[w][lane], rr = L.r[w][lane];
                     const bool lane_ok = qq < kk;
                     const int col = R.c0 + rr;
-                    for (int row0 = R.r0; row0 < R.r1; row0 += 2 * kk) {
-                        const int ra = row0 + qq, rb = row0 + kk + qq;
-                        const bool oka = lane_ok && ra < R.r1, okb = lane_ok && rb < R.r1;
-                        const float2 ca = oka ? Tab::load(ctab + (cs.x + ra * s + col)) : make_float2(0.f, 0.f);
-                        const float2 cb = okb ? Tab::load(ctab + (cs.x + rb * s + col)) : make_float2(0.f, 0.f);
-                        if (oka) {
-                            float2& g = acc[pbase + ra * kDTW + col];
-                            float2 t = g;
-                            cmac<Tab::kReal>(t, dv, ca);
-                            g = t;
+                    for (int row0 = R.r0; row0 < R.r1; row0 += U * kk) {
+                        float2 cv[U];
+                        bool ok[U];
+#pragma unroll
+                        for (int e = 0; e < U; ++e) {
+                            const int row = row0 + e * kk + qq;
+                            ok[e] = lane_ok && row < R.r1;
+                            cv[e] = ok[e] ? Tab::load(ctab + (cs.x + row * s + col)) : make_float2(0.f, 0.f);
                         }
-                        if (okb) {
-                            float2& g = acc[pbase + rb * kDTW + col];
-                            float2 t = g;
-                            cmac<Tab::kReal>(t, dv, cb);
-                            g = t;
+#pragma unroll
+                        for (int e = 0; e < U; ++e) {
+                            if (ok[e]) {
+                                float2& g = acc[pbase + (row0 + e * kk + qq) * kDTW + col];
+                                float2 t = g;
+                                cmac<Tab::kReal>(t, dv, cv[e]);
+                                g = t;
+                            }
                         }
                     }
                 } else {
                     const int ca0 = R.c0 + lane, cb0 = R.c0 + 32 + lane;
                     const bool oka = ca0 < R.c1, okb = cb0 < R.c1;
-                    for (int row = R.r0; row < R.r1; ++row) {
-                        const float2 ca = oka ? Tab::load(ctab + (cs.x + row * s + ca0)) : make_float2(0.f, 0.f);
-                        const float2 cb = okb ? Tab::load(ctab + (cs.x + row * s + cb0)) : make_float2(0.f, 0.f);
-                        if (oka) {
-                            float2& g = acc[pbase + row * kDTW + ca0];
-                            float2 t = g;
-                            cmac<Tab::kReal>(t, dv, ca);
-                            g = t;
+                    for (int row0 = R.r0; row0 < R.r1; row0 += U / 2) {
+                        float2 cv[U];
+                        bool ok[U];
+#pragma unroll
+                        for (int e = 0; e < U; ++e) {
+                            const int row = row0 + e / 2;
+                            ok[e] = row < R.r1 && ((e & 1) ? okb : oka);
+                            cv[e] = ok[e] ? Tab::load(ctab + (cs.x + row * s + ((e & 1) ? cb0 : ca0)))
+                                          : make_float2(0.f, 0.f);
                         }
-                        if (okb) {
-                            float2& g = acc[pbase + row * kDTW + cb0];
-                            float2 t = g;
-                            cmac<Tab::kReal>(t, dv, cb);
-                            g = t;
+#pragma unroll
+                        for (int e = 0; e < U; ++e) {
+                            if (ok[e]) {
+                                float2& g = acc[pbase + (row0 + e / 2) * kDTW + ((e & 1) ? cb0 : ca0)];
+                                float2 t = g;
+                                cmac<Tab::kReal>(t, dv, cv[e]);
+                                g = t;
+                            }
                         }
                     }
                 }

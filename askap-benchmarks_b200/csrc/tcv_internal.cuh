@@ -46,7 +46,8 @@ struct PlanGeom {
     int rows, tw, th;
     int split;          // samples per gridding work unit of a split cell (0: cells are never split)
     int dsplit;         // the same for degridding
-    bool dense;         // variable-width plans: sample-parallel kernels (tcv_dense.cu)
+    bool dense;         // variable-width plans: sample-parallel gridding kernel (tcv_dense.cu)
+    bool ddense;        // variable-width plans: sample-parallel degridding kernel
     int ntx, nty;       // tiles per row / column of a one-job plan
     int64_t ntiles;     // tiles of all jobs
     int max_tiles;      // tiles one footprint can touch

@@ -111,8 +111,9 @@ class Benchmark:
 
     def set_tuning(self, group_mib: int = 32, split: int = 0, degrid_split: int = 0, tile_rows: int = 16,
                    kernel: int = 0):
-        """Plane-group slice, work-unit sizes, tile height (rows per warp, 8 or 16) and kernel family
-        (0 tile kernels, 1 sample-parallel kernels, which need tile_rows 8) of the plan."""
+        """Plane-group slice, work-unit sizes, tile height (rows per warp, 8 or 16) and the passes
+        that use the sample-parallel kernels (bit mask: 1 gridding, 2 degridding; needs tile_rows
+        8) of the plan."""
         t = TcvTuning(int(tile_rows), int(group_mib), int(split), int(degrid_split), int(kernel))
         check(lib().tcv_cur_set_tuning(self._ctx, ctypes.byref(t)), "tcv_cur_set_tuning")
         self._tuning = t.as_tuple()
@@ -197,7 +198,8 @@ def main(argv=None) -> int:
     ap.add_argument("--sort", type=int, default=0)
     ap.add_argument("--tune", action="store_true")
     ap.add_argument("--tuning", default=None,
-                    help="fixed plan: tile rows,group MiB,split,degrid split[,kernel (1: sample-parallel)]")
+                    help="fixed plan: tile rows,group MiB,split,degrid split[,kernel bits (1 gridding, "
+                         "2 degridding: sample-parallel)]")
     ap.add_argument("--repeat", type=int, default=1)
     a = ap.parse_args(argv)
     b = Benchmark()

@@ -190,9 +190,10 @@ typedef struct tcv_tuning {
                       (the units write partial tiles that are folded into the grid in unit
                       order); 0 = cells are never split */
     int degrid_split; /* the same for degridding (units need no fold there) */
-    int kernel;    /* 0: the tile kernels (every lane owns grid columns); 1: the sample-parallel
-                      kernels of variable-width plans (one warp per sample, lanes spread densely
-                      over the footprint; for kernels much narrower than 32; tile rows must be 8) */
+    int kernel;    /* bit mask of the passes that use the sample-parallel kernels of variable-width
+                      plans (one warp per sample, lanes spread densely over the footprint, for
+                      kernels much narrower than 32; tile rows must be 8): 1 gridding,
+                      2 degridding; 0 = the tile kernels (every lane owns grid columns) */
 } tcv_tuning;
 
 /* Workspace of a batched plan (0 for invalid arguments).  tuning may be NULL (defaults). */

@@ -200,7 +200,7 @@ def _check_tuned(b, orc):
     s_size, _ = b.planes()
     g = b.geometry()
     split = b.tuning()[2]
-    ref_order = split == 0 and len(b.tuning()) == 4  # tile kernels, cells whole
+    ref_order = split == 0 and not (len(b.tuning()) > 4 and b.tuning()[4] & 1)  # tile gridding, cells whole
     if ref_order:  # gridding cells whole: the reference's order at every point
         assert orc.rel_l2(g1, grid_ref) <= REL_L2_FP32
     else:
@@ -214,12 +214,12 @@ def _check_tuned(b, orc):
 
 @pytest.mark.parametrize("tuning", [(32, 0, 0, 16), (8, 0, 64, 16), (8, 64, 64, 16), (-1, 256, 128, 16),
                                     (32, 0, 0, 8), (-1, 128, 64, 8), (32, 256, 8, 8),
-                                    (32, 0, 0, 8, 1), (-1, 256, 128, 8, 1), (8, 64, 16, 8, 1)])
+                                    (32, 0, 0, 8, 3), (-1, 256, 128, 8, 3), (8, 64, 16, 8, 2), (32, 0, 0, 8, 1)])
 def test_current_tunings_and_determinism(tcv, orc, cuda_ok, tuning):
-    """Plane groups, work units, tile heights and the sample-parallel kernels (fifth entry 1)
-    change the summation order only: every tuning within its bar (module docstring; the
-    sample-parallel kernels group each point's sum by warp, so they are judged as split cells
-    are), each bit-identical when rerun."""
+    """Plane groups, work units, tile heights and the sample-parallel kernels (fifth entry: 1
+    gridding, 2 degridding, 3 both) change the summation order only: every tuning within its bar
+    (module docstring; sample-parallel gridding groups each point's sum by warp, so it is judged as
+    split cells are), each bit-identical when rerun."""
     from tconvolve.current import Benchmark
 
     b = Benchmark()
