@@ -63,6 +63,33 @@ __device__ __forceinline__ Rect clip(int fx, int fy, int s, int tx0, int ty0)
     return R;
 }
 
+// A staged sample, prepared once by the staging thread so that the warp that takes it only
+// walks its rectangle: the table index and tile point of the rectangle's first element, the table
+// row stride (the kernel width), and the rectangle's width, height and rows per step.
+struct DenseRec {
+    int c0;      // table index of the rectangle's first element (cOffset + r0 * s + c0)
+    int p0;      // tile point of that element
+    int s;       // table row stride
+    int shape;   // w | h << 8 | rows per step << 16 (h = 0: nothing to do)
+};
+
+__device__ __forceinline__ DenseRec prepare(int coffk, int s, int fx, int fy, int tx0, int ty0, const DenseLut& L)
+{
+    const Rect R = clip(fx, fy, s, tx0, ty0);
+    const int w = R.c1 - R.c0, h = R.r1 - R.r0;
+    DenseRec d;
+    d.s = s;
+    if (w <= 0 || h <= 0) {  // no overlap (a binned sample always has one)
+        d.c0 = d.p0 = 0;
+        d.shape = 0;
+        return d;
+    }
+    d.c0 = coffk + R.r0 * s + R.c0;
+    d.p0 = (fy + R.r0 - ty0) * kDTW + (fx + R.c0 - tx0);
+    d.shape = w | (h << 8) | ((w <= 32 ? int(L.k[w]) : 0) << 16);
+    return d;
+}
+
 template <class Tab>
 __global__ void __launch_bounds__(kGThreads)
 dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
@@ -72,13 +99,14 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
 {
     extern __shared__ float2 dsm[];
     float2* acc_all = dsm;                                                // [kGWarps][kDPts]
-    float4* rec = reinterpret_cast<float4*>(dsm + kGWarps * kDPts);      // [kGThreads]
-    int2* rci = reinterpret_cast<int2*>(rec + kGThreads);                 // (cOffset, width)
+    DenseRec* rec = reinterpret_cast<DenseRec*>(dsm + kGWarps * kDPts);  // [kGThreads]
+    float2* rdv = reinterpret_cast<float2*>(rec + kGThreads);             // scaled data
     __shared__ DenseLut L;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     build_lut(L, threadIdx.x, kGThreads);
     float2* acc = acc_all + warp * kDPts;
     for (int i = lane; i < kDPts; i += 32) acc[i] = make_float2(0.f, 0.f);
+    __syncthreads();  // the lane table is complete
     const u32 i1 = group_ustart[a.group + 1];
     for (u32 it = group_ustart[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
         const uint4 u = units[it];
@@ -91,41 +119,36 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
             if (int(threadIdx.x) < m) {
                 const u32 k = order[start + base + threadIdx.x];
                 const float2 d = data[k];
-                const int s = int(a.ssz[k]);
-                rec[threadIdx.x] = make_float4(d.x * a.c_scale, d.y * a.c_scale, __int_as_float(iu[k] - s / 2),
-                                               __int_as_float(iv[k]));
-                rci[threadIdx.x] = make_int2(coff[k], s);
+                const int sk = int(a.ssz[k]);
+                rec[threadIdx.x] = prepare(coff[k], sk, iu[k] - sk / 2, iv[k], tx0, ty0, L);
+                rdv[threadIdx.x] = make_float2(d.x * a.c_scale, d.y * a.c_scale);
             }
             __syncthreads();
+            // U steps per iteration: every table load of the iteration is issued before any update
+            // of the warp's tile copy (memory in flight at 12 warps per SM)
+            constexpr int U = 4;
             for (int j = warp; j < m; j += kGWarps) {
-                const float4 q = rec[j];
-                const int2 cs = rci[j];
-                const int s = cs.y, fx = __float_as_int(q.z), fy = __float_as_int(q.w);
-                const float2 dv = make_float2(q.x, q.y);
-                const Rect R = clip(fx, fy, s, tx0, ty0);
-                const int w = R.c1 - R.c0;
-                if (w <= 0 || R.r1 <= R.r0) continue;  // no overlap (a binned sample always has one); warp-uniform
-                const int pbase = (fy - ty0) * kDTW + (fx - tx0);  // tile point of footprint (0, 0)
-                // U steps per iteration: every table load of the iteration is issued before any
-                // update of the warp's tile copy (memory in flight at 12 warps per SM)
-                constexpr int U = 4;
+                const DenseRec d = rec[j];
+                const float2 dv = rdv[j];
+                const int w = d.shape & 255, h = (d.shape >> 8) & 255, kk = d.shape >> 16;
+                if (h == 0) continue;  // warp-uniform
                 if (w <= 32) {
-                    const int kk = L.k[w], qq = L.q[w][lane], rr = L.r[w][lane];
+                    const int qq = L.q[w][lane], rr = L.r[w][lane];
                     const bool lane_ok = qq < kk;
-                    const int col = R.c0 + rr;
-                    for (int row0 = R.r0; row0 < R.r1; row0 += U * kk) {
+                    const int cbase = d.c0 + qq * d.s + rr, pbase = d.p0 + qq * kDTW + rr;
+                    for (int row0 = 0; row0 < h; row0 += U * kk) {
                         float2 cv[U];
                         bool ok[U];
 #pragma unroll
                         for (int e = 0; e < U; ++e) {
-                            const int row = row0 + e * kk + qq;
-                            ok[e] = lane_ok && row < R.r1;
-                            cv[e] = ok[e] ? Tab::load(ctab + (cs.x + row * s + col)) : make_float2(0.f, 0.f);
+                            const int ro = row0 + e * kk;  // this step's first row; the lane's is ro + qq
+                            ok[e] = lane_ok && ro + qq < h;
+                            cv[e] = ok[e] ? Tab::load(ctab + (cbase + ro * d.s)) : make_float2(0.f, 0.f);
                         }
 #pragma unroll
                         for (int e = 0; e < U; ++e) {
                             if (ok[e]) {
-                                float2& g = acc[pbase + (row0 + e * kk + qq) * kDTW + col];
+                                float2& g = acc[pbase + (row0 + e * kk) * kDTW];
                                 float2 t = g;
                                 cmac<Tab::kReal>(t, dv, cv[e]);
                                 g = t;
@@ -133,22 +156,21 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
                         }
                     }
                 } else {
-                    const int ca0 = R.c0 + lane, cb0 = R.c0 + 32 + lane;
-                    const bool oka = ca0 < R.c1, okb = cb0 < R.c1;
-                    for (int row0 = R.r0; row0 < R.r1; row0 += U / 2) {
+                    const bool oka = lane < w, okb = lane + 32 < w;
+                    for (int row0 = 0; row0 < h; row0 += U / 2) {
                         float2 cv[U];
                         bool ok[U];
 #pragma unroll
                         for (int e = 0; e < U; ++e) {
                             const int row = row0 + e / 2;
-                            ok[e] = row < R.r1 && ((e & 1) ? okb : oka);
-                            cv[e] = ok[e] ? Tab::load(ctab + (cs.x + row * s + ((e & 1) ? cb0 : ca0)))
+                            ok[e] = row < h && ((e & 1) ? okb : oka);
+                            cv[e] = ok[e] ? Tab::load(ctab + (d.c0 + row * d.s + lane + (e & 1) * 32))
                                           : make_float2(0.f, 0.f);
                         }
 #pragma unroll
                         for (int e = 0; e < U; ++e) {
                             if (ok[e]) {
-                                float2& g = acc[pbase + (row0 + e / 2) * kDTW + ((e & 1) ? cb0 : ca0)];
+                                float2& g = acc[d.p0 + (row0 + e / 2) * kDTW + lane + (e & 1) * 32];
                                 float2 t = g;
                                 cmac<Tab::kReal>(t, dv, cv[e]);
                                 g = t;
@@ -198,9 +220,9 @@ dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int* __re
                     const uint4* __restrict__ units, const u32* __restrict__ group_ustart,
                     float2* __restrict__ slots, int max_tiles, GridArgs a)
 {
-    __shared__ float2 gt[kDPts];          // the grid tile
-    __shared__ int4 rec[kDThreads];       // (sample, first column, first row, cOffset)
-    __shared__ int rw[kDThreads];         // widths
+    __shared__ float2 gt[kDPts];           // the grid tile
+    __shared__ DenseRec rec[kDThreads];
+    __shared__ unsigned long long rslot[kDThreads];  // slot index of (sample, this tile)
     __shared__ DenseLut L;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     build_lut(L, threadIdx.x, kDThreads);
@@ -224,42 +246,35 @@ dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int* __re
             __syncthreads();
             if (int(threadIdx.x) < m) {
                 const u32 k = order[start + base + threadIdx.x];
-                const int s = int(a.ssz[k]);
-                rec[threadIdx.x] = make_int4(int(k), iu[k] - s / 2, iv[k], coff[k]);
-                rw[threadIdx.x] = s;
+                const int sk = int(a.ssz[k]);
+                const int fx = iu[k] - sk / 2, fy = iv[k];
+                rec[threadIdx.x] = prepare(coff[k], sk, fx, fy, tx0, ty0, L);
+                const int sx0 = fx / kDTW, sx1 = (fx + sk - 1) / kDTW, sy0 = fy / kDTH;
+                rslot[threadIdx.x] = (unsigned long long)(k) * max_tiles + (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0);
             }
             __syncthreads();
             for (int j = warp; j < m; j += kDWarps) {
-                const int4 q = rec[j];
-                const int s = rw[j], fx = q.y, fy = q.z;
-                const Rect R = clip(fx, fy, s, tx0, ty0);
-                const int w = R.c1 - R.c0;
-                const int pbase = (fy - ty0) * kDTW + (fx - tx0);
-                if (w <= 0 || R.r1 <= R.r0) {  // no overlap (a binned sample always has one): an empty slot
-                    if (lane == 0) {
-                        const int sx0 = fx / kDTW, sx1 = (fx + s - 1) / kDTW, sy0 = fy / kDTH;
-                        slots[(unsigned long long)(u32(q.x)) * max_tiles + (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0)] =
-                            make_float2(0.f, 0.f);
-                    }
-                    continue;
-                }
+                const DenseRec d = rec[j];
+                const int w = d.shape & 255, h = (d.shape >> 8) & 255, kk = d.shape >> 16;
                 float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);  // two FMA chains
-                if (w <= 32) {
-                    const int kk = L.k[w], qq = L.q[w][lane], rr = L.r[w][lane];
+                if (h > 0 && w <= 32) {
+                    const int qq = L.q[w][lane], rr = L.r[w][lane];
                     const bool lane_ok = qq < kk;
-                    const int col = R.c0 + rr;
-                    for (int row0 = R.r0; row0 < R.r1; row0 += 2 * kk) {
-                        const int ra = row0 + qq, rb = row0 + kk + qq;
-                        const bool oka = lane_ok && ra < R.r1, okb = lane_ok && rb < R.r1;
-                        if (oka) cmac<Tab::kReal>(p0, gt[pbase + ra * kDTW + col], Tab::load(ctab + (q.w + ra * s + col)));
-                        if (okb) cmac<Tab::kReal>(p1, gt[pbase + rb * kDTW + col], Tab::load(ctab + (q.w + rb * s + col)));
+                    const int cbase = d.c0 + qq * d.s + rr, pbase = d.p0 + qq * kDTW + rr;
+                    for (int row0 = 0; row0 < h; row0 += 2 * kk) {
+                        const bool oka = lane_ok && row0 + qq < h, okb = lane_ok && row0 + kk + qq < h;
+                        if (oka) cmac<Tab::kReal>(p0, gt[pbase + row0 * kDTW], Tab::load(ctab + (cbase + row0 * d.s)));
+                        if (okb)
+                            cmac<Tab::kReal>(p1, gt[pbase + (row0 + kk) * kDTW],
+                                             Tab::load(ctab + (cbase + (row0 + kk) * d.s)));
                     }
-                } else {
-                    const int ca0 = R.c0 + lane, cb0 = R.c0 + 32 + lane;
-                    const bool oka = ca0 < R.c1, okb = cb0 < R.c1;
-                    for (int row = R.r0; row < R.r1; ++row) {
-                        if (oka) cmac<Tab::kReal>(p0, gt[pbase + row * kDTW + ca0], Tab::load(ctab + (q.w + row * s + ca0)));
-                        if (okb) cmac<Tab::kReal>(p1, gt[pbase + row * kDTW + cb0], Tab::load(ctab + (q.w + row * s + cb0)));
+                } else if (h > 0) {
+                    const bool oka = lane < w, okb = lane + 32 < w;
+                    for (int row = 0; row < h; ++row) {
+                        if (oka) cmac<Tab::kReal>(p0, gt[d.p0 + row * kDTW + lane], Tab::load(ctab + (d.c0 + row * d.s + lane)));
+                        if (okb)
+                            cmac<Tab::kReal>(p1, gt[d.p0 + row * kDTW + lane + 32],
+                                             Tab::load(ctab + (d.c0 + row * d.s + lane + 32)));
                     }
                 }
                 float2 v = make_float2(p0.x + p1.x, p0.y + p1.y);
@@ -268,11 +283,7 @@ dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int* __re
                     v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
                     v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
                 }
-                if (lane == 0) {
-                    const int sx0 = fx / kDTW, sx1 = (fx + s - 1) / kDTW, sy0 = fy / kDTH;
-                    const int slot = (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0);
-                    slots[(unsigned long long)(u32(q.x)) * max_tiles + slot] = v;
-                }
+                if (lane == 0) slots[rslot[j]] = v;  // an empty overlap writes its empty slot
             }
         }
     }
@@ -288,7 +299,7 @@ int resident(const void* kernel, int threads, size_t smem)
     return per_sm * sms;
 }
 
-constexpr size_t kGridSmem = size_t(kGWarps) * kDPts * sizeof(float2) + size_t(kGThreads) * (sizeof(float4) + sizeof(int2));
+constexpr size_t kGridSmem = size_t(kGWarps) * kDPts * sizeof(float2) + size_t(kGThreads) * (sizeof(DenseRec) + sizeof(float2));
 
 GridArgs dense_args(const tcv_plan* p, int grp, float c_scale, float2* grid)
 {
