@@ -3,21 +3,25 @@
 //
 // The output-stationary tile kernels (tcv_device.cuh) give every lane a fixed grid column and
 // make all eight warps test every sample of the tile; with a 9-wide footprint a warp then works
-// with 9 of its 32 lanes and most warps only test and skip.  Here each sample of a work unit is
-// handled by one warp (sample j by warp j mod kWarps), whose lanes cover the intersection of the
-// footprint with the 64 x 32 tile densely: a rectangle w x h is walked as floor(32 / w) rows of w
-// lanes per step (w <= 32) or as 32-column strips (w > 32).
+// with 9 of its 32 lanes and most warps only test and skip.  Here each sample is handled by one
+// warp per region of the tile it meets, whose lanes cover the intersection densely: a w-wide
+// rectangle is walked floor(32 / w) rows of w lanes per step (w <= 32) or in 32-column strips.
+// The staging thread of each sample prepares its rectangle once (tile coordinates, table index
+// of its first element, rows per step), so a warp only walks it.
 //
-// Gridding accumulates into a warp-private copy of the tile in shared memory (no two warps write
-// one copy, so no atomics); at the end of the unit the copies are added in warp order into the
-// grid, or into the unit's partial tile for a split cell (fold_kernel then adds those in unit
-// order, as for the tile kernels).  Degridding stages the grid tile in shared memory once per unit
-// and reduces each sample's products across its warp into the sample's slot for the tile
-// (slot_reduce_kernel adds the slots in tile order).  Every sum is taken in a fixed order, so
-// results are deterministic; they group the reference's per-point sums differently (by warp),
-// which moves them by FP32 rounding only.
+// Gridding: each 32-column half of the 64 x 32 tile has four warps with private copies of the
+// half in shared memory (8 KB each, no two warps write one copy: no atomics); sample j is added by
+// warp j mod 4 of each half it meets.  A warp keeps the next sample's first table loads in flight
+// while it updates its copy with the current one (a two-stage software pipeline).  At the end of
+// the unit the copies are added in warp order into the grid, or into the unit's partial tile for
+// a split cell (fold_kernel then adds those in unit order, as for the tile kernels).
+// Degridding: the grid tile is staged in shared memory once per unit; sample j is taken by warp
+// j mod 8, which reduces its products across the warp into the sample's slot for the tile
+// (slot_reduce_kernel adds the slots in tile order).
 //
-// Tiles are the plans' 64 x 32 tiles (tile rows 8), so the plans are those of the tile kernels.
+// Every sum is taken in a fixed order, so results are deterministic; they group the reference's
+// per-point sums differently (by warp), which moves them by FP32 rounding only.  Tiles are the
+// plans' 64 x 32 tiles (tile rows 8), so the plans are those of the tile kernels.
 #include "tcv_internal.cuh"
 
 namespace tcv {
@@ -26,7 +30,7 @@ namespace {
 constexpr int kDTW = kTileW;              // 64 columns
 constexpr int kDTH = 32;                  // rows (tile_height(8))
 constexpr int kDPts = kDTW * kDTH;        // 2048 points
-constexpr int kGWarps = 4;                // gridding: warps per CTA (private tile copies)
+constexpr int kGWarps = 8;                // gridding: warps per CTA, four per 32-column half
 constexpr int kGThreads = kGWarps * 32;
 constexpr int kDWarps = 8;                // degridding: warps per CTA
 constexpr int kDThreads = kDWarps * 32;
@@ -90,6 +94,32 @@ __device__ __forceinline__ DenseRec prepare(int coffk, int s, int fx, int fy, in
     return d;
 }
 
+// A staged sample for gridding: its rectangle in tile coordinates (first column and row, width,
+// height) and the table index of the rectangle's first element.  Each warp clips it to its half.
+struct GridRec {
+    int c0;     // table index of the rectangle's first element
+    int s;      // table row stride
+    int shape;  // first tile column | first tile row << 8 | w << 16 | h << 24 (h = 0: no overlap)
+};
+
+__device__ __forceinline__ GridRec prepare_grid(int coffk, int s, int fx, int fy, int tx0, int ty0)
+{
+    const Rect R = clip(fx, fy, s, tx0, ty0);
+    const int w = R.c1 - R.c0, h = R.r1 - R.r0;
+    GridRec g;
+    g.s = s;
+    if (w <= 0 || h <= 0) {  // no overlap (a binned sample always has one)
+        g.c0 = 0;
+        g.shape = 0;
+        return g;
+    }
+    g.c0 = coffk + R.r0 * s + R.c0;
+    g.shape = (fx + R.c0 - tx0) | ((fy + R.r0 - ty0) << 8) | (w << 16) | (h << 24);
+    return g;
+}
+
+// Gridding: the tile's two 32-column halves each have kGWarps / 2 warps; sample j goes to warp
+// j mod (kGWarps / 2) of each half it meets, which adds it into its private copy of that half.
 template <class Tab>
 __global__ void __launch_bounds__(kGThreads)
 dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
@@ -97,16 +127,19 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
                   const u32* __restrict__ order, const uint4* __restrict__ units,
                   const u32* __restrict__ group_ustart, GridArgs a)
 {
+    constexpr int kHalf = kDTW / 2;            // 32 columns
+    constexpr int kHPts = kHalf * kDTH;        // 1024 points per half
+    constexpr int kPerHalf = kGWarps / 2;      // warps per half
     extern __shared__ float2 dsm[];
-    float2* acc_all = dsm;                                                // [kGWarps][kDPts]
-    DenseRec* rec = reinterpret_cast<DenseRec*>(dsm + kGWarps * kDPts);  // [kGThreads]
-    float2* rdv = reinterpret_cast<float2*>(rec + kGThreads);             // scaled data
+    float2* acc_all = dsm;                                               // [kGWarps][kHPts]
+    GridRec* rec = reinterpret_cast<GridRec*>(dsm + kGWarps * kHPts);   // [kGThreads]
+    float2* rdv = reinterpret_cast<float2*>(rec + kGThreads);            // scaled data
     __shared__ DenseLut L;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int half = warp / kPerHalf, sub = warp % kPerHalf, hx0 = half * kHalf;
     build_lut(L, threadIdx.x, kGThreads);
-    float2* acc = acc_all + warp * kDPts;
-    for (int i = lane; i < kDPts; i += 32) acc[i] = make_float2(0.f, 0.f);
-    __syncthreads();  // the lane table is complete
+    float2* acc = acc_all + warp * kHPts;
+    for (int i = lane; i < kHPts; i += 32) acc[i] = make_float2(0.f, 0.f);
     const u32 i1 = group_ustart[a.group + 1];
     for (u32 it = group_ustart[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
         const uint4 u = units[it];
@@ -115,91 +148,111 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
         const int tx0 = rec_tx(ti) * kDTW, ty0 = rec_ty(ti) * kDTH;
         for (u32 base = 0; base < cnt; base += kGThreads) {
             const int m = int(cnt - base < u32(kGThreads) ? cnt - base : u32(kGThreads));
-            __syncthreads();  // the previous chunk's records are consumed
+            __syncthreads();  // the previous chunk's records are consumed (and the lane table built)
             if (int(threadIdx.x) < m) {
                 const u32 k = order[start + base + threadIdx.x];
                 const float2 d = data[k];
                 const int sk = int(a.ssz[k]);
-                rec[threadIdx.x] = prepare(coff[k], sk, iu[k] - sk / 2, iv[k], tx0, ty0, L);
+                rec[threadIdx.x] = prepare_grid(coff[k], sk, iu[k] - sk / 2, iv[k], tx0, ty0);
                 rdv[threadIdx.x] = make_float2(d.x * a.c_scale, d.y * a.c_scale);
             }
             __syncthreads();
-            // U steps per iteration: every table load of the iteration is issued before any update
-            // of the warp's tile copy (memory in flight at 12 warps per SM)
+            // Software pipeline over this warp's samples: the next sample's first U steps of table
+            // loads are in flight while the current sample updates the copy.
             constexpr int U = 4;
-            for (int j = warp; j < m; j += kGWarps) {
-                const DenseRec d = rec[j];
-                const float2 dv = rdv[j];
-                const int w = d.shape & 255, h = (d.shape >> 8) & 255, kk = d.shape >> 16;
-                if (h == 0) continue;  // warp-uniform
-                if (w <= 32) {
-                    const int qq = L.q[w][lane], rr = L.r[w][lane];
-                    const bool lane_ok = qq < kk;
-                    const int cbase = d.c0 + qq * d.s + rr, pbase = d.p0 + qq * kDTW + rr;
-                    for (int row0 = 0; row0 < h; row0 += U * kk) {
-                        float2 cv[U];
-                        bool ok[U];
+            struct Job {
+                int h, hf, kk, s, cbase, pbase;  // h: rows from the lane's first; hf: the rectangle's
+                bool lane_ok;
+                float2 dv;
+            };
+            // the next sample from index j on that meets this half; false when there is none
+            auto setup = [&](int& j, Job& jb) -> bool {
+                for (; j < m; j += kPerHalf) {
+                    const GridRec g = rec[j];
+                    const int tc = g.shape & 255, tr = (g.shape >> 8) & 255, w = (g.shape >> 16) & 255,
+                              h = g.shape >> 24;
+                    const int lo = max(tc, hx0), hi = min(tc + w, hx0 + kHalf);
+                    if (h == 0 || lo >= hi) continue;  // warp-uniform
+                    const int wc = hi - lo;
+                    jb.kk = L.k[wc];
+                    const int qq = L.q[wc][lane], rr = L.r[wc][lane];
+                    jb.lane_ok = qq < jb.kk;
+                    jb.h = h - qq;  // rows left for this lane, from its first
+                    jb.hf = h;
+                    jb.s = g.s;
+                    jb.cbase = g.c0 + (lo - tc) + qq * g.s + rr;
+                    jb.pbase = (tr + qq) * kHalf + (lo - hx0) + rr;
+                    jb.dv = rdv[j];
+                    return true;
+                }
+                return false;
+            };
+            auto load = [&](const Job& jb, int row0, float2 (&cv)[U]) {
 #pragma unroll
-                        for (int e = 0; e < U; ++e) {
-                            const int ro = row0 + e * kk;  // this step's first row; the lane's is ro + qq
-                            ok[e] = lane_ok && ro + qq < h;
-                            cv[e] = ok[e] ? Tab::load(ctab + (cbase + ro * d.s)) : make_float2(0.f, 0.f);
-                        }
+                for (int e = 0; e < U; ++e) {
+                    const int ro = row0 + e * jb.kk;
+                    cv[e] = (jb.lane_ok && ro < jb.h) ? Tab::load(ctab + (jb.cbase + ro * jb.s)) : make_float2(0.f, 0.f);
+                }
+            };
+            auto apply = [&](const Job& jb, int row0, const float2 (&cv)[U]) {
 #pragma unroll
-                        for (int e = 0; e < U; ++e) {
-                            if (ok[e]) {
-                                float2& g = acc[pbase + (row0 + e * kk) * kDTW];
-                                float2 t = g;
-                                cmac<Tab::kReal>(t, dv, cv[e]);
-                                g = t;
-                            }
-                        }
-                    }
-                } else {
-                    const bool oka = lane < w, okb = lane + 32 < w;
-                    for (int row0 = 0; row0 < h; row0 += U / 2) {
-                        float2 cv[U];
-                        bool ok[U];
-#pragma unroll
-                        for (int e = 0; e < U; ++e) {
-                            const int row = row0 + e / 2;
-                            ok[e] = row < h && ((e & 1) ? okb : oka);
-                            cv[e] = ok[e] ? Tab::load(ctab + (d.c0 + row * d.s + lane + (e & 1) * 32))
-                                          : make_float2(0.f, 0.f);
-                        }
-#pragma unroll
-                        for (int e = 0; e < U; ++e) {
-                            if (ok[e]) {
-                                float2& g = acc[d.p0 + (row0 + e / 2) * kDTW + lane + (e & 1) * 32];
-                                float2 t = g;
-                                cmac<Tab::kReal>(t, dv, cv[e]);
-                                g = t;
-                            }
-                        }
+                for (int e = 0; e < U; ++e) {
+                    const int ro = row0 + e * jb.kk;
+                    if (jb.lane_ok && ro < jb.h) {
+                        float2& gp = acc[jb.pbase + ro * kHalf];
+                        float2 t = gp;
+                        cmac<Tab::kReal>(t, jb.dv, cv[e]);
+                        gp = t;
                     }
                 }
+            };
+            int j = sub;
+            Job cur;
+            float2 cvc[U];
+            bool have = setup(j, cur);
+            if (have) load(cur, 0, cvc);
+            while (have) {
+                int jn = j + kPerHalf;
+                Job nxt;
+                float2 cvn[U];
+                const bool more = setup(jn, nxt);
+                if (more) load(nxt, 0, cvn);  // in flight during the updates below
+                apply(cur, 0, cvc);
+                for (int row0 = U * cur.kk; row0 < cur.hf; row0 += U * cur.kk) {  // tall rectangles (warp-uniform)
+                    float2 cv[U];
+                    load(cur, row0, cv);
+                    apply(cur, row0, cv);
+                }
                 __syncwarp();  // this sample's updates land before another lane reads them for the next
+                if (!more) break;
+                cur = nxt;
+                j = jn;
+#pragma unroll
+                for (int e = 0; e < U; ++e) cvc[e] = cvn[e];
             }
         }
         __syncthreads();  // every warp's copy is complete
-        // the copies in warp order, into the grid (a whole cell) or the unit's partial tile
+        // each half's copies in warp order, into the grid (a whole cell) or the unit's partial tile
         const JobDesc& jd = a.jobs[rec_job(ti)];
         const int gs = jd.g_size;
         float2* grid = a.grid ? a.grid : jd.grid;
         for (int p = threadIdx.x; p < kDPts; p += kGThreads) {
-            float2 v = acc_all[p];
+            const int px = p % kDTW, py = p / kDTW;
+            const int hh = px / kHalf, hp = py * kHalf + (px % kHalf);
+            float2* c = acc_all + hh * kPerHalf * kHPts + hp;
+            float2 v = c[0];
 #pragma unroll
-            for (int w = 1; w < kGWarps; ++w) {
-                const float2 o = acc_all[w * kDPts + p];
+            for (int w = 1; w < kPerHalf; ++w) {
+                const float2 o = c[w * kHPts];
                 v.x += o.x;
                 v.y += o.y;
             }
 #pragma unroll
-            for (int w = 0; w < kGWarps; ++w) acc_all[w * kDPts + p] = make_float2(0.f, 0.f);
+            for (int w = 0; w < kPerHalf; ++w) c[w * kHPts] = make_float2(0.f, 0.f);
             if (pslot != kDirect) {
                 a.partial[(unsigned long long)(pslot) * kDPts + p] = v;
             } else {
-                const int gx = tx0 + (p % kDTW), gy = ty0 + (p / kDTW);
+                const int gx = tx0 + px, gy = ty0 + py;
                 if (gx < gs && gy < gs) {
                     float2* gp = grid + ((unsigned long long)(gy) * gs + gx);
                     float2 o = *gp;
@@ -299,7 +352,7 @@ int resident(const void* kernel, int threads, size_t smem)
     return per_sm * sms;
 }
 
-constexpr size_t kGridSmem = size_t(kGWarps) * kDPts * sizeof(float2) + size_t(kGThreads) * (sizeof(DenseRec) + sizeof(float2));
+constexpr size_t kGridSmem = size_t(kGWarps) * (kDPts / 2) * sizeof(float2) + size_t(kGThreads) * (sizeof(GridRec) + sizeof(float2));
 
 GridArgs dense_args(const tcv_plan* p, int grp, float c_scale, float2* grid)
 {
