@@ -684,14 +684,16 @@ tcv_status tcv_cur_tune(tcv_cur_ctx* c, int reps, tcv_tuning* best_out, float* b
         return TCV_OK;
     };
     // stage 1: kernel families and tile height x plane-group slice (slices that give the same
-    // grouping timed once).  Variants: 64 x 64 and 64 x 32 tile kernels; on 64 x 32 tiles the
-    // sample-parallel degridding, and both passes sample-parallel (kernel bits 2 and 3).
+    // grouping timed once), with typical work units (256 gridding, 128 degridding samples: these
+    // problems' busy cells need them, and the families rank differently without).  Variants:
+    // 64 x 64 and 64 x 32 tile kernels; on 64 x 32 tiles the sample-parallel degridding, and both
+    // passes sample-parallel (kernel bits 2 and 3).
     if (s == TCV_OK) {
         std::vector<std::pair<int, int>> seen;  // (variant, number of plane groups)
         for (int variant : {16, 8, -2, -3})
             for (int mib : {32, 128, -1}) {
                 const int rows = variant < 0 ? 8 : variant;
-                const tcv_tuning t{rows, mib, 0, 0, variant < 0 ? -variant : 0};
+                const tcv_tuning t{rows, mib, 256, 128, variant < 0 ? -variant : 0};
                 int groups = 1;
                 const int64_t budget = mib > 0 ? (int64_t(mib) << 20) : INT64_MAX;
                 int64_t used = 0;
@@ -712,12 +714,14 @@ tcv_status tcv_cur_tune(tcv_cur_ctx* c, int reps, tcv_tuning* best_out, float* b
     }
     if (s == TCV_OK) {  // stage 2: gridding work units
         const tcv_tuning base = best;
-        for (int split : {256, 128, 64})  // the partial-tile bound grows as 1 / split
-            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, split, 0, base.kernel})) != TCV_OK) break;
+        for (int split : {512, 128, 64})  // the partial-tile bound grows as 1 / split
+            if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, split, base.degrid_split, base.kernel})) !=
+                TCV_OK)
+                break;
     }
     if (s == TCV_OK) {  // stage 3: degridding work units
         const tcv_tuning base = best;
-        for (int split : {128, 64, 32, 16})
+        for (int split : {256, 64, 32, 16})
             if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, base.split, split, base.kernel})) != TCV_OK)
                 break;
     }

@@ -524,8 +524,8 @@ tcv_status tcv_cur_set_ctype(tcv_cur_ctx *ctx, int c_type);
 tcv_status tcv_cur_set_tuning(tcv_cur_ctx *ctx, const tcv_tuning *tuning);
 /* Time one gridding and one degridding pass of the initialised problem per candidate tuning
  * (median of reps, into scratch buffers: the context's grid and samples are left untouched) and
- * keep the fastest: tile height x plane groups, then gridding work units, then degridding work
- * units.  The candidates and their times are readable with tcv_autotune_report.  Set-up path:
+ * keep the fastest: kernel family x tile height x plane groups (with 256 / 128-sample work
+ * units), then gridding work units, then degridding work units.  The candidates and their times are readable with tcv_autotune_report.  Set-up path:
  * allocates and synchronises. */
 tcv_status tcv_cur_tune(tcv_cur_ctx *ctx, int reps, tcv_tuning *best_out, float *best_ms_out);
 tcv_status tcv_cur_init(tcv_cur_ctx *ctx);       /* Benchmark::init */
