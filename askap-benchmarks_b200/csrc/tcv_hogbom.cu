@@ -177,57 +177,62 @@ __device__ __forceinline__ unsigned long long iter_body(const HogArgs& a, unsign
         }
     };
     if (kVec) {
-        // whole rows per block; per row every thread loads its float4s (up to U) before any store
+        // whole rows per block, walked as items (row, column chunk of 256 float4) in index order;
+        // every thread loads the float4s of U items (of one or several rows) before any store
         constexpr int U = 4;
         const int rows_per = (W + a.nblocks - 1) / a.nblocks;
         const int r0 = int(blockIdx.x) * rows_per, r1 = min(W, r0 + rows_per);
-        for (int y = r0; y < r1; ++y) {
-            const int prow = y - diffy;
-            const bool row_in = y >= starty && y <= stopy;
-            const bool prow_ok = prow >= 0 && prow < P;
-            const bool row_sub = row_in && prow_ok;
-            if (row_in && !prow_ok && threadIdx.x == 0) ++skipped;
-            float* rrow = a.residual + (long long)y * W;
-            const long long pbase = (long long)prow * P - diffx;  // + x: inside the PSF row for x in range
-            const unsigned int ibase = unsigned(y) * unsigned(W);
-            for (int xb = 4 * int(threadIdx.x); xb < W; xb += 4 * kHogThreads * U) {
-                float4 r[U];
-                float pv[U][4];
-                bool sub[U];
+        const int nch = (W / 4 + kHogThreads - 1) / kHogThreads;  // chunks per row
+        if (threadIdx.x == 0)
+            for (int y = r0; y < r1; ++y)
+                if (y >= starty && y <= stopy && !(y - diffy >= 0 && y - diffy < P)) ++skipped;
+        int y = r0, c = 0;
+        while (y < r1) {
+            float4 r[U];
+            float pv[U][4];
+            bool sub[U], val[U];
+            int xs[U], ys[U];
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int x0 = xb + 4 * kHogThreads * u;
-                    sub[u] = false;
-                    r[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (x0 < W) {
-                        r[u] = __ldcg(reinterpret_cast<const float4*>(rrow + x0));
-                        sub[u] = row_sub && x0 + 3 >= startx && x0 <= stopx;
+            for (int u = 0; u < U; ++u) {
+                ys[u] = y;
+                xs[u] = 4 * (int(threadIdx.x) + kHogThreads * c);
+                val[u] = y < r1 && xs[u] < W;
+                if (++c == nch) {
+                    c = 0;
+                    ++y;
+                }
+                sub[u] = false;
+                r[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (val[u]) {
+                    r[u] = __ldcg(reinterpret_cast<const float4*>(a.residual + ((long long)ys[u] * W + xs[u])));
+                    const int prow = ys[u] - diffy;
+                    sub[u] = ys[u] >= starty && ys[u] <= stopy && prow >= 0 && prow < P && xs[u] + 3 >= startx &&
+                             xs[u] <= stopx;
+                    const long long pbase = (long long)prow * P - diffx;  // + x: inside the PSF row for x in range
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int x = x0 + j;
-                            pv[u][j] = (sub[u] && x >= startx && x <= stopx) ? __ldg(a.psf + (pbase + x)) : 0.f;
-                        }
+                    for (int j = 0; j < 4; ++j) {
+                        const int x = xs[u] + j;
+                        pv[u][j] = (sub[u] && x >= startx && x <= stopx) ? __ldg(a.psf + (pbase + x)) : 0.f;
                     }
                 }
+            }
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int x0 = xb + 4 * kHogThreads * u;
-                    if (x0 >= W) continue;
-                    if (sub[u]) {
-                        float* rv = reinterpret_cast<float*>(&r[u]);
+            for (int u = 0; u < U; ++u) {
+                if (!val[u]) continue;
+                if (sub[u]) {
+                    float* rv = reinterpret_cast<float*>(&r[u]);
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const int x = x0 + j;
-                            if (x >= startx && x <= stopx) rv[j] = __fsub_rn(rv[j], __fmul_rn(t, pv[u][j]));
-                        }
-                        __stcg(reinterpret_cast<float4*>(rrow + x0), r[u]);
+                    for (int j = 0; j < 4; ++j) {
+                        const int x = xs[u] + j;
+                        if (x >= startx && x <= stopx) rv[j] = __fsub_rn(rv[j], __fmul_rn(t, pv[u][j]));
                     }
-                    const unsigned int i0 = ibase + unsigned(x0);
-                    track(r[u].x, i0);
-                    track(r[u].y, i0 + 1);
-                    track(r[u].z, i0 + 2);
-                    track(r[u].w, i0 + 3);
+                    __stcg(reinterpret_cast<float4*>(a.residual + ((long long)ys[u] * W + xs[u])), r[u]);
                 }
+                const unsigned int i0 = unsigned(ys[u]) * unsigned(W) + unsigned(xs[u]);
+                track(r[u].x, i0);
+                track(r[u].y, i0 + 1);
+                track(r[u].z, i0 + 2);
+                track(r[u].w, i0 + 3);
             }
         }
     } else {
@@ -301,7 +306,7 @@ __device__ __forceinline__ unsigned long long global_ns()
 // generation; the others wait for it, bounded by an iteration count and 2 s of %globaltimer, after
 // which they flag the error and return (the host reports TCV_ERR_TIMEOUT).
 template <bool kVec>
-__global__ void __launch_bounds__(kHogThreads, 4) hog_persist_kernel(HogArgs a, int niters)
+__global__ void __launch_bounds__(kHogThreads, 2) hog_persist_kernel(HogArgs a, int niters)
 {
     HogState* st = a.state;
     const unsigned int psf_pos = st->psf_pos;
