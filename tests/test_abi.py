@@ -228,3 +228,66 @@ def test_current_geometry_matches_oracle(tcv, orc):
     # current/tConvolveMPI/Benchmark.cc:697-739 evaluated by hand
     assert rates[0] == np.float32(10 * 5443200 * 10 * 3 * 3 * 400 / 5250.0)
     assert rates[1] == np.float32(10 * 3758400 * 4 * 3 * 78 * 100 / 5500.0)
+
+
+def test_hogbom_fft_major_argument_validation(tcv):
+    """The minor-cycle, FFT and major-cycle entry points refuse bad arguments before any device
+    use (so these run without a GPU)."""
+    from tconvolve._lib import TcvMajorConfig, lib
+
+    L = lib()
+    P = ctypes.c_void_p
+    fake = P(0x1000)  # never dereferenced: every call below fails its argument checks first
+    f = ctypes.c_float
+    # Hogbom: null images, bad widths, negative iterations, too small a workspace
+    assert L.tcv_hogbom_workspace_bytes(0) == 0 and L.tcv_hogbom_workspace_bytes(4096) > 0
+    assert L.tcv_hogbom_deconvolve(None, 64, fake, 64, fake, fake, 10, f(0.1), f(0.0), None, None, fake, 1 << 20,
+                                   None) == 1
+    assert L.tcv_hogbom_deconvolve(fake, 0, fake, 64, fake, fake, 10, f(0.1), f(0.0), None, None, fake, 1 << 20,
+                                   None) == 1
+    assert L.tcv_hogbom_deconvolve(fake, 64, fake, 64, fake, fake, -1, f(0.1), f(0.0), None, None, fake, 1 << 20,
+                                   None) == 1
+    assert L.tcv_hogbom_deconvolve(fake, 70000, fake, 64, fake, fake, 10, f(0.1), f(0.0), None, None, fake,
+                                   1 << 20, None) == 8  # width^2 beyond 32-bit indices
+    assert L.tcv_hogbom_deconvolve(fake, 64, fake, 64, fake, fake, 10, f(0.1), f(0.0), None, None, fake, 16,
+                                   None) == 7  # workspace
+    assert L.tcv_find_peak(None, 10, None, None, fake, 1 << 20, None) == 1
+    # FFT steps: null grids, odd sizes (refused as the reference refuses them)
+    assert L.tcv_fft_exec(None, 64, 1, None) == 1
+    assert L.tcv_fft_exec(fake, 63, 1, None) == 8
+    assert L.tcv_image_from_grid(fake, 63, f(1.0), fake, None) == 8
+    assert L.tcv_grid_from_image(fake, 63, fake, None) == 8
+    assert L.tcv_fft_fix(None, 10, f(1.0), None) == 1
+    # major cycle: bad configurations
+    cfg = TcvMajorConfig()
+    L.tcv_major_config_default(ctypes.byref(cfg))
+    assert (cfg.n_samples, cfg.w_size, cfg.g_size, cfg.n_major, cfg.n_minor, cfg.n_sources) == (160000, 33, 4096, 5,
+                                                                                              100, 100)
+    ctx = P()
+    bad = TcvMajorConfig.from_buffer_copy(cfg)
+    bad.g_size = 4095
+    assert L.tcv_major_create(ctypes.byref(bad), ctypes.byref(ctx)) == 8
+    bad = TcvMajorConfig.from_buffer_copy(cfg)
+    bad.n_samples = 0
+    assert L.tcv_major_create(ctypes.byref(bad), ctypes.byref(ctx)) == 1
+    assert L.tcv_major_create(None, ctypes.byref(ctx)) == 1
+
+
+def test_tuning_kernel_field_validation(tcv):
+    """The sample-parallel kernels (tuning.kernel bits) need 8-row tiles; a plan workspace query
+    with another tile height, or an unknown bit, is refused (0 bytes)."""
+    import numpy as np
+
+    from tconvolve._lib import TcvTuning, lib
+
+    L = lib()
+    s = np.array([7, 9, 11], np.int32)
+    off0 = np.array([0, 49 * 64, (49 + 81) * 64], np.int32)
+    c_len = int((49 + 81 + 121) * 64)
+    args = (1000, s.ctypes.data_as(ctypes.c_void_p), off0.ctypes.data_as(ctypes.c_void_p), 3, 512, c_len)
+    assert L.tcv_plan_workspace_bytes_var(*args, ctypes.byref(TcvTuning(8, 32, 0, 0, 3))) > 0
+    assert L.tcv_plan_workspace_bytes_var(*args, ctypes.byref(TcvTuning(8, 32, 0, 0, 2))) > 0
+    assert L.tcv_plan_workspace_bytes_var(*args, ctypes.byref(TcvTuning(16, 32, 0, 0, 1))) == 0
+    assert L.tcv_plan_workspace_bytes_var(*args, ctypes.byref(TcvTuning(8, 32, 0, 0, 4))) == 0
+    assert TcvTuning(8, 32, 0, 0, 3).as_tuple() == (8, 32, 0, 0, 3)
+    assert TcvTuning(8, 32, 0, 0, 0).as_tuple() == (8, 32, 0, 0)
