@@ -250,3 +250,41 @@ def test_current_autotune(tcv, orc, cuda_ok):
     assert {t[0] for t, _ in report} == {8, 16}
     _check_tuned(b, orc)
     b.close()
+
+
+def _reference_check(a: np.ndarray, b: np.ndarray):
+    """runGridCheck / runDegridCheck (current/tConvolveACC/Benchmark.cc:324-364): every point's
+    |a - b| / |a| <= 1e-4 (a point where a == 0 must be 0 in b too: the quotient is inf otherwise,
+    and 0/0 passes as the reference's NaN comparison does), and the null test: both sums of
+    absolute values positive.  Returns (passed, worst relative error over a != 0)."""
+    a64, b64 = a.astype(np.complex128), b.astype(np.complex128)
+    d = np.abs(a64 - b64)
+    nz = np.abs(a64) > 0
+    if np.any(~nz & (d > 0)):
+        return False, np.inf
+    rel = d[nz] / np.abs(a64[nz])
+    worst = float(rel.max()) if rel.size else 0.0
+    return worst <= 1e-4 and np.abs(a64).sum() > 0 and np.abs(b64).sum() > 0, worst
+
+
+@pytest.mark.parametrize("tuning", [None, (32, 512, 256, 8, 3)], ids=["default", "sample-parallel"])
+def test_current_reference_point_checks(tcv, orc, cuda_ok, tuning):
+    """The reference's own GPU-port check on the spectral-line run: grid and degridded samples
+    against the CPU result (the oracle, pinned to the reference), point by point."""
+    from tconvolve.current import Benchmark
+
+    b = Benchmark()
+    b.setRunType(1)
+    if tuning:
+        b.set_tuning(*tuning)
+    b.init()
+    b.runGrid()
+    b.runDegrid()
+    b.sync()
+    iu, iv, wp, co = b.offsets()
+    _, grid_ref, out_ref = _oracle_run(orc, 1, iu, iv, wp, co)
+    ok_g, worst_g = _reference_check(grid_ref, b.grid())
+    ok_d, worst_d = _reference_check(out_ref, b.outdata())
+    print(f"\nper-point relative error: grid {worst_g:.2e}, degridded {worst_d:.2e}")
+    assert ok_g and ok_d, (worst_g, worst_d)
+    b.close()
