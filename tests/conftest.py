@@ -22,7 +22,7 @@ for p in (REPO, PKG):
 GOLDEN_DIR = os.path.join(REPO, "tests", "golden")
 VIS_SEED = 1234
 
-# relative L2 bound for the plain FP32 form against the reference output (north-star parity bar)
+# relative L2 bound for the plain FP32 form against the reference output (the parity bar of the path)
 REL_L2_FP32 = 1e-5
 
 

@@ -5,7 +5,7 @@ Bars (written here, used below):
   * table C: bit-exact expected; at most 1 in 2^20 entries may differ, by at most 1 ulp
     (the FP64 cos/exp of CUDA and glibc may round a value differently near a float boundary);
   * grid and degridded samples, plain FP32 form: relative L2 <= 1e-5 against the reference
-    (REL_L2_FP32), the north-star bar; the measured error is ~1e-7 (FP32 summation order).
+    (REL_L2_FP32), the parity bar of the path; the measured error is ~1e-7 (FP32 summation order).
 """
 from __future__ import annotations
 

@@ -6,7 +6,7 @@ Run with -s to print the tables (the figures quoted in the design notes come fro
     python -m pytest tests/test_precision.py -m gpu -s
 
 Bars (relative L2 against the FP64 oracle, written here, used below):
-  * plain forms (c64, r32): <= 1e-5, the north-star bar (measured ~5e-7: FP32 summation);
+  * plain forms (c64, r32): <= 1e-5, the parity bar of the path (measured ~5e-7: FP32 summation);
   * float16 forms (cf16, rf16, power-of-two scaled): <= 8e-4;
   * bfloat16 forms (cbf16, rbf16): <= 6e-3;
   * the same bounds for the bf16 form run batched on the 129^2-footprint table.
