@@ -159,12 +159,15 @@ def test_current_wide_kernels_subset(tcv, orc, cur_golden, cuda_ok):
     b.close()
 
 
+@pytest.mark.parametrize("tuning", [None, (32, 512, 256, 8, 3)], ids=["tile", "sample-parallel"])
 @pytest.mark.parametrize("form,bound", [("cbf16", 6e-3), ("cf16", 8e-4)])
-def test_current_reduced_forms(tcv, orc, cuda_ok, form, bound):
+def test_current_reduced_forms(tcv, orc, cuda_ok, form, bound, tuning):
     from tconvolve.current import Benchmark
 
     b = Benchmark()
     b.setRunType(1)
+    if tuning:
+        b.set_tuning(*tuning)
     b.init()
     iu, iv, wp, co = b.offsets()
     rng = np.random.default_rng(11)
