@@ -35,12 +35,12 @@ constexpr int kHogMaxBlocks = 592;  // 4 x 148: one wave of four 256-thread CTAs
 struct HogState {
     unsigned long long win_key[3];  // winners: [0], [1] by iteration parity, [2] the PSF's
     float win_val[3];
-    unsigned int arrived;           // blocks finished in the current launch
+    unsigned int arrived;           // blocks finished in the current launch (persistent loop: in all
+                                    // iterations so far)
     int stopped;                    // 1 + the iteration whose |peak| fell below the threshold; 0 = running
     int done;                       // iterations carried out
     unsigned int psf_pos;           // PSF peak index
     unsigned long long skipped_rows;  // PSF rows outside the PSF (reference out-of-bounds reads)
-    unsigned int gen;                 // persistent kernel: barrier generation
     int error;                        // persistent kernel: a barrier wait gave up
 };
 
@@ -50,6 +50,8 @@ struct HogArgs {
     float* model;
     unsigned long long* keys;  // one candidate per block
     float* vals;
+    unsigned long long* keys2;  // persistent loop: the candidates of odd iterations
+    float* vals2;
     HogState* state;
     float* hist_val;         // per iteration: peak value (may be null)
     unsigned int* hist_pos;  // per iteration: peak index (may be null)
@@ -301,22 +303,24 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
-// All iterations in one cooperative launch (every CTA resident): per iteration each CTA leaves its
-// candidate; the last to arrive reduces them, publishes the winner and advances the barrier
-// generation; the others wait for it, bounded by an iteration count and 2 s of %globaltimer, after
-// which they flag the error and return (the host reports TCV_ERR_TIMEOUT).
+// All iterations in one cooperative launch (every CTA resident).  Per iteration each CTA leaves its
+// candidate in the buffer of the iteration's parity and adds one to a monotonic arrival count;
+// once the count reaches the iteration's target every CTA reads all candidates itself and reduces
+// them in the same order (so every CTA holds the same winner), with no second round trip through a
+// published winner.  Waits are bounded by an iteration count and 2 s of %globaltimer, after which
+// the CTA flags the error and returns (the host reports TCV_ERR_TIMEOUT).  Two candidate buffers
+// suffice: a CTA cannot write iteration it + 1's candidates before every CTA has arrived at barrier
+// it, i.e. has read iteration it - 1's.
 template <bool kVec>
 __global__ void __launch_bounds__(kHogThreads, 2) hog_persist_kernel(HogArgs a, int niters)
 {
     HogState* st = a.state;
     const unsigned int psf_pos = st->psf_pos;
-    __shared__ bool last;
     __shared__ int ok;
+    unsigned int ppos = key_index(__ldcg(&st->win_key[0]));  // the dirty image's scan
+    float peak = __ldcg(&st->win_val[0]);
     for (int it = 0; it < niters; ++it) {
-        const int par = it & 1;
-        const unsigned int ppos = key_index(__ldcg(&st->win_key[par]));
-        const float peak = __ldcg(&st->win_val[par]);
-        if (fabsf(peak) < a.threshold) {  // every CTA reads the same winner: all stop here
+        if (fabsf(peak) < a.threshold) {  // every CTA holds the same winner: all stop here
             if (blockIdx.x == 0 && threadIdx.x == 0) st->stopped = it + 1;
             return;
         }
@@ -329,40 +333,18 @@ __global__ void __launch_bounds__(kHogThreads, 2) hog_persist_kernel(HogArgs a, 
         unsigned long long best = iter_body<kVec>(a, ppos, peak, psf_pos, bv, skipped);
         if (skipped) atomicAdd(&st->skipped_rows, skipped);
         best = block_max(best, bv);
-        // barrier `it`: st->gen counts completed barriers, so it passes once gen > it
+        unsigned long long* keys = (it & 1) ? a.keys2 : a.keys;
+        float* vals = (it & 1) ? a.vals2 : a.vals;
         if (threadIdx.x == 0) {
-            a.keys[blockIdx.x] = best;
-            a.vals[blockIdx.x] = bv;
+            keys[blockIdx.x] = best;
+            vals[blockIdx.x] = bv;
             __threadfence();
-            last = atomicAdd(&st->arrived, 1u) == unsigned(a.nblocks - 1);
-        }
-        __syncthreads();
-        if (last) {
-            __threadfence();
-            unsigned long long k = 0;
-            float v = 0.f;
-            for (int i = threadIdx.x; i < a.nblocks; i += kHogThreads) {
-                const unsigned long long ki = __ldcg(a.keys + i);
-                if (ki > k) {
-                    k = ki;
-                    v = __ldcg(a.vals + i);
-                }
-            }
-            k = block_max(k, v);
-            if (threadIdx.x == 0) {
-                const bool zero = (k >> 32) == 0;
-                st->win_key[par ^ 1] = zero ? static_cast<unsigned long long>(~0u) : k;
-                st->win_val[par ^ 1] = zero ? 0.f : v;
-                st->arrived = 0;
-                __threadfence();
-                atomicExch(&st->gen, unsigned(it + 1));  // release
-                ok = 1;
-            }
-        } else if (threadIdx.x == 0) {
+            atomicAdd(&st->arrived, 1u);
+            const unsigned int target = unsigned(it + 1) * unsigned(a.nblocks);
             ok = 0;
             const unsigned long long t0 = global_ns();
             for (unsigned int spin = 0; spin < (1u << 24); ++spin) {
-                if (*reinterpret_cast<volatile unsigned int*>(&st->gen) > unsigned(it)) {
+                if (*reinterpret_cast<volatile unsigned int*>(&st->arrived) >= target) {
                     ok = 1;
                     break;
                 }
@@ -375,6 +357,20 @@ __global__ void __launch_bounds__(kHogThreads, 2) hog_persist_kernel(HogArgs a, 
         }
         __syncthreads();
         if (!ok) return;
+        // every CTA: the winner of this iteration's candidates, in the same order everywhere
+        unsigned long long k = 0;
+        float v = 0.f;
+        for (int i = threadIdx.x; i < a.nblocks; i += kHogThreads) {
+            const unsigned long long ki = __ldcg(keys + i);
+            if (ki > k) {
+                k = ki;
+                v = __ldcg(vals + i);
+            }
+        }
+        k = block_max(k, v);
+        const bool zero = (k >> 32) == 0;  // an all-zero residual: the reference keeps maxPos = 0, maxVal = 0
+        ppos = zero ? 0u : key_index(k);
+        peak = zero ? 0.f : v;
     }
 }
 
@@ -400,7 +396,7 @@ extern "C" {
 size_t tcv_hogbom_workspace_bytes(int width)
 {
     if (width < 1) return 0;
-    return align256(sizeof(HogState)) + align256(size_t(kHogMaxBlocks) * 8) + align256(size_t(kHogMaxBlocks) * 4);
+    return align256(sizeof(HogState)) + 2 * align256(size_t(kHogMaxBlocks) * 8) + 2 * align256(size_t(kHogMaxBlocks) * 4);
 }
 
 tcv_status tcv_hogbom_deconvolve(const float* d_dirty, int width, const float* d_psf, int psf_width, float* d_model,
@@ -416,8 +412,14 @@ tcv_status tcv_hogbom_deconvolve(const float* d_dirty, int width, const float* d
     char* w = static_cast<char*>(d_work);
     HogArgs a{};
     a.state = reinterpret_cast<HogState*>(w);
-    a.keys = reinterpret_cast<unsigned long long*>(w + align256(sizeof(HogState)));
-    a.vals = reinterpret_cast<float*>(w + align256(sizeof(HogState)) + align256(size_t(kHogMaxBlocks) * 8));
+    {
+        char* q = w + align256(sizeof(HogState));
+        a.keys = reinterpret_cast<unsigned long long*>(q);
+        a.keys2 = reinterpret_cast<unsigned long long*>(q + align256(size_t(kHogMaxBlocks) * 8));
+        q += 2 * align256(size_t(kHogMaxBlocks) * 8);
+        a.vals = reinterpret_cast<float*>(q);
+        a.vals2 = reinterpret_cast<float*>(q + align256(size_t(kHogMaxBlocks) * 4));
+    }
     a.psf = d_psf;
     a.residual = d_residual;
     a.model = d_model;
@@ -453,6 +455,8 @@ tcv_status tcv_hogbom_deconvolve(const float* d_dirty, int width, const float* d
             TCV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hog_persist_kernel<false>, kHogThreads, 0));
         persist = coop && per_sm > 0;
     }
+    // the persistent loop's arrival count reaches niters x CTAs: keep it within 32 bits
+    if (persist && uint64_t(niters) * uint64_t(std::max(1, sms * 2)) >= (1ull << 32)) persist = false;
     if (persist && niters > 0) {
         // two CTAs per SM at most (fewer candidates per barrier), never more than resident
         a.nblocks = std::max(1, std::min({sms * std::min(per_sm, 2), hog_blocks(a.n), width}));
@@ -502,7 +506,7 @@ tcv_status tcv_find_peak(const float* d_image, int64_t n, float* val_out, int64_
     char* w = static_cast<char*>(d_work);
     HogState* state = reinterpret_cast<HogState*>(w);
     unsigned long long* keys = reinterpret_cast<unsigned long long*>(w + align256(sizeof(HogState)));
-    float* vals = reinterpret_cast<float*>(w + align256(sizeof(HogState)) + align256(size_t(kHogMaxBlocks) * 8));
+    float* vals = reinterpret_cast<float*>(w + align256(sizeof(HogState)) + 2 * align256(size_t(kHogMaxBlocks) * 8));
     TCV_CUDA(cudaMemsetAsync(state, 0, sizeof(HogState), st));
     const int nb = hog_blocks(n);
     hog_scan_kernel<<<nb, kHogThreads, 0, st>>>(d_image, nullptr, n, nb, keys, vals, state, 0);
