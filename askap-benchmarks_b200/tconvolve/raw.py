@@ -149,7 +149,8 @@ class VarPlan(Plan):
         self.g_size, self.c_len = g_size, c_len
         s_size = np.ascontiguousarray(s_size, np.int32)
         c_off0 = np.ascontiguousarray(c_off0, np.int32)
-        t = TcvTuning(*(tuple(tuning) + (0, 0, 0, 0))[:4]) if tuning is not None else None
+        # (tile_rows, group_mib, split, degrid_split[, kernel bits]); missing entries are 0 (defaults)
+        t = TcvTuning(*(tuple(tuning) + (0, 0, 0, 0, 0))[:5]) if tuning is not None else None
         tp = ctypes.byref(t) if t is not None else None
         sp, op = ctypes.c_void_p(s_size.ctypes.data), ctypes.c_void_p(c_off0.ctypes.data)
         nbytes = lib().tcv_plan_workspace_bytes_var(self.n, sp, op, s_size.size, g_size, c_len, tp)
