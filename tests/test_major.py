@@ -23,7 +23,7 @@ def _fft_case(n, seed):
     return (rng.standard_normal(n * n) + 1j * rng.standard_normal(n * n)).astype(np.complex64)
 
 
-@pytest.mark.parametrize("n", [256, 4096])
+@pytest.mark.parametrize("n", [256, 1034, 4096])
 def test_fft_steps(tcv, orc, cuda_ok, n):
     import torch
 
@@ -78,8 +78,9 @@ def _close(got, ref, psf_scale):
 
 @pytest.mark.parametrize("cfg", [
     dict(n_samples=2000, w_size=9, cell_size=25.0, g_size=512, n_minor=20, cycles=3),
+    dict(n_samples=1500, w_size=9, n_chan=3, cell_size=25.0, g_size=512, n_minor=20, cycles=2),
     dict(n_samples=160000, w_size=33, cell_size=5.0, g_size=4096, n_minor=100, cycles=1),
-], ids=["512", "4096"])
+], ids=["512", "512-3chan", "4096"])
 def test_major_cycle_against_oracle(tcv, orc, cuda_ok, cfg):
     """The small problem over three cycles; tMajorACC's own problem (160000 samples, 4096^2,
     100 minor iterations) over its first cycle."""
@@ -89,7 +90,8 @@ def test_major_cycle_against_oracle(tcv, orc, cuda_ok, cfg):
     cycles = cfg.pop("cycles")
     m = MajorCycle(keep_stages=1, **cfg)
     m.init()
-    st = orc.major_setup(cfg["n_samples"], cfg["w_size"], 1, cfg["cell_size"], cfg["g_size"], 2000, 100)
+    st = orc.major_setup(cfg["n_samples"], cfg["w_size"], cfg.get("n_chan", 1), cfg["cell_size"], cfg["g_size"], 2000,
+                         100)
     iu, iv, co = m.offsets()
     assert np.array_equal(iu, st["iu"]) and np.array_equal(iv, st["iv"]) and np.array_equal(co, st["coff"])
     assert m.info()["support"] == st["support"] and m.info()["scale"] == np.float32(st["scale"])
