@@ -289,6 +289,22 @@ __global__ void __launch_bounds__(kHogThreads, 4) hog_iter_kernel(HogArgs a, int
         model_update(a, it, ppos, peak);
         st->done = it + 1;
     }
+    if (kVec && it > 0) {
+        // rows wholly outside this iteration's PSF overlap do not change: the CTA's candidate from
+        // an earlier iteration (same row partition; iteration 0 always scans, after the image
+        // scan's pixel partition) still holds, so it is left as it is without reading the rows
+        const int W = a.width, P = a.psf_width;
+        const int ry = int(ppos / unsigned(W)), py = int(st->psf_pos / unsigned(P));
+        const int starty = max(0, ry - py), stopy = min(W - 1, ry + (P - py - 1));
+        const int rows_per = (W + a.nblocks - 1) / a.nblocks;
+        const int r0 = int(blockIdx.x) * rows_per, r1 = min(W, r0 + rows_per);
+        if (r1 <= starty || r0 > stopy) {
+            const unsigned long long old = __ldcg(a.keys + blockIdx.x);
+            const float oldv = __ldcg(a.vals + blockIdx.x);
+            finish_scan(old, oldv, a.keys, a.vals, a.nblocks, st, par ^ 1);
+            return;
+        }
+    }
     float bv;
     unsigned long long skipped;
     const unsigned long long best = iter_body<kVec>(a, ppos, peak, st->psf_pos, bv, skipped);
