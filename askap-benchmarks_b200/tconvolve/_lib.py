@@ -197,6 +197,8 @@ SIGNATURES = {
     "tcv_hogbom_set_strategy": (None, [_I]),
     "tcv_find_peak": (_I, [_P, _I64, _P, _P, _P, _S, _P]),
     "tcv_fft_exec": (_I, [_P, _I, _I, _P]),
+    "tcv_probe_table_threads": (_I64, []),
+    "tcv_probe_table_stream": (_I, [_P, _I64, _I, _I, _P, _P, _P]),
     "tcv_fft_fix": (_I, [_P, _I64, _F, _P]),
     "tcv_image_from_grid": (_I, [_P, _I, _F, _P, _P]),
     "tcv_grid_from_image": (_I, [_P, _I, _P, _P]),

@@ -431,6 +431,8 @@ def b200_arm(args):
              ("degrid", "direct"): ("degrid_tile_kernel + slot_reduce_kernel" if args.degrid == "tiles"
                                     else "degrid_staged_kernel")}[(dom, args.path)]
 
+    l2_ceiling = l2_table_ceiling(torch, stream, updates, g_ms, d_ms, args.form) if args.path == "direct" else None
+
     # the other workloads run after the headline's context is released
     batched = serving = current = hogbom = major = None
     if not (args.no_batched and args.no_serving and args.no_current and args.no_hogbom and args.no_major):
@@ -479,7 +481,8 @@ def b200_arm(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kname,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",
-                         "alg_bytes_per_update": ALG_BYTES[dom], "launch_ms": dom_ms},
+                         "alg_bytes_per_update": ALG_BYTES[dom], "launch_ms": dom_ms,
+                         "l2_table_ceiling": l2_ceiling},
             "kernels": {"plan_ms": statistics.mean(plan_ms), "grid_ms": g_ms, "degrid_ms": d_ms,
                         "grid_alg_GBps": ALG_BYTES["grid"] * updates / (g_ms * 1e-3) / 1e9,
                         "degrid_alg_GBps": ALG_BYTES["degrid"] * updates / (d_ms * 1e-3) / 1e9,
@@ -824,6 +827,41 @@ def major_cpu_port():
             "kind": "port", "setup_s": setup_s,
             "sample": "one full-size major cycle of the oracle restatement (C gridding/degridding on all threads, "
                       "numpy FFT, C Hogbom)"}
+
+
+def l2_table_ceiling(torch, stream, updates, g_ms, d_ms, form):
+    """The tile kernels' own ceiling, measured live: the L2-to-SM bandwidth of random 128-byte
+    row segments (16 rows at the 129-entry table stride, from a 64 MiB buffer that stays in L2,
+    tcv_probe_table_stream), against which their table stream (table bytes per update x updates
+    / pass time) is set.  The HBM roofline above counts the reference's per-update grid traffic,
+    which these kernels keep on chip."""
+    import tconvolve
+    from tconvolve.raw import _ptr
+
+    L = tconvolve.lib()
+    buf = torch.rand(16 << 20, dtype=torch.float32, device="cuda")
+    out = torch.empty(int(L.tcv_probe_table_threads()), dtype=torch.float32, device="cuda")
+    nbytes = ctypes.c_int64()
+    launch = lambda: L.tcv_probe_table_stream(_ptr(buf), buf.numel(), 129, 256, _ptr(out), ctypes.byref(nbytes),
+                                              ctypes.c_void_p(stream.cuda_stream))
+    for _ in range(3):
+        if launch() != 0:
+            return None
+    ms = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    probe = nbytes.value / (statistics.median(ms) * 1e-3) / 1e9
+    tb = L.tcv_ctype_bytes(tconvolve.CTYPE_BY_NAME[form])
+    grid_gbs = tb * updates / (g_ms * 1e-3) / 1e9
+    degrid_gbs = tb * updates / (d_ms * 1e-3) / 1e9
+    return {"unit": "GB/s", "probe": probe, "table_bytes_per_update": tb,
+            "grid": grid_gbs, "grid_frac": grid_gbs / probe, "degrid": degrid_gbs, "degrid_frac": degrid_gbs / probe,
+            "probe_shape": "random 128-byte row segments, 16 rows at a 129-entry stride, 64 MiB L2-resident buffer"}
 
 
 def count_step_kernels(torch, step):

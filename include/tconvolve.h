@@ -648,6 +648,19 @@ tcv_status tcv_major_get_grid(tcv_major_ctx *ctx, int which, float *out);
 tcv_status tcv_major_get_vis(tcv_major_ctx *ctx, int which, float *out);
 tcv_status tcv_major_get_offsets(tcv_major_ctx *ctx, int32_t *iu, int32_t *iv, int32_t *coff);
 
+/* ------------------------------------------------------------------------------------------
+ * A measurement, not part of the path: the L2-to-SM bandwidth of this GPU for the tile kernels'
+ * table reads (random 128-byte row segments, 16 rows at a row stride, from an L2-resident
+ * buffer), the ceiling those kernels are bound by.  No counterpart in the reference.
+ * ---------------------------------------------------------------------------------------- */
+/* Threads of one probe launch (d_out must hold as many floats). */
+int64_t tcv_probe_table_threads(void);
+/* One launch over d_buf (n_floats, ideally a few tens of MB so that it stays in L2), each warp
+ * reading `samples` random 16-row windows of `stride` floats; *bytes_out receives the bytes the
+ * warps read (128 per row segment).  Asynchronous on the stream: time it with events. */
+tcv_status tcv_probe_table_stream(const float *d_buf, int64_t n_floats, int stride, int samples,
+                                  float *d_out, int64_t *bytes_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
