@@ -199,6 +199,13 @@ SIGNATURES = {
     "tcv_fft_exec": (_I, [_P, _I, _I, _P]),
     "tcv_probe_table_threads": (_I64, []),
     "tcv_probe_table_stream": (_I, [_P, _I64, _I, _I, _P, _P, _P]),
+    "tcv_band_histogram": (_I, [_P, _I64, _I, _I, _P, _P]),
+    "tcv_band_bounds": (_I, [_P, _I, _I, _I, _P]),
+    "tcv_band_workspace_bytes": (_S, [_I64, _I]),
+    "tcv_band_bucket": (_I, [_P, _P, _P, _P, _I64, _I, _I, _P, _I, _P, _P, _P, _P, _S, _P]),
+    "tcv_band_unpack": (_I, [_P, _I64, _P, _P, _P, _P, _P]),
+    "tcv_band_scatter": (_I, [_P, _P, _I64, _P, _P]),
+    "tcv_rows_add": (_I, [_P, _P, _I64, _P]),
     "tcv_fft_fix": (_I, [_P, _I64, _F, _P]),
     "tcv_image_from_grid": (_I, [_P, _I, _F, _P, _P]),
     "tcv_grid_from_image": (_I, [_P, _I, _P, _P]),

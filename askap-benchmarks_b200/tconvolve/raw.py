@@ -83,18 +83,32 @@ def init_offsets(u, v, w, freq, cell_size, w_cell_size, w_size, g_size, support,
 class Plan:
     """A binning plan (tcv_plan) in a torch-allocated workspace."""
 
-    def __init__(self, iu, iv, coff, support: int, g_size: int, c_len: int, stream=None):
+    def __init__(self, iu, iv, coff, support: int, g_size: int, c_len: int, stream=None, tuning=None):
+        """tuning: (tile_rows, group_mib, split, degrid_split) for tcv_plan_build_tuned; None for
+        the default plan (tcv_plan_build)."""
         import torch
+
+        from ._lib import TcvTuning
 
         self.n = iu.numel()
         self.support, self.g_size, self.c_len = support, g_size, c_len
-        nbytes = lib().tcv_plan_workspace_bytes(self.n, support, g_size, c_len)
-        self.work = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=iu.device)
         self._keep = (iu, iv, coff)
         self.handle = ctypes.c_void_p()
-        check(lib().tcv_plan_build(ctypes.byref(self.handle), _ptr(iu), _ptr(iv), _ptr(coff),
-                                   self.n, support, g_size, c_len, _ptr(self.work), nbytes,
-                                   _stream(stream)), "tcv_plan_build")
+        if tuning is None:
+            nbytes = lib().tcv_plan_workspace_bytes(self.n, support, g_size, c_len)
+            self.work = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=iu.device)
+            check(lib().tcv_plan_build(ctypes.byref(self.handle), _ptr(iu), _ptr(iv), _ptr(coff),
+                                       self.n, support, g_size, c_len, _ptr(self.work), nbytes,
+                                       _stream(stream)), "tcv_plan_build")
+        else:
+            t = TcvTuning(*(tuple(tuning) + (0, 0, 0, 0, 0))[:5])
+            nbytes = lib().tcv_plan_workspace_bytes_tuned(self.n, support, g_size, c_len, ctypes.byref(t))
+            if nbytes == 0:
+                raise _lib.TcvError(1, "tcv_plan_workspace_bytes_tuned")
+            self.work = torch.empty(nbytes, dtype=torch.uint8, device=iu.device)
+            check(lib().tcv_plan_build_tuned(ctypes.byref(self.handle), _ptr(iu), _ptr(iv), _ptr(coff),
+                                             self.n, support, g_size, c_len, ctypes.byref(t),
+                                             _ptr(self.work), nbytes, _stream(stream)), "tcv_plan_build_tuned")
 
     def grid(self, data, c, c_type: int, grid, c_scale: float = 1.0, stream=None):
         check(lib().tcv_plan_grid(self.handle, _ptr(data), _ptr(c), c_type, c_scale, _ptr(grid),

@@ -70,6 +70,9 @@ def parse_args():
     p.add_argument("--no-major", action="store_true", help="skip the imaging major cycle measurement")
     p.add_argument("--no-current", action="store_true",
                    help="skip the variable-support (current/tConvolveMPI) continuum and spectral measurement")
+    p.add_argument("--bands", action="store_true",
+                   help="also time the headline job split into row bands over the ranks (tconvolve.bands: "
+                        "halo rows exchanged over NCCL; strong scaling)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=4.0, help="target wall time of the CPU sample")
     return p.parse_args()
@@ -432,6 +435,11 @@ def b200_arm(args):
                                     else "degrid_staged_kernel")}[(dom, args.path)]
 
     l2_ceiling = l2_table_ceiling(torch, stream, updates, g_ms, d_ms, args.form) if args.path == "direct" else None
+    bands = None
+    if args.bands and args.path == "direct":
+        t = tuning["t"]
+        bands = bands_section(args, torch, stream, world, rank, prob, support, c_len, (iu_h, iv_h, co_h), vis,
+                              b.C(), form, (t.tile_rows, t.group_mib, t.split, t.degrid_split), updates, flush)
 
     # the other workloads run after the headline's context is released
     batched = serving = current = hogbom = major = None
@@ -494,6 +502,7 @@ def b200_arm(args):
             "current": current,
             "hogbom": hogbom,
             "major": major,
+            "bands": bands,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * (8 + 4 * 3),
                     "d2h_bytes_per_step": n * 8, "ms_per_step": e2e_mean},
             "gpu_launches": launches_per_step * args.steps if launches_per_step else None,
@@ -510,6 +519,101 @@ def b200_arm(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def bands_section(args, torch, stream, world, rank, prob, support, c_len, offsets, vis, c64_h, form, tuning, updates,
+                  flush):
+    """The headline job split into row bands over the ranks (tconvolve.bands): rank r starts with
+    the r-th contiguous share of the samples, the set-up moves each sample to the rank that owns
+    its footprint's centre row, and a step is one gridding pass (halo rows added into their
+    owners') and one degridding pass (halo rows fetched, values returned to the ranks that hold
+    those samples) of the whole job.  Device time of a step, max over ranks; the job is the same at
+    every N (strong scaling).  Checked once against one GPU's plan over all samples."""
+    import torch.distributed as dist
+
+    import tconvolve
+    from tconvolve import raw, replicas
+    from tconvolve.bands import BandJob, CudaBandOps, DistComm, SoloComm
+
+    iu_h, iv_h, co_h = offsets
+    n, g = iu_h.size, prob.g_size
+    a, e = rank * n // world, (rank + 1) * n // world
+
+    def dev(x):
+        return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+    c64 = dev(c64_h)
+    tab, scale = (c64, 1.0) if form == tconvolve.C64 else raw.convert_c(c64, form)[:2]
+    t0 = time.perf_counter()
+    job = BandJob(dev(vis[a:e]), dev(iu_h[a:e]), dev(iv_h[a:e]), dev(co_h[a:e]), support, g, c_len,
+                  comm=DistComm() if world > 1 else SoloComm(), ops=CudaBandOps(), tuning=tuning)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    grid = torch.zeros(g * g, dtype=torch.complex64, device="cuda")
+    out = torch.empty(e - a, dtype=torch.complex64, device="cuda")
+
+    # one pass of each against one GPU's plan over every sample (the band rows of the grid; the
+    # degridded values of this rank's share)
+    job.grid(grid, tab, form, scale)
+    job.degrid(grid, tab, form, out, scale)
+    plan = raw.Plan(dev(iu_h), dev(iv_h), dev(co_h), support, g, c_len, tuning=tuning)
+    one = torch.zeros(g * g, dtype=torch.complex64, device="cuda")
+    plan.grid(dev(vis), tab, form, one, scale)
+    one_out = torch.empty(n, dtype=torch.complex64, device="cuda")
+    plan.degrid(one, tab, form, one_out, scale)
+    r0, r1 = job.band
+    sums = torch.stack([(grid[r0 * g:r1 * g] - one[r0 * g:r1 * g]).abs().double().pow(2).sum(),
+                        one[r0 * g:r1 * g].abs().double().pow(2).sum(),
+                        (out - one_out[a:e]).abs().double().pow(2).sum(),
+                        one_out[a:e].abs().double().pow(2).sum()])
+    if world > 1:
+        dist.all_reduce(sums)
+    sums = sums.cpu().tolist()
+    del plan, one, one_out
+
+    steps = max(args.steps // 2, 5)
+    for _ in range(args.warmup):
+        job.grid(grid, tab, form, scale)
+        job.degrid(grid, tab, form, out, scale)
+        flush.zero_()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = []
+    for _ in range(steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(stream)
+        job.grid(grid, tab, form, scale)
+        ev[1].record(stream)
+        job.degrid(grid, tab, form, out, scale)
+        ev[2].record(stream)
+        flush.zero_()
+        ms.append((ev[0], ev[1], ev[2]))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    g_ms = statistics.mean(x[0].elapsed_time(x[1]) for x in ms)
+    d_ms = statistics.mean(x[1].elapsed_time(x[2]) for x in ms)
+    step_ms = statistics.mean(x[0].elapsed_time(x[2]) for x in ms)
+    mine = [float(job.n_band), float(r1 - r0)]
+    if world > 1:
+        step_ms, g_ms, d_ms, setup_s = replicas.max_over_ranks([step_ms, g_ms, d_ms, setup_s], device="cuda")
+        every = torch.zeros(2 * world, dtype=torch.float64, device="cuda")
+        every[2 * rank:2 * rank + 2] = torch.tensor(mine, dtype=torch.float64)
+        dist.all_reduce(every)
+        every = every.cpu().tolist()
+    else:
+        every = mine
+    return {"value": 2 * updates / (step_ms * 1e-3), "unit": UNIT, "ranks": world, "scaling": "strong",
+            "ms_per_step": step_ms, "grid_ms": g_ms, "degrid_ms": d_ms, "steps": steps,
+            "rows": job.rows, "samples_per_rank": [int(x) for x in every[0::2]],
+            "setup_s": setup_s, "tuning": list(tuning),
+            "grid_rel_l2_vs_one_gpu": (sums[0] / sums[1]) ** 0.5 if sums[1] else None,
+            "degrid_rel_l2_vs_one_gpu": (sums[2] / sums[3]) ** 0.5 if sums[3] else None,
+            # halo rows: each interior band edge, both ways, after gridding and before degridding;
+            # the degridded values of samples that changed rank (at most all of them)
+            "exchange_bytes_per_step_at_most": 2 * 2 * (world - 1) * support * g * 8 + n * 8,
+            "setup_exchange_bytes_at_most": n * 20}
 
 
 def batched_section(args, torch, stream, world):

@@ -649,6 +649,43 @@ tcv_status tcv_major_get_vis(tcv_major_ctx *ctx, int which, float *out);
 tcv_status tcv_major_get_offsets(tcv_major_ctx *ctx, int32_t *iu, int32_t *iv, int32_t *coff);
 
 /* ------------------------------------------------------------------------------------------
+ * Row-band split of one job over several GPUs (one process per GPU): rank b owns grid rows
+ * [rows[b], rows[b+1]); a sample goes to the band of its footprint's centre row iv + support
+ * (the footprint covers rows iv .. iv + 2*support, attic/tConvolveMPI/Benchmark.cc:137-150), so
+ * its updates reach at most `support` rows past its band's edges, into the neighbouring band
+ * (every band is at least `support` rows high).  These are the device steps; the host exchanges
+ * the records (one all-to-all) and the halo rows (one send/receive per band edge) with NCCL.
+ * No counterpart in the reference, whose ranks are independent replicas
+ * (attic/tConvolveMPI/tConvolveMPI.cc:78-119).
+ * ---------------------------------------------------------------------------------------- */
+/* d_hist[r] += samples whose centre row (iv + support, clamped to the grid) is r; d_hist holds
+ * g_size int64 counts, zeroed by the caller (then summed over the ranks). */
+tcv_status tcv_band_histogram(const int32_t *d_iv, int64_t n, int support, int g_size, int64_t *d_hist,
+                              void *stream);
+/* Host arithmetic: rows_out[0..n_bands] with rows_out[0] = 0, rows_out[n_bands] = g_size, bound b
+ * the first row where the histogram's samples below reach b/n_bands of the total, then moved
+ * (up from the bottom, down from the top) so that every band is at least max(support, 1) rows
+ * high.  TCV_ERR_ARG if n_bands is outside 1..64 or n_bands * max(support, 1) > g_size. */
+tcv_status tcv_band_bounds(const int64_t *hist, int g_size, int support, int n_bands, int32_t *rows_out);
+/* Workspace of tcv_band_bucket (0 for invalid arguments). */
+size_t tcv_band_workspace_bytes(int64_t n, int n_bands);
+/* Stable partition of n samples by band (rows: host array of n_bands + 1 bounds): records band
+ * by band in input order, 5 int32 per sample (data re and im bits, iu, iv, cOffset), perm[j] =
+ * the input index of record j, d_counts[b] (int64, device) = samples of band b.  n < 2^31. */
+tcv_status tcv_band_bucket(const float *d_data, const int32_t *d_iu, const int32_t *d_iv,
+                           const int32_t *d_coff, int64_t n, int support, int g_size,
+                           const int32_t *rows, int n_bands, int32_t *d_records, int32_t *d_perm,
+                           int64_t *d_counts, void *d_work, size_t work_bytes, void *stream);
+/* Records -> complex64 data and the iu, iv, cOffset arrays. */
+tcv_status tcv_band_unpack(const int32_t *d_records, int64_t n, float *d_data, int32_t *d_iu,
+                           int32_t *d_iv, int32_t *d_coff, void *stream);
+/* d_dst[perm[i]] = d_src[i] for n complex64 values. */
+tcv_status tcv_band_scatter(const float *d_src, const int32_t *d_perm, int64_t n, float *d_dst,
+                            void *stream);
+/* d_dst += d_src over n_complex complex64 values (a received halo into the owner's rows). */
+tcv_status tcv_rows_add(float *d_dst, const float *d_src, int64_t n_complex, void *stream);
+
+/* ------------------------------------------------------------------------------------------
  * A measurement, not part of the path: the L2-to-SM bandwidth of this GPU for the tile kernels'
  * table reads (random 128-byte row segments, 16 rows at a row stride, from an L2-resident
  * buffer), the ceiling those kernels are bound by.  No counterpart in the reference.
