@@ -490,6 +490,10 @@ def b200_arm(args):
                          "frac": achieved / peak, "traffic": traffic, "kernel": kname,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",
                          "alg_bytes_per_update": ALG_BYTES[dom], "launch_ms": dom_ms,
+                         "reading": ("frac above 1: the reference loop's bytes per update (table entry, grid "
+                                     "point read and written) are served from registers (the grid tile) and "
+                                     "L2 (the table's plane group); DRAM moves `traffic` bytes per launch; "
+                                     "the binding ceiling is l2_table_ceiling"),
                          "l2_table_ceiling": l2_ceiling},
             "kernels": {"plan_ms": statistics.mean(plan_ms), "grid_ms": g_ms, "degrid_ms": d_ms,
                         "grid_alg_GBps": ALG_BYTES["grid"] * updates / (g_ms * 1e-3) / 1e9,
