@@ -106,6 +106,8 @@ struct tcv_plan {
     int degrid_variant;            // TCV_DEGRID_TILES or TCV_DEGRID_ANCHOR (reference-layout tables)
     bool batch;                    // jobs carry their own grids (tcv_batch_plan_create)
     bool binned;
+    bool anchors_ready = false;    // the anchor binning matches the last binning
+    bool anchors_stale = false;    // a captured binning skipped it: anchor degridding re-bins always
     std::vector<tcv::JobDesc> host_jobs;  // the job table (kept alive for its asynchronous copy)
     std::vector<uint32_t> host_job_start;
     // variable-width plans

@@ -70,12 +70,18 @@ struct VarPlanes {
     uint16_t* ssz;
 };
 
+// anchor tile of a footprint's top-left corner (fx, fy) in plane group grp
+__device__ __forceinline__ uint32_t anchor_cell(const PlanGeom& g, uint32_t grp, uint32_t fx, uint32_t fy)
+{
+    return grp * uint32_t(g.natx * g.naty) + (fy / uint32_t(g.ta)) * uint32_t(g.natx) + fx / uint32_t(g.ta);
+}
+
 template <typename K>
 __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* __restrict__ iv,
                                  const int32_t* __restrict__ coff, PlanGeom g, const JobDesc* __restrict__ jobs,
                                  const uint32_t* __restrict__ job_start, K* keys, uint32_t* vals, K* akeys,
                                  uint32_t* avals, uint32_t* tile_count, uint32_t* atile_count, uint16_t* ntl,
-                                 unsigned long long* rejected, VarPlanes var)
+                                 unsigned long long* rejected, VarPlanes var, bool with_anchors)
 {
     const int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (d >= g.n) return;
@@ -106,16 +112,22 @@ __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* 
             vp[t] = uint32_t(d);
         }
         ntl[d] = 0;
-        if (g.anchors) {
+        if (with_anchors) {
             akeys[d] = K(1) << (g.akey_bits - 1);
             avals[d] = uint32_t(d);
         }
         return;
     }
-    const uint32_t grp = g.var ? uint32_t(var.plane_grp[plane]) : uint32_t(co / (s * s) / g.kid_group);
+    // in bounds, every operand below fits 32 bits (fx + s <= g_size, s*s <= c_len): 32-bit
+    // divisions (a 64-bit one is a long software sequence, several per sample)
+    const uint32_t ufx = uint32_t(fx), ufy = uint32_t(fy), us = uint32_t(s);
+    const uint32_t grp = g.var ? uint32_t(var.plane_grp[plane])
+                               : (co <= int64_t(0xffffffffll) ? uint32_t(co) / (us * us) : uint32_t(co / (s * s))) /
+                                     uint32_t(g.kid_group);
     const uint32_t cell0 = grp * uint32_t(g.ntiles) + jd.tile_base;
-    const int tx0 = int(fx / g.tw), tx1 = int((fx + s - 1) / g.tw);
-    const int ty0 = int(fy / g.th), ty1 = int((fy + s - 1) / g.th);
+    const uint32_t utw = uint32_t(g.tw), uth = uint32_t(g.th);
+    const int tx0 = int(ufx / utw), tx1 = int((ufx + us - 1) / utw);
+    const int ty0 = int(ufy / uth), ty1 = int((ufy + us - 1) / uth);
     int t = 0;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
@@ -130,12 +142,37 @@ __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* 
         kp[t] = sentinel;
         vp[t] = uint32_t(d);
     }
-    if (g.anchors) {
-        const uint32_t at = grp * uint32_t(g.natx * g.naty) + uint32_t(fy / g.ta) * g.natx + uint32_t(fx / g.ta);
+    if (with_anchors) {
+        const uint32_t at = anchor_cell(g, grp, ufx, ufy);
         akeys[d] = K(at);
         avals[d] = uint32_t(d);
         atomicAdd(&atile_count[at], 1u);
     }
+}
+
+// The anchor keys alone (one-job plans of one footprint width), for an anchor binning made after
+// the plan's own: the same bounds and cells as plan_keys_kernel.
+template <typename K>
+__global__ void anchor_keys_kernel(const int32_t* __restrict__ iu, const int32_t* __restrict__ iv,
+                                   const int32_t* __restrict__ coff, PlanGeom g, K* akeys, uint32_t* avals,
+                                   uint32_t* atile_count)
+{
+    const int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (d >= g.n) return;
+    const int64_t s = g.s;
+    const int64_t fx = (int64_t)iu[d] - g.support, fy = iv[d], co = coff[d];
+    const bool ok = fx >= 0 && fx + s <= g.g_size && fy >= 0 && fy + s <= g.g_size && co >= 0 && co + s * s <= g.c_len;
+    avals[d] = uint32_t(d);
+    if (!ok) {
+        akeys[d] = K(1) << (g.akey_bits - 1);
+        return;
+    }
+    const uint32_t us = uint32_t(s);
+    const uint32_t grp =
+        (co <= int64_t(0xffffffffll) ? uint32_t(co) / (us * us) : uint32_t(co / (s * s))) / uint32_t(g.kid_group);
+    const uint32_t at = anchor_cell(g, grp, uint32_t(fx), uint32_t(fy));
+    akeys[d] = K(at);
+    atomicAdd(&atile_count[at], 1u);
 }
 
 // the job table of a one-job plan (written on the device, so building such a plan is device
@@ -300,37 +337,87 @@ tcv_status build_units(tcv_plan* p, int split, uint32_t* nunits, uint32_t* ustar
     return TCV_OK;
 }
 
+// sort, scan and compact the anchor keys (written by plan_keys_kernel or anchor_keys_kernel)
+template <typename K>
+tcv_status sort_anchors(tcv_plan* p, cudaStream_t st)
+{
+    const PlanGeom& g = p->g;
+    const int acells = int(anchor_cells(g));
+    if (g.n > 0) {
+        cub::DoubleBuffer<K> akb(static_cast<K*>(p->akeys[0]), static_cast<K*>(p->akeys[1]));
+        cub::DoubleBuffer<uint32_t> avb(p->avals[0], p->avals[1]);
+        size_t tb = p->cub_bytes;
+        TCV_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_temp, tb, akb, avb, g.n, 0, g.akey_bits, st));
+        p->asel = avb.selector;
+    } else {
+        p->asel = 0;
+    }
+    thrust::counting_iterator<uint32_t> it(0);
+    size_t tb = p->cub_bytes;
+    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->atile_count, p->atile_start, acells, st));
+    thrust::transform_iterator<NonZero, const uint32_t*> afl(p->atile_count, NonZero());
+    tb = p->cub_bytes;
+    TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, afl, p->aitems, p->n_aitems, acells, st));
+    return TCV_OK;
+}
+
+template <typename K>
+tcv_status bin_anchors_now(tcv_plan* p, cudaStream_t st)
+{
+    const PlanGeom& g = p->g;
+    TCV_CUDA(cudaMemsetAsync(p->atile_count, 0, sizeof(uint32_t) * anchor_cells(g), st));
+    if (g.n > 0) {
+        anchor_keys_kernel<K><<<unsigned((g.n + 255) / 256), 256, 0, st>>>(
+            p->iu, p->iv, p->coff, g, static_cast<K*>(p->akeys[0]), p->avals[0], p->atile_count);
+        TCV_CUDA(cudaGetLastError());
+    }
+    return sort_anchors<K>(p, st);
+}
+
+bool stream_capturing(cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+// The anchor binning of a plan's samples, made now unless the last binning made it (a cache of
+// the plan's samples, so a const plan may fill it).
+tcv_status plan_anchors_ready(const tcv_plan* cp, cudaStream_t st)
+{
+    tcv_plan* p = const_cast<tcv_plan*>(cp);
+    if (p->anchors_ready && !p->anchors_stale) return TCV_OK;
+    const tcv_status s = p->g.key64 ? bin_anchors_now<uint64_t>(p, st) : bin_anchors_now<uint32_t>(p, st);
+    if (s == TCV_OK && !stream_capturing(st)) p->anchors_ready = true;  // a captured one runs at each replay
+    return s;
+}
+
+// The anchor binning is made with the plan's only when the plan degrids by anchor tiles at that
+// time; otherwise the first anchor degridding makes it (plan_anchors_ready).
 template <typename K>
 tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_t* coff, cudaStream_t st)
 {
     const PlanGeom& g = p->g;
     const int64_t np = g.n * g.max_tiles;
     const int cells = int(grid_cells(g)), acells = int(anchor_cells(g));
+    const bool with_anchors = g.anchors && p->degrid_variant == TCV_DEGRID_ANCHOR;
     TCV_CUDA(cudaMemsetAsync(p->tile_count, 0, sizeof(uint32_t) * size_t(cells), st));
-    if (g.anchors) TCV_CUDA(cudaMemsetAsync(p->atile_count, 0, sizeof(uint32_t) * size_t(acells), st));
+    if (with_anchors) TCV_CUDA(cudaMemsetAsync(p->atile_count, 0, sizeof(uint32_t) * size_t(acells), st));
     TCV_CUDA(cudaMemsetAsync(p->rejected, 0, sizeof(unsigned long long), st));
     TCV_CUDA(cudaMemsetAsync(p->status, 0, sizeof(unsigned int), st));
     if (g.n > 0) {
         const VarPlanes var{p->wplane, p->plane_s, p->plane_grp, p->ssz};
         plan_keys_kernel<K><<<unsigned((g.n + 255) / 256), 256, 0, st>>>(
             iu, iv, coff, g, p->jobs, p->job_start, static_cast<K*>(p->keys[0]), p->vals[0],
-            static_cast<K*>(p->akeys[0]), p->avals[0], p->tile_count, p->atile_count, p->ntl, p->rejected, var);
+            static_cast<K*>(p->akeys[0]), p->avals[0], p->tile_count, p->atile_count, p->ntl, p->rejected, var,
+            with_anchors);
         TCV_CUDA(cudaGetLastError());
         cub::DoubleBuffer<K> kb(static_cast<K*>(p->keys[0]), static_cast<K*>(p->keys[1]));
         cub::DoubleBuffer<uint32_t> vb(p->vals[0], p->vals[1]);
         size_t tb = p->cub_bytes;
         TCV_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_temp, tb, kb, vb, np, 0, g.key_bits, st));
         p->sel = vb.selector;
-        if (g.anchors) {
-            cub::DoubleBuffer<K> akb(static_cast<K*>(p->akeys[0]), static_cast<K*>(p->akeys[1]));
-            cub::DoubleBuffer<uint32_t> avb(p->avals[0], p->avals[1]);
-            tb = p->cub_bytes;
-            TCV_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_temp, tb, akb, avb, g.n, 0, g.akey_bits, st));
-            p->asel = avb.selector;
-        }
     } else {
         p->sel = 0;
-        p->asel = 0;
     }
     thrust::counting_iterator<uint32_t> it(0);
     size_t tb = p->cub_bytes;
@@ -338,13 +425,11 @@ tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_
     thrust::transform_iterator<NonZero, const uint32_t*> fl(p->tile_count, NonZero());
     tb = p->cub_bytes;
     TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, fl, p->items, p->n_items, cells, st));
-    if (g.anchors) {
-        tb = p->cub_bytes;
-        TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->atile_count, p->atile_start, acells, st));
-        thrust::transform_iterator<NonZero, const uint32_t*> afl(p->atile_count, NonZero());
-        tb = p->cub_bytes;
-        TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, afl, p->aitems, p->n_aitems, acells, st));
-    }
+    if (with_anchors) TCV_CHECK(sort_anchors<K>(p, st));
+    p->anchors_ready = with_anchors;
+    // a captured binning without anchors may be replayed on new samples behind the host's back:
+    // from then on an anchor degridding always bins the anchors itself
+    if (g.anchors && !with_anchors && stream_capturing(st)) p->anchors_stale = true;
     group_ranges_kernel<<<(g.n_groups + 1 + 127) / 128, 128, 0, st>>>(p->items, p->n_items, g.n_groups,
                                                                        uint32_t(g.ntiles), p->group_start);
     TCV_CUDA(cudaGetLastError());
@@ -892,6 +977,7 @@ tcv_status tcv_plan_degrid(const tcv_plan* plan, const float* d_grid, const void
         return launch_degrid_tiles(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type, c_scale,
                                    reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
     }
+    TCV_CHECK(plan_anchors_ready(plan, static_cast<cudaStream_t>(stream)));
     return launch_degrid(plan, reinterpret_cast<const float2*>(d_grid), d_c, c_type, c_scale,
                          reinterpret_cast<float2*>(d_data), static_cast<cudaStream_t>(stream));
 }

@@ -118,6 +118,18 @@ class Plan:
         check(lib().tcv_plan_degrid(self.handle, _ptr(grid), _ptr(c), c_type, c_scale, _ptr(out),
                                     _stream(stream)), "tcv_plan_degrid")
 
+    def capture(self, passes: int, data, c, c_type: int, grid, vis=None, c_scale: float = 1.0):
+        """CUDA graph of this plan's passes (tcv_graph_capture: bin, grid into `grid`, degrid into
+        `vis`, as the _lib.PASS_* bits say), replayed with Graph.launch()."""
+        from .batch import Graph
+
+        iu, iv, coff = self._keep
+        h = ctypes.c_void_p()
+        check(lib().tcv_graph_capture(ctypes.byref(h), self.handle, passes, _ptr(iu), _ptr(iv), _ptr(coff),
+                                      _ptr(data), _ptr(c), c_type, c_scale, _ptr(grid),
+                                      _ptr(vis) if vis is not None else None), "tcv_graph_capture")
+        return Graph(h, (data, c, grid, vis, self))
+
     def set_degrid_variant(self, variant: int):
         check(lib().tcv_plan_set_degrid_variant(self.handle, variant), "tcv_plan_set_degrid_variant")
 

@@ -273,6 +273,50 @@ def test_raw_out_of_bounds_samples_are_rejected(tcv, orc, cuda_ok):
     assert orc.rel_l2(o[keep], ref_o) <= REL_L2_FP32
 
 
+def test_anchor_binning_made_when_needed(tcv, orc, cuda_ok):
+    """A plan binned for the tile kernels has no anchor binning; the first anchor degridding makes
+    it, and it follows new samples binned by a replayed graph."""
+    import torch
+
+    from tconvolve import raw
+    from tconvolve._lib import PASS_BIN
+
+    prob = PROBLEMS["g2"]
+    c, support, iu, iv, co = _setup(orc, prob)
+    g = prob.g_size
+    vis = normal_vis(iu.size, 21)
+    dvis, dc, diu, div, dco = _dev(vis, c, iu, iv, co)
+    grid = torch.zeros(g * g, dtype=torch.complex64, device="cuda")
+    plan = raw.Plan(diu, div, dco, support, g, c.size)
+    plan.grid(dvis, dc, tcv.C64, grid)
+    h_grid = grid.cpu().numpy()
+    ref = orc.degrid_f32(h_grid, g, support, c, co, iu, iv)
+    out_t = torch.empty(iu.size, dtype=torch.complex64, device="cuda")
+    plan.degrid(grid, dc, tcv.C64, out_t)
+    plan.set_degrid_variant(1)
+    out_a = torch.empty_like(out_t)
+    plan.degrid(grid, dc, tcv.C64, out_a)
+    assert orc.rel_l2(out_t.cpu().numpy(), ref) <= REL_L2_FP32
+    assert orc.rel_l2(out_a.cpu().numpy(), ref) <= REL_L2_FP32
+    # a binning captured with the tile kernels' variant, replayed on other samples in the same
+    # buffers (the reversed order of a different subset)
+    plan.set_degrid_variant(0)
+    graph = plan.capture(PASS_BIN, dvis, dc, tcv.C64, grid)
+    sel = np.arange(iu.size)[::-1][: iu.size // 2].copy()
+    iu2, iv2, co2 = (np.concatenate([a[sel], a[sel]]) for a in (iu, iv, co))
+    for d, h in ((diu, iu2), (div, iv2), (dco, co2)):
+        d.copy_(torch.from_numpy(h))
+    graph.launch()
+    plan.set_degrid_variant(1)
+    plan.degrid(grid, dc, tcv.C64, out_a)
+    ref2 = orc.degrid_f32(h_grid, g, support, c, co2, iu2, iv2)
+    assert orc.rel_l2(out_a.cpu().numpy(), ref2) <= REL_L2_FP32
+    plan.set_degrid_variant(0)
+    plan.degrid(grid, dc, tcv.C64, out_t)
+    assert orc.rel_l2(out_t.cpu().numpy(), ref2) <= REL_L2_FP32
+    graph.close()
+
+
 def test_raw_extreme_positions_and_collisions(tcv, orc, cuda_ok):
     """Footprints touching all four grid edges, and 3000 samples piled on one position (one tile
     list far longer than a staging chunk)."""
