@@ -222,66 +222,221 @@ struct NonZero {
     __host__ __device__ __forceinline__ bool operator()(const uint32_t& v) const { return v != 0; }
 };
 
-// per non-empty cell k: the work units it is split into (cells of fewer than 2*split samples
-// stay whole) and the partial tiles those write (none for a whole cell)
-__global__ void unit_count_kernel(const uint32_t* __restrict__ items, const uint32_t* __restrict__ n_items,
-                                  const uint32_t* __restrict__ tile_count, uint32_t cap, uint32_t split,
-                                  uint32_t* nunits, uint32_t* nparts)
+// ------------------------------------------------------------------------------------------
+// Cell bookkeeping after the sort, in three launches over the cells (c = group * ntiles + tile):
+// per-block sums, one scan of those sums, then every cell's outputs.
+//   tile_start[c]     first sorted pair of cell c (exclusive sum of tile_count)
+//   items, n_items    the non-empty cells in order; group_start[g] = non-empty cells before
+//                     cell g*ntiles (group g's first item)
+//   per unit list (the gridding split, and the degridding split when it differs): per item its
+//   units (a cell of cnt >= 2*split samples makes cnt/split units, any other non-empty cell one),
+//   first unit and first partial tile (split cells only); the units themselves, unit q of a cell
+//   taking its samples [q*cnt/nu, (q+1)*cnt/nu); group_ustart[g] = units of the cells before
+//   cell g*ntiles
+// Item-indexed entries past n_items hold 0 units and the totals, as exclusive sums would.
+// ------------------------------------------------------------------------------------------
+constexpr int kCellThreads = 256;
+constexpr int kCellPer = 4;  // consecutive cells per thread
+constexpr uint32_t kCellBlock = uint32_t(kCellThreads) * kCellPer;
+constexpr int kCellVals = 6;  // pairs, non-empty, units, partials (gridding), units, partials (degridding)
+
+struct CellArgs {
+    const uint32_t* tile_count;
+    uint32_t cells, ntiles, split, dsplit;
+    int n_groups;
+    bool own_d;
+    uint32_t* part;  // [kCellVals][blocks] block sums, scanned in place, then the kCellVals totals
+    uint32_t *tile_start, *items, *n_items, *group_start;
+    uint32_t *nunits, *ustart, *pstart, *group_ustart;
+    uint4* units;
+    uint32_t *d_nunits, *d_ustart, *d_pstart, *d_group_ustart;
+    uint4* d_units;
+};
+
+__device__ __forceinline__ uint32_t units_of(uint32_t cnt, uint32_t split)
 {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= cap) return;
-    uint32_t nu = 0, np = 0;
-    if (k < *n_items) {
-        const uint32_t cnt = tile_count[items[k]];
-        nu = (split && cnt >= 2 * split) ? cnt / split : 1;
-        np = nu > 1 ? nu : 0;
-    }
-    nunits[k] = nu;
-    nparts[k] = np;
+    return cnt == 0 ? 0u : ((split && cnt >= 2u * split) ? cnt / split : 1u);
 }
 
-// the unit list: unit q of cell k takes samples [q*cnt/nu, (q+1)*cnt/nu) of the cell
-__global__ void unit_expand_kernel(const uint32_t* __restrict__ items, const uint32_t* __restrict__ n_items,
-                                   const uint32_t* __restrict__ tile_count, const uint32_t* __restrict__ tile_start,
-                                   const uint32_t* __restrict__ nunits, const uint32_t* __restrict__ ustart,
-                                   const uint32_t* __restrict__ pstart, uint4* units)
+__device__ __forceinline__ void cell_vals(uint32_t cnt, uint32_t split, uint32_t dsplit, uint32_t* v)
 {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= *n_items) return;
-    const uint32_t cell = items[k], cnt = tile_count[cell], first = tile_start[cell], nu = nunits[k];
+    const uint32_t nu = units_of(cnt, split), dnu = units_of(cnt, dsplit);
+    v[0] = cnt;
+    v[1] = cnt ? 1u : 0u;
+    v[2] = nu;
+    v[3] = nu > 1 ? nu : 0u;
+    v[4] = dnu;
+    v[5] = dnu > 1 ? dnu : 0u;
+}
+
+__device__ __forceinline__ void load_counts(const CellArgs& a, uint32_t c0, uint32_t* cnt)
+{
+#pragma unroll
+    for (int e = 0; e < kCellPer; ++e) cnt[e] = c0 + e < a.cells ? a.tile_count[c0 + e] : 0u;
+}
+
+__global__ void __launch_bounds__(kCellThreads) cell_sums_kernel(CellArgs a)
+{
+    __shared__ uint32_t ws[kCellVals][kCellThreads / 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t cnt[kCellPer], s[kCellVals] = {};
+    load_counts(a, blockIdx.x * kCellBlock + threadIdx.x * kCellPer, cnt);
+#pragma unroll
+    for (int e = 0; e < kCellPer; ++e) {
+        uint32_t v[kCellVals];
+        cell_vals(cnt[e], a.split, a.dsplit, v);
+#pragma unroll
+        for (int j = 0; j < kCellVals; ++j) s[j] += v[j];
+    }
+#pragma unroll
+    for (int j = 0; j < kCellVals; ++j) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) s[j] += __shfl_xor_sync(0xffffffffu, s[j], o);
+        if (lane == 0) ws[j][warp] = s[j];
+    }
+    __syncthreads();
+    if (threadIdx.x < kCellVals) {
+        uint32_t t = 0;
+        for (int w = 0; w < kCellThreads / 32; ++w) t += ws[threadIdx.x][w];
+        a.part[threadIdx.x * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// one block: exclusive sums of every row of part, the totals after them, and the totals'
+// entries of n_items, group_start and group_ustart
+__global__ void __launch_bounds__(1024) cell_scan_kernel(CellArgs a, uint32_t blocks)
+{
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry_s;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int j = 0; j < kCellVals; ++j) {
+        uint32_t* row = a.part + size_t(j) * blocks;
+        if (threadIdx.x == 0) carry_s = 0;
+        __syncthreads();
+        for (uint32_t base = 0; base < blocks; base += 1024) {
+            const uint32_t i = base + threadIdx.x;
+            const uint32_t v = i < blocks ? row[i] : 0u;
+            uint32_t x = v;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+                if (lane >= d) x += y;
+            }
+            if (lane == 31) wsum[warp] = x;
+            __syncthreads();
+            if (warp == 0) {
+                uint32_t t = wsum[lane];
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, t, d);
+                    if (lane >= d) t += y;
+                }
+                wsum[lane] = t;
+            }
+            __syncthreads();
+            const uint32_t excl = carry_s + (warp ? wsum[warp - 1] : 0u) + x - v;
+            if (i < blocks) row[i] = excl;
+            __syncthreads();  // carry_s and wsum are read before they change
+            if (threadIdx.x == 1023) carry_s = excl + v;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) a.part[size_t(kCellVals) * blocks + j] = carry_s;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const uint32_t* tot = a.part + size_t(kCellVals) * blocks;
+        *a.n_items = tot[1];
+        a.group_start[a.n_groups] = tot[1];
+        a.group_ustart[a.n_groups] = tot[2];
+        if (a.own_d) a.d_group_ustart[a.n_groups] = tot[4];
+    }
+}
+
+__device__ __forceinline__ void write_units(uint4* units, uint32_t cell, uint32_t cnt, uint32_t first, uint32_t nu,
+                                            uint32_t u0, uint32_t p0)
+{
     for (uint32_t q = 0; q < nu; ++q) {
         const uint32_t b0 = uint32_t(uint64_t(q) * cnt / nu), b1 = uint32_t(uint64_t(q + 1) * cnt / nu);
-        units[ustart[k] + q] = make_uint4(cell, first + b0, b1 - b0, nu > 1 ? pstart[k] + q : kDirect);
+        units[u0 + q] = make_uint4(cell, first + b0, b1 - b0, nu > 1 ? p0 + q : kDirect);
     }
 }
 
-// group_start[g] = first item whose cell belongs to group g or later (items are sorted)
-__global__ void group_ranges_kernel(const uint32_t* items, const uint32_t* n_items, int n_groups,
-                                    uint32_t cells_per_group, uint32_t* group_start)
+__global__ void __launch_bounds__(kCellThreads) cell_out_kernel(CellArgs a)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g > n_groups) return;
-    const uint32_t key = uint32_t(g) * cells_per_group;
-    const uint32_t n = *n_items;
-    uint32_t lo = 0, hi = n;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (items[mid] < key)
-            lo = mid + 1;
-        else
-            hi = mid;
+    __shared__ uint32_t ws[kCellVals][kCellThreads / 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t blocks = gridDim.x;
+    const uint32_t* tot = a.part + size_t(kCellVals) * blocks;
+    const uint32_t c0 = blockIdx.x * kCellBlock + threadIdx.x * kCellPer;
+    uint32_t cnt[kCellPer], s[kCellVals] = {};
+    load_counts(a, c0, cnt);
+#pragma unroll
+    for (int e = 0; e < kCellPer; ++e) {
+        uint32_t v[kCellVals];
+        cell_vals(cnt[e], a.split, a.dsplit, v);
+#pragma unroll
+        for (int j = 0; j < kCellVals; ++j) s[j] += v[j];
     }
-    group_start[g] = lo;
-}
-
-// group_ustart[g] = the first unit of group g's first item
-__global__ void group_units_kernel(const uint32_t* group_start, const uint32_t* n_items, int n_groups,
-                                   const uint32_t* nunits, const uint32_t* ustart, uint32_t* group_ustart)
-{
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g > n_groups) return;
-    const uint32_t lo = group_start[g], n = *n_items;
-    group_ustart[g] = lo < n ? ustart[lo] : (n ? ustart[n - 1] + nunits[n - 1] : 0);
+    // the thread's first cell: block offset + the lower warps' sums + the lower lanes' sums
+    uint32_t x[kCellVals];
+#pragma unroll
+    for (int j = 0; j < kCellVals; ++j) {
+        x[j] = s[j];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x[j], d);
+            if (lane >= d) x[j] += y;
+        }
+        if (lane == 31) ws[j][warp] = x[j];
+    }
+    __syncthreads();
+    uint32_t pre[kCellVals];
+#pragma unroll
+    for (int j = 0; j < kCellVals; ++j) {
+        uint32_t w = 0;
+        for (int k = 0; k < warp; ++k) w += ws[j][k];
+        pre[j] = a.part[size_t(j) * blocks + blockIdx.x] + w + x[j] - s[j];
+    }
+#pragma unroll
+    for (int e = 0; e < kCellPer; ++e) {
+        const uint32_t c = c0 + e;
+        if (c >= a.cells) break;
+        uint32_t v[kCellVals];
+        cell_vals(cnt[e], a.split, a.dsplit, v);
+        a.tile_start[c] = pre[0];
+        if (c % a.ntiles == 0) {
+            const uint32_t gi = c / a.ntiles;
+            a.group_start[gi] = pre[1];
+            a.group_ustart[gi] = pre[2];
+            if (a.own_d) a.d_group_ustart[gi] = pre[4];
+        }
+        if (cnt[e]) {
+            const uint32_t k = pre[1];
+            a.items[k] = c;
+            a.nunits[k] = v[2];
+            a.ustart[k] = pre[2];
+            a.pstart[k] = pre[3];
+            write_units(a.units, c, cnt[e], pre[0], v[2], pre[2], pre[3]);
+            if (a.own_d) {
+                a.d_nunits[k] = v[4];
+                a.d_ustart[k] = pre[4];
+                a.d_pstart[k] = pre[5];
+                write_units(a.d_units, c, cnt[e], pre[0], v[4], pre[4], pre[5]);
+            }
+        }
+        if (c >= tot[1]) {  // item-indexed entries past the last item
+            a.nunits[c] = 0;
+            a.ustart[c] = tot[2];
+            a.pstart[c] = tot[3];
+            if (a.own_d) {
+                a.d_nunits[c] = 0;
+                a.d_ustart[c] = tot[4];
+                a.d_pstart[c] = tot[5];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kCellVals; ++j) pre[j] += v[j];
+    }
 }
 
 inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
@@ -294,47 +449,27 @@ inline size_t max_units(const PlanGeom& g, int split) { return grid_cells(g) + m
 inline bool own_degrid_units(const PlanGeom& g) { return g.dsplit != g.split; }
 inline size_t anchor_cells(const PlanGeom& g) { return g.anchors ? size_t(g.n_groups) * g.natx * g.naty : 0; }
 
+inline uint32_t cell_blocks(const PlanGeom& g) { return uint32_t((grid_cells(g) + kCellBlock - 1) / kCellBlock); }
+inline size_t cell_scratch_bytes(const PlanGeom& g) { return (size_t(cell_blocks(g)) + 1) * kCellVals * 4; }
+
 template <typename K>
 size_t cub_temp_bytes(const PlanGeom& g)
 {
-    size_t a = 0, b = 0, c = 0, d = 0, e = 0, f = 0;
+    size_t a = 0, b = 0, c = 0, d = 0, f = 0;
     const int64_t np = g.n * g.max_tiles;
-    const int cells = int(grid_cells(g)), acells = int(anchor_cells(g));
+    const int acells = int(anchor_cells(g));
     cub::DoubleBuffer<K> kb(nullptr, nullptr);
     cub::DoubleBuffer<uint32_t> vb(nullptr, nullptr);
     thrust::counting_iterator<uint32_t> it(0);
     thrust::transform_iterator<NonZero, const uint32_t*> fl((const uint32_t*)nullptr, NonZero());
     cub::DeviceRadixSort::SortPairs(nullptr, a, kb, vb, np, 0, g.key_bits);
-    cub::DeviceScan::ExclusiveSum(nullptr, c, (uint32_t*)nullptr, (uint32_t*)nullptr, cells);
-    cub::DeviceSelect::Flagged(nullptr, e, it, fl, (uint32_t*)nullptr, (uint32_t*)nullptr, cells);
+    c = cell_scratch_bytes(g);  // the cell sums use this space after the sort
     if (g.anchors) {
         cub::DeviceRadixSort::SortPairs(nullptr, b, kb, vb, g.n, 0, g.akey_bits);
         cub::DeviceScan::ExclusiveSum(nullptr, d, (uint32_t*)nullptr, (uint32_t*)nullptr, acells);
         cub::DeviceSelect::Flagged(nullptr, f, it, fl, (uint32_t*)nullptr, (uint32_t*)nullptr, acells);
     }
-    return std::max(std::max(std::max(a, b), std::max(c, d)), std::max(e, f));
-}
-
-// the unit list of one unit size over the plan's non-empty cells, with its per-group ranges
-tcv_status build_units(tcv_plan* p, int split, uint32_t* nunits, uint32_t* ustart, uint32_t* pstart, uint4* units,
-                       uint32_t* group_ustart, cudaStream_t st)
-{
-    const PlanGeom& g = p->g;
-    const int cells = int(grid_cells(g));
-    unit_count_kernel<<<unsigned((cells + 255) / 256), 256, 0, st>>>(p->items, p->n_items, p->tile_count,
-                                                                      uint32_t(cells), uint32_t(split), nunits, pstart);
-    TCV_CUDA(cudaGetLastError());
-    size_t tb = p->cub_bytes;
-    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, nunits, ustart, cells, st));
-    tb = p->cub_bytes;
-    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, pstart, pstart, cells, st));
-    unit_expand_kernel<<<unsigned((cells + 255) / 256), 256, 0, st>>>(p->items, p->n_items, p->tile_count,
-                                                                       p->tile_start, nunits, ustart, pstart, units);
-    TCV_CUDA(cudaGetLastError());
-    group_units_kernel<<<(g.n_groups + 1 + 127) / 128, 128, 0, st>>>(p->group_start, p->n_items, g.n_groups, nunits,
-                                                                      ustart, group_ustart);
-    TCV_CUDA(cudaGetLastError());
-    return TCV_OK;
+    return std::max(std::max(std::max(a, b), std::max(c, d)), f);
 }
 
 // sort, scan and compact the anchor keys (written by plan_keys_kernel or anchor_keys_kernel)
@@ -419,24 +554,24 @@ tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_
     } else {
         p->sel = 0;
     }
-    thrust::counting_iterator<uint32_t> it(0);
-    size_t tb = p->cub_bytes;
-    TCV_CUDA(cub::DeviceScan::ExclusiveSum(p->cub_temp, tb, p->tile_count, p->tile_start, cells, st));
-    thrust::transform_iterator<NonZero, const uint32_t*> fl(p->tile_count, NonZero());
-    tb = p->cub_bytes;
-    TCV_CUDA(cub::DeviceSelect::Flagged(p->cub_temp, tb, it, fl, p->items, p->n_items, cells, st));
+    const bool own_d = own_degrid_units(g);
+    const CellArgs ca{p->tile_count, uint32_t(cells), uint32_t(g.ntiles), uint32_t(g.split), uint32_t(g.dsplit),
+                      g.n_groups, own_d, static_cast<uint32_t*>(p->cub_temp), p->tile_start, p->items, p->n_items,
+                      p->group_start, p->nunits, p->ustart, p->pstart, p->group_ustart, p->units,
+                      own_d ? p->d_nunits : nullptr, own_d ? p->d_ustart : nullptr, own_d ? p->d_pstart : nullptr,
+                      own_d ? p->d_group_ustart : nullptr, own_d ? p->d_units : nullptr};
+    const uint32_t cb = cell_blocks(g);
+    cell_sums_kernel<<<cb, kCellThreads, 0, st>>>(ca);
+    TCV_CUDA(cudaGetLastError());
+    cell_scan_kernel<<<1, 1024, 0, st>>>(ca, cb);
+    TCV_CUDA(cudaGetLastError());
+    cell_out_kernel<<<cb, kCellThreads, 0, st>>>(ca);
+    TCV_CUDA(cudaGetLastError());
     if (with_anchors) TCV_CHECK(sort_anchors<K>(p, st));
     p->anchors_ready = with_anchors;
     // a captured binning without anchors may be replayed on new samples behind the host's back:
     // from then on an anchor degridding always bins the anchors itself
     if (g.anchors && !with_anchors && stream_capturing(st)) p->anchors_stale = true;
-    group_ranges_kernel<<<(g.n_groups + 1 + 127) / 128, 128, 0, st>>>(p->items, p->n_items, g.n_groups,
-                                                                       uint32_t(g.ntiles), p->group_start);
-    TCV_CUDA(cudaGetLastError());
-    // work units: the gridding list, and the degridding list when its unit size differs
-    TCV_CHECK(build_units(p, g.split, p->nunits, p->ustart, p->pstart, p->units, p->group_ustart, st));
-    if (own_degrid_units(g))
-        TCV_CHECK(build_units(p, g.dsplit, p->d_nunits, p->d_ustart, p->d_pstart, p->d_units, p->d_group_ustart, st));
     return TCV_OK;
 }
 
