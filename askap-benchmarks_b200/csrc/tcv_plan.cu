@@ -76,15 +76,15 @@ __device__ __forceinline__ uint32_t anchor_cell(const PlanGeom& g, uint32_t grp,
     return grp * uint32_t(g.natx * g.naty) + (fy / uint32_t(g.ta)) * uint32_t(g.natx) + fx / uint32_t(g.ta);
 }
 
+// The pairs of sample d (its footprint's tiles, then sentinels up to max_tiles) into kp/vp.
 template <typename K>
-__global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* __restrict__ iv,
-                                 const int32_t* __restrict__ coff, PlanGeom g, const JobDesc* __restrict__ jobs,
-                                 const uint32_t* __restrict__ job_start, K* keys, uint32_t* vals, K* akeys,
-                                 uint32_t* avals, uint32_t* tile_count, uint32_t* atile_count, uint16_t* ntl,
-                                 unsigned long long* rejected, VarPlanes var, bool with_anchors)
+__device__ __forceinline__ void sample_keys(const int32_t* __restrict__ iu, const int32_t* __restrict__ iv,
+                                            const int32_t* __restrict__ coff, const PlanGeom& g,
+                                            const JobDesc* __restrict__ jobs, const uint32_t* __restrict__ job_start,
+                                            int64_t d, K* kp, uint32_t* vp, K* akeys, uint32_t* avals,
+                                            uint32_t* atile_count, uint16_t* ntl, unsigned long long* rejected,
+                                            const VarPlanes& var, bool with_anchors)
 {
-    const int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (d >= g.n) return;
     const int job = g.n_jobs > 1 ? job_of(job_start, g.n_jobs, uint32_t(d)) : 0;
     const JobDesc jd = jobs[job];
     int64_t s = g.s, support = g.support;
@@ -102,8 +102,6 @@ __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* 
     const int64_t co = coff[d];
     const bool ok = plane_ok && fx >= 0 && fx + s <= jd.g_size && fy >= 0 && fy + s <= jd.g_size && co >= 0 &&
                     co + s * s <= g.c_len;
-    K* kp = keys + d * g.max_tiles;
-    uint32_t* vp = vals + d * g.max_tiles;
     const K sentinel = K(1) << (g.key_bits - 1);
     if (!ok) {
         atomicAdd(rejected, 1ull);
@@ -131,10 +129,8 @@ __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* 
     int t = 0;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
-            const uint32_t cell = cell0 + uint32_t(ty) * uint32_t(jd.ntx) + uint32_t(tx);
-            kp[t] = K(cell);
+            kp[t] = K(cell0 + uint32_t(ty) * uint32_t(jd.ntx) + uint32_t(tx));
             vp[t] = uint32_t(d);
-            atomicAdd(&tile_count[cell], 1u);
             ++t;
         }
     ntl[d] = uint16_t(t);
@@ -147,6 +143,56 @@ __global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* 
         akeys[d] = K(at);
         avals[d] = uint32_t(d);
         atomicAdd(&atile_count[at], 1u);
+    }
+}
+
+// (sample, tile) pairs, max_tiles per sample in sample order.  kStaged: a block's pairs are built
+// in shared memory and written out in one coalesced sweep (a sample's pairs are max_tiles apart
+// across a warp otherwise).  The cells' sample counts come later from the sorted keys.
+template <typename K, bool kStaged>
+__global__ void plan_keys_kernel(const int32_t* __restrict__ iu, const int32_t* __restrict__ iv,
+                                 const int32_t* __restrict__ coff, PlanGeom g, const JobDesc* __restrict__ jobs,
+                                 const uint32_t* __restrict__ job_start, K* keys, uint32_t* vals, K* akeys,
+                                 uint32_t* avals, uint32_t* atile_count, uint16_t* ntl, unsigned long long* rejected,
+                                 VarPlanes var, bool with_anchors)
+{
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    const int64_t d0 = int64_t(blockIdx.x) * blockDim.x;
+    const int64_t d = d0 + threadIdx.x;
+    K* sk = reinterpret_cast<K*>(pk_smem);
+    uint32_t* sv = reinterpret_cast<uint32_t*>(sk + size_t(blockDim.x) * g.max_tiles);
+    K* kp = kStaged ? sk + size_t(threadIdx.x) * g.max_tiles : keys + d * g.max_tiles;
+    uint32_t* vp = kStaged ? sv + size_t(threadIdx.x) * g.max_tiles : vals + d * g.max_tiles;
+    if (d < g.n)
+        sample_keys<K>(iu, iv, coff, g, jobs, job_start, d, kp, vp, akeys, avals, atile_count, ntl, rejected, var,
+                       with_anchors);
+    if (kStaged) {
+        __syncthreads();
+        const int64_t rows = g.n - d0 < int64_t(blockDim.x) ? g.n - d0 : int64_t(blockDim.x);
+        const int64_t m = rows * g.max_tiles;
+        K* gk = keys + d0 * g.max_tiles;
+        uint32_t* gv = vals + d0 * g.max_tiles;
+        for (int64_t i = threadIdx.x; i < m; i += blockDim.x) {
+            gk[i] = sk[i];
+            gv[i] = sv[i];
+        }
+    }
+}
+
+// Cell bounds from the sorted keys: run_start[c] = first pair of cell c, run_end[c] = one past its
+// last (both stay 0 for an empty cell); sentinel pairs (left-out samples) sort last and count for
+// no cell.
+template <typename K>
+__global__ void run_bounds_kernel(const K* __restrict__ keys, int64_t np, int key_bits, uint32_t* run_start,
+                                  uint32_t* run_end)
+{
+    const K sentinel = K(1) << (key_bits - 1);
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < np; i += stride) {
+        const K k = keys[i];
+        if (k >= sentinel) continue;
+        if (i == 0 || keys[i - 1] != k) run_start[k] = uint32_t(i);
+        if (i + 1 == np || keys[i + 1] != k) run_end[k] = uint32_t(i + 1);
     }
 }
 
@@ -236,12 +282,12 @@ struct NonZero {
 // Item-indexed entries past n_items hold 0 units and the totals, as exclusive sums would.
 // ------------------------------------------------------------------------------------------
 constexpr int kCellThreads = 256;
-constexpr int kCellPer = 4;  // consecutive cells per thread
+constexpr int kCellPer = 1;  // consecutive cells per thread
 constexpr uint32_t kCellBlock = uint32_t(kCellThreads) * kCellPer;
 constexpr int kCellVals = 6;  // pairs, non-empty, units, partials (gridding), units, partials (degridding)
 
 struct CellArgs {
-    const uint32_t* tile_count;
+    uint32_t* tile_count;  // run ends on entry (run_bounds_kernel), the cells' pair counts on exit
     uint32_t cells, ntiles, split, dsplit;
     int n_groups;
     bool own_d;
@@ -269,10 +315,11 @@ __device__ __forceinline__ void cell_vals(uint32_t cnt, uint32_t split, uint32_t
     v[5] = dnu > 1 ? dnu : 0u;
 }
 
+// pairs of each cell: run end - run start (tile_start holds the run starts until cell_out_kernel)
 __device__ __forceinline__ void load_counts(const CellArgs& a, uint32_t c0, uint32_t* cnt)
 {
 #pragma unroll
-    for (int e = 0; e < kCellPer; ++e) cnt[e] = c0 + e < a.cells ? a.tile_count[c0 + e] : 0u;
+    for (int e = 0; e < kCellPer; ++e) cnt[e] = c0 + e < a.cells ? a.tile_count[c0 + e] - a.tile_start[c0 + e] : 0u;
 }
 
 __global__ void __launch_bounds__(kCellThreads) cell_sums_kernel(CellArgs a)
@@ -352,12 +399,22 @@ __global__ void __launch_bounds__(1024) cell_scan_kernel(CellArgs a, uint32_t bl
     }
 }
 
+// unit q takes the cell's pairs [floor(q*cnt/nu), floor((q+1)*cnt/nu)), stepped without a division
+// per unit: floor((q+1)*cnt/nu) = floor(q*cnt/nu) + cnt/nu + (carry of the remainders)
 __device__ __forceinline__ void write_units(uint4* units, uint32_t cell, uint32_t cnt, uint32_t first, uint32_t nu,
                                             uint32_t u0, uint32_t p0)
 {
+    const uint32_t base = cnt / nu, rem = cnt % nu;
+    uint32_t b0 = 0, r = 0;
     for (uint32_t q = 0; q < nu; ++q) {
-        const uint32_t b0 = uint32_t(uint64_t(q) * cnt / nu), b1 = uint32_t(uint64_t(q + 1) * cnt / nu);
+        uint32_t b1 = b0 + base;
+        r += rem;
+        if (r >= nu) {
+            r -= nu;
+            ++b1;
+        }
         units[u0 + q] = make_uint4(cell, first + b0, b1 - b0, nu > 1 ? p0 + q : kDirect);
+        b0 = b1;
     }
 }
 
@@ -404,6 +461,7 @@ __global__ void __launch_bounds__(kCellThreads) cell_out_kernel(CellArgs a)
         uint32_t v[kCellVals];
         cell_vals(cnt[e], a.split, a.dsplit, v);
         a.tile_start[c] = pre[0];
+        a.tile_count[c] = cnt[e];
         if (c % a.ntiles == 0) {
             const uint32_t gi = c / a.ntiles;
             a.group_start[gi] = pre[1];
@@ -535,22 +593,41 @@ tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_
     const int64_t np = g.n * g.max_tiles;
     const int cells = int(grid_cells(g)), acells = int(anchor_cells(g));
     const bool with_anchors = g.anchors && p->degrid_variant == TCV_DEGRID_ANCHOR;
-    TCV_CUDA(cudaMemsetAsync(p->tile_count, 0, sizeof(uint32_t) * size_t(cells), st));
+    TCV_CUDA(cudaMemsetAsync(p->tile_count, 0, sizeof(uint32_t) * size_t(cells), st));  // run ends
+    TCV_CUDA(cudaMemsetAsync(p->tile_start, 0, sizeof(uint32_t) * size_t(cells), st));  // run starts
     if (with_anchors) TCV_CUDA(cudaMemsetAsync(p->atile_count, 0, sizeof(uint32_t) * size_t(acells), st));
     TCV_CUDA(cudaMemsetAsync(p->rejected, 0, sizeof(unsigned long long), st));
     TCV_CUDA(cudaMemsetAsync(p->status, 0, sizeof(unsigned int), st));
     if (g.n > 0) {
         const VarPlanes var{p->wplane, p->plane_s, p->plane_grp, p->ssz};
-        plan_keys_kernel<K><<<unsigned((g.n + 255) / 256), 256, 0, st>>>(
-            iu, iv, coff, g, p->jobs, p->job_start, static_cast<K*>(p->keys[0]), p->vals[0],
-            static_cast<K*>(p->akeys[0]), p->avals[0], p->tile_count, p->atile_count, p->ntl, p->rejected, var,
-            with_anchors);
+        // staged key writes while a block's pairs fit the default 48 KB of shared memory
+        const size_t per = size_t(g.max_tiles) * (sizeof(K) + 4);
+        int threads = 256;
+        while (threads > 64 && size_t(threads) * per > (48u << 10)) threads /= 2;
+        const bool staged = size_t(threads) * per <= (48u << 10);
+        if (!staged) threads = 256;
+        const unsigned blocks = unsigned((g.n + threads - 1) / threads);
+        K* k0 = static_cast<K*>(p->keys[0]);
+        K* ak0 = static_cast<K*>(p->akeys[0]);
+        if (staged)
+            plan_keys_kernel<K, true><<<blocks, threads, size_t(threads) * per, st>>>(
+                iu, iv, coff, g, p->jobs, p->job_start, k0, p->vals[0], ak0, p->avals[0], p->atile_count, p->ntl,
+                p->rejected, var, with_anchors);
+        else
+            plan_keys_kernel<K, false><<<blocks, threads, 0, st>>>(iu, iv, coff, g, p->jobs, p->job_start, k0,
+                                                                   p->vals[0], ak0, p->avals[0], p->atile_count,
+                                                                   p->ntl, p->rejected, var, with_anchors);
         TCV_CUDA(cudaGetLastError());
         cub::DoubleBuffer<K> kb(static_cast<K*>(p->keys[0]), static_cast<K*>(p->keys[1]));
         cub::DoubleBuffer<uint32_t> vb(p->vals[0], p->vals[1]);
         size_t tb = p->cub_bytes;
         TCV_CUDA(cub::DeviceRadixSort::SortPairs(p->cub_temp, tb, kb, vb, np, 0, g.key_bits, st));
         p->sel = vb.selector;
+        int sms = 148, dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t rb = std::min<int64_t>((np + 255) / 256, int64_t(sms) * 8);
+        run_bounds_kernel<K><<<unsigned(rb), 256, 0, st>>>(kb.Current(), np, g.key_bits, p->tile_start, p->tile_count);
+        TCV_CUDA(cudaGetLastError());
     } else {
         p->sel = 0;
     }
