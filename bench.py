@@ -293,31 +293,58 @@ def b200_arm(args):
 
     dvariant = {"tiles": tconvolve._lib.DEGRID_TILES, "anchor": tconvolve._lib.DEGRID_ANCHOR}[args.degrid]
 
-    def step(tab, evs=None):
-        """One step with table `tab` (a tcv_device_buffers): plan, gridding pass, degridding pass."""
-        sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)  # the capture stream too
-        plan = ctypes.c_void_p()
-        if evs:
-            evs[0].record(stream)
-        check(L.tcv_plan_build_tuned(ctypes.byref(plan), P(tab.iu), P(tab.iv), P(tab.coff), n, support,
-                                     prob.g_size, c_len, ctypes.byref(tuning["t"]), P(work.data_ptr()), wbytes,
-                                     sp), "plan")
-        L.tcv_plan_set_degrid_variant(plan, dvariant)
-        if evs:
-            evs[1].record(stream)
-        check(L.tcv_plan_grid(plan, P(tab.data), P(tab.c_active), tab.c_type, tab.c_scale,
-                              P(tab.grid), sp), "grid")
-        if evs:
-            evs[2].record(stream)
-        check(L.tcv_plan_degrid(plan, P(tab.grid), P(tab.c_active), tab.c_type, tab.c_scale,
-                                P(tab.outdata), sp), "degrid")
-        if evs:
-            evs[3].record(stream)
-        L.tcv_plan_destroy(plan)
+    PASS_BIN, PASS_GRID, PASS_DEGRID = tconvolve._lib.PASS_BIN, tconvolve._lib.PASS_GRID, tconvolve._lib.PASS_DEGRID
 
-    def timed(tab, steps):
+    def make_step(tab, iu, iv, coff, data, grid, out, passes_list):
+        """A persistent plan over the arrays (device pointers) with table `tab`, and its passes
+        captured as CUDA graphs (tcv_graph_capture), one graph per entry of passes_list: the
+        binning, gridding and degridding all run at every launch.  Returns (run(evs), eager(),
+        close()): run launches the graphs in order, recording evs[0] before and evs[k+1] after
+        graph k; eager makes the same passes as plain calls (for counting their kernels)."""
+        plan = ctypes.c_void_p()
+        check(L.tcv_plan_build_tuned(ctypes.byref(plan), P(iu), P(iv), P(coff), n, support, prob.g_size, c_len,
+                                     ctypes.byref(tuning["t"]), P(work.data_ptr()), wbytes, sp), "plan")
+        check(L.tcv_plan_set_degrid_variant(plan, dvariant), "degrid variant")
+        graphs = []
+        for passes in passes_list:
+            gph = ctypes.c_void_p()
+            check(L.tcv_graph_capture(ctypes.byref(gph), plan, passes, P(iu), P(iv), P(coff), P(data),
+                                      P(tab.c_active), tab.c_type, tab.c_scale, P(grid), P(out)), "capture")
+            graphs.append(gph)
+
+        def run(evs=None):
+            if evs:
+                evs[0].record(stream)
+            for k, gph in enumerate(graphs):
+                check(L.tcv_graph_launch(gph, sp), "graph launch")
+                if evs:
+                    evs[k + 1].record(stream)
+
+        def eager():
+            cs = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)  # the capture stream too
+            check(L.tcv_plan_bin(plan, P(iu), P(iv), P(coff), cs), "bin")
+            check(L.tcv_plan_grid(plan, P(data), P(tab.c_active), tab.c_type, tab.c_scale, P(grid), cs), "grid")
+            check(L.tcv_plan_degrid(plan, P(grid), P(tab.c_active), tab.c_type, tab.c_scale, P(out), cs), "degrid")
+
+        def close():
+            for gph in graphs:
+                L.tcv_graph_destroy(gph)
+            L.tcv_plan_destroy(plan)
+
+        return run, eager, close
+
+    def timed(tab, steps, count=False):
+        """Timed steps with table `tab` (a tcv_device_buffers): binning, gridding and degridding
+        passes, each one graph launch, events between them."""
+        run, eager, close = make_step(tab, tab.iu, tab.iv, tab.coff, tab.data, tab.grid, tab.outdata,
+                                      (PASS_BIN, PASS_GRID, PASS_DEGRID))
+        counted = None
+        if count:
+            eager()
+            torch.cuda.synchronize()
+            counted = count_step_kernels(torch, eager)  # kernels of one step, from a capture of it
         for _ in range(args.warmup):
-            step(tab)
+            run()
             flush.zero_()
         torch.cuda.synchronize()
         evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
@@ -326,24 +353,20 @@ def b200_arm(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for k in range(steps):
-            step(tab, evs[k])
+            run(evs[k])
             flush.zero_()  # L2 flush between timed steps (outside the events)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         wall = time.perf_counter() - t0
+        close()
         return ([e[0].elapsed_time(e[1]) for e in evs], [e[1].elapsed_time(e[2]) for e in evs],
-                [e[2].elapsed_time(e[3]) for e in evs], [e[0].elapsed_time(e[3]) for e in evs], wall)
-
-    # kernels launched by one step, counted from a CUDA-graph capture of it
-    step(bufs)
-    torch.cuda.synchronize()
-    launches_per_step = count_step_kernels(torch, lambda: step(bufs))
+                [e[2].elapsed_time(e[3]) for e in evs], [e[0].elapsed_time(e[3]) for e in evs], wall, counted)
 
     gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     clocks = ClockSampler(gpu_uuid)
     clocks.start()
-    plan_ms, grid_ms, degrid_ms, step_ms, t_wall = timed(bufs, args.steps)
+    plan_ms, grid_ms, degrid_ms, step_ms, t_wall, launches_per_step = timed(bufs, args.steps, count=True)
     plain = None
     if args.form != "c64":
         # the plain form (complex64 table, the reference's storage) measured beside the chosen one
@@ -351,7 +374,7 @@ def b200_arm(args):
         chosen_t = tuning["t"]
         if "c64" in tunings:
             tuning["t"] = TcvTuning(*tunings["c64"][0])
-        p_plan, p_grid, p_degrid, p_step, _ = timed(b.device_buffers(), args.steps)
+        p_plan, p_grid, p_degrid, p_step, _, _ = timed(b.device_buffers(), args.steps)
         tuning["t"] = chosen_t
         b.set_ctype(form)
         bufs = b.device_buffers()
@@ -374,23 +397,20 @@ def b200_arm(args):
     d_co = torch.empty_like(d_iu)
     d_out = torch.empty(n, dtype=torch.complex64, device="cuda")
 
+    d_vis.copy_(h_vis)
+    d_iu.copy_(h_iu)
+    d_iv.copy_(h_iv)
+    d_co.copy_(h_co)
+    e2e_run, _, e2e_close = make_step(bufs, d_iu.data_ptr(), d_iv.data_ptr(), d_co.data_ptr(), d_vis.data_ptr(),
+                                      bufs.grid, d_out.data_ptr(), (PASS_BIN | PASS_GRID | PASS_DEGRID,))
+
     def e2e_step():
         d_vis.copy_(h_vis, non_blocking=True)
         d_iu.copy_(h_iu, non_blocking=True)
         d_iv.copy_(h_iv, non_blocking=True)
         d_co.copy_(h_co, non_blocking=True)
-        plan = ctypes.c_void_p()
-        sp = ctypes.c_void_p(stream.cuda_stream)
-        check(L.tcv_plan_build_tuned(ctypes.byref(plan), P(d_iu.data_ptr()), P(d_iv.data_ptr()),
-                                     P(d_co.data_ptr()), n, support, prob.g_size, c_len, ctypes.byref(tuning["t"]),
-                                     P(work.data_ptr()), wbytes, sp), "plan")
-        L.tcv_plan_set_degrid_variant(plan, dvariant)
-        check(L.tcv_plan_grid(plan, P(d_vis.data_ptr()), P(bufs.c_active), bufs.c_type, bufs.c_scale,
-                              P(bufs.grid), sp), "grid")
-        check(L.tcv_plan_degrid(plan, P(bufs.grid), P(bufs.c_active), bufs.c_type, bufs.c_scale,
-                                P(d_out.data_ptr()), sp), "degrid")
+        e2e_run()
         h_out.copy_(d_out, non_blocking=True)
-        L.tcv_plan_destroy(plan)
 
     for _ in range(args.warmup):
         e2e_step()
@@ -406,6 +426,7 @@ def b200_arm(args):
         e2e_ms.append(a.elapsed_time(z))
         flush.zero_()
     torch.cuda.synchronize()
+    e2e_close()
     clk = clocks.stop()
     if int(torch.count_nonzero(torch.isnan(torch.view_as_real(h_out)))) != 0:
         raise RuntimeError("non-finite degridded output")
@@ -485,7 +506,10 @@ def b200_arm(args):
                                   if tunings else "default"},
                        "parallelism": f"replicas x{world}",
                        "l2": f"{L2_FLUSH_BYTES >> 20} MiB buffer written between timed steps",
-                       "step": "binning plan + gridding pass + degridding pass"},
+                       "step": ("binning + gridding pass + degridding pass, every step; each pass one CUDA "
+                                "graph launch (tcv_graph_capture) on a persistent plan, events between them"),
+                       "e2e_step": ("H2D of the samples (data, iu, iv, cOffset) from pinned memory, one graph "
+                                    "launch of the three passes, D2H of the degridded samples")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kname,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",
