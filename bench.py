@@ -125,6 +125,12 @@ def cpu_sample_size(threads: int, seconds: float) -> int:
     return max(200, min(per, 160000))
 
 
+def workload_name(name: str, prob, support: int) -> str:
+    """The workload as both arms name it in config.workload."""
+    return (f"{name}: {prob.n_samples} samples x {prob.n_chan} chan, gSize {prob.g_size}, wSize {prob.w_size}, "
+            f"support {support} ({2 * support + 1}^2 footprint), cellSize {prob.cell_size}")
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -141,8 +147,7 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * statistics.mean(step_s), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (reference generator, vis = 1+0i)",
-        "config": {"workload": f"{args.workload}: {prob.n_samples} samples, gSize {prob.g_size}, "
-                               f"wSize {prob.w_size}, support {prob.support()}",
+        "config": {"workload": workload_name(args.workload, prob, prob.support()),
                    "form": "reference CPU (std::complex<float>)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": sample},
@@ -493,9 +498,7 @@ def b200_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": f"synthetic: reference generator u,v,w (seed 0); N(0,1) complex64 visibilities "
                     f"(PCG64 seed {VIS_SEED})",
-            "config": {"workload": f"{args.workload}: {prob.n_samples} samples x {prob.n_chan} chan, "
-                                   f"gSize {prob.g_size}, wSize {prob.w_size}, support {support} "
-                                   f"({2 * support + 1}^2 footprint), cellSize {prob.cell_size}",
+            "config": {"workload": workload_name(args.workload, prob, support),
                        "form": (f"{args.form} (chosen form: real parts of the reference's table, whose "
                                 "imaginary parts are zero; bit-identical to the plain c64 result)"
                                 if args.form == "r32" else args.form),
