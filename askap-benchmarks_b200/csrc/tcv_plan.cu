@@ -6,7 +6,12 @@
 //   gridding  : every output tile of tw x th points gets the list of samples whose footprint
 //               overlaps it (a footprint of sSize^2 touches up to max_tiles tiles);
 //   degridding: every anchor tile of ta x ta gets the samples whose footprint's top-left corner
-//               lies in it (each sample exactly once; one-job plans only).
+//               lies in it (each sample exactly once; one-job plans only; made with the plan's
+//               binning only while the plan degrids by anchor tiles, else at that variant's first
+//               use).
+// Each cell's pair range comes from the run bounds of the sorted keys (no per-pair atomics), and
+// the per-cell bookkeeping (tile offsets, the non-empty cells, per-group ranges, the work-unit
+// lists) takes three launches over the cells.
 // Kernel indices kid = cOffset / sSize^2 (w-plane major, then the oversampling offsets) are
 // grouped into runs of whole w-planes whose slice of the table fits in L2 with room to spare.
 // The sort key is the work cell (group, tile), ordered group-major, so all SMs work through the
