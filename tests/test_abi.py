@@ -291,3 +291,32 @@ def test_tuning_kernel_field_validation(tcv):
     assert L.tcv_plan_workspace_bytes_var(*args, ctypes.byref(TcvTuning(8, 32, 0, 0, 4))) == 0
     assert TcvTuning(8, 32, 0, 0, 3).as_tuple() == (8, 32, 0, 0, 3)
     assert TcvTuning(8, 32, 0, 0, 0).as_tuple() == (8, 32, 0, 0)
+
+
+def test_band_split_argument_validation(tcv):
+    """The row-band steps refuse bad arguments before any device work."""
+    L = tcv.lib()
+    P = ctypes.c_void_p
+    one = P(16)  # never dereferenced: every call below fails its argument checks first
+    rows = (ctypes.c_int32 * 3)(0, 100, 256)
+    bad_rows = (ctypes.c_int32 * 3)(0, 300, 256)  # not ascending
+    counts = P(32)
+    assert L.tcv_band_histogram(None, 10, 4, 256, counts, None) == 1          # no iv
+    assert L.tcv_band_histogram(one, 10, 4, 256, None, None) == 1             # no histogram
+    assert L.tcv_band_histogram(one, -1, 4, 256, counts, None) == 1
+    assert L.tcv_band_histogram(one, 0, 4, 256, counts, None) == 0            # nothing to count
+    assert L.tcv_band_workspace_bytes(10, 0) == 0 and L.tcv_band_workspace_bytes(10, 65) == 0
+    assert L.tcv_band_workspace_bytes(10, 2) > 0
+    args = [one, one, one, one, 10, 4, 256, rows, 2, one, one, counts, one, 1 << 20, None]
+    for i, bad in ((7, bad_rows), (8, 0), (8, 65), (4, -1), (11, None), (12, None)):
+        a = list(args)
+        a[i] = bad
+        assert L.tcv_band_bucket(*a) == 1, i
+    a = list(args)
+    a[13] = 16  # workspace smaller than tcv_band_workspace_bytes
+    assert L.tcv_band_bucket(*a) == 7
+    assert L.tcv_band_unpack(None, 5, one, one, one, one, None) == 1
+    assert L.tcv_band_unpack(one, 0, None, None, None, None, None) == 0
+    assert L.tcv_band_scatter(one, None, 5, one, None) == 1
+    assert L.tcv_rows_add(None, one, 5, None) == 1
+    assert L.tcv_rows_add(one, one, -1, None) == 1
