@@ -344,3 +344,137 @@ def test_band_split_threads_full_size(tcv, cuda_ok):
     counts = np.bincount(np.searchsorted(np.asarray(rows[1:-1]), np.clip(iv + support, 0, prob.g_size - 1),
                                          side="right"), minlength=4)
     assert counts.max() <= 1.5 * iu.size / 4
+
+
+def _narrow_samples(orc, prob):
+    """The problem's samples moved into a narrow band of rows (so that the bounds leave some band
+    without samples), plus a few whose footprint leaves the grid."""
+    c, support, iu, iv, co = _setup(orc, prob)
+    g = prob.g_size
+    rng = np.random.default_rng(3)
+    iv = (g // 3 + rng.integers(0, 8, iv.size)).astype(np.int32)  # centre rows in [g/3 + s, g/3 + s + 8)
+    bad = np.array([5, 17, iu.size - 1])
+    iv[bad[:2]] = -1  # footprint starts above the first row
+    iu = iu.copy()
+    iu[bad[2]] = support - 1  # one column past the left edge
+    return c, support, iu, iv, co, bad
+
+
+def _band_worker_narrow(rank, world, port, q):
+    import datetime
+    import sys
+
+    for p in (REPO, PKG, os.path.join(REPO, "tests")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import torch
+    import torch.distributed as dist
+
+    from band_helpers import NumpyBandOps
+    from oracle import oracle as O
+    from tconvolve.bands import BandJob, DistComm
+    from tconvolve.workload import PROBLEMS, normal_vis
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        prob = PROBLEMS["g2"]
+        c, support, iu, iv, co, bad = _narrow_samples(O, prob)
+        keep = np.ones(iu.size, bool)
+        keep[bad] = False
+        vis = normal_vis(iu.size, VIS_SEED)
+        a, e = _shares(iu.size, world)[rank]
+        t = torch.from_numpy
+        # the oracle plans grid every sample they are given: hand them the in-bounds ones, as the
+        # device plans do after counting the others out
+        sl = slice(a, e)
+        m = keep[sl]
+        job = BandJob(t(vis[sl][m].copy()), t(iu[sl][m].copy()), t(iv[sl][m].copy()), t(co[sl][m].copy()), support,
+                      prob.g_size, c.size, comm=DistComm(), ops=NumpyBandOps(O, c))
+        grid = torch.zeros(prob.g_size ** 2, dtype=torch.complex64)
+        job.grid(grid, None, 0)
+        r0, r1 = job.band
+        q.put((rank, job.rows, grid[r0 * prob.g_size:r1 * prob.g_size].numpy().copy(), np.zeros(0, np.complex64),
+               job.n_band))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_band_split_gloo_empty_band(orc):
+    """Samples in a narrow range of rows: the bounds keep every band at least `support` rows high,
+    so one band holds no sample and its rank only takes part in the exchanges."""
+    prob = PROBLEMS["g2"]
+    c, support, iu, iv, co, bad = _narrow_samples(orc, prob)
+    keep = np.ones(iu.size, bool)
+    keep[bad] = False
+    vis = normal_vis(iu.size, VIS_SEED)
+    ref = np.zeros(prob.g_size ** 2, np.complex64)
+    orc.grid_f32(vis[keep], support, c, co[keep], iu[keep], iv[keep], ref, prob.g_size)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_band_worker_narrow, args=(r, 3, port, q)) for r in range(3)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=180) for _ in procs], key=lambda x: x[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert min(o[4] for o in out) == 0  # a band without samples
+    assert sum(o[4] for o in out) == int(keep.sum())
+    grid, _ = _assemble(out, prob.g_size)
+    assert orc.rel_l2(grid, ref) <= REL_L2_FP32
+
+
+@pytest.mark.gpu
+def test_band_split_threads_empty_band_and_rejected(tcv, orc, cuda_ok):
+    """On one GPU (ranks as threads): a band without samples, and samples outside the grid counted
+    out by whichever rank receives them, as one GPU's plan counts them."""
+    import sys
+
+    import torch
+
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    from band_helpers import run_threads
+    from tconvolve import raw
+    from tconvolve.bands import BandJob, CudaBandOps
+
+    prob = PROBLEMS["g2"]
+    c, support, iu, iv, co, bad = _narrow_samples(orc, prob)
+    g = prob.g_size
+    vis = normal_vis(iu.size, VIS_SEED)
+    dc = torch.from_numpy(c).cuda()
+    shares = _shares(iu.size, 3)
+
+    def rank_fn(rank, comm):
+        a, e = shares[rank]
+        d = [torch.from_numpy(np.ascontiguousarray(x[a:e])).cuda() for x in (vis, iu, iv, co)]
+        job = BandJob(*d, support, g, c.size, comm=comm, ops=CudaBandOps(), tuning=(16, 32, 0, 0))
+        grid = torch.zeros(g * g, dtype=torch.complex64, device="cuda")
+        job.grid(grid, dc, tcv.C64)
+        r0, r1 = job.band
+        out = torch.full((e - a,), 7 + 7j, dtype=torch.complex64, device="cuda")
+        job.degrid(grid, dc, tcv.C64, out)
+        return job.rows, grid[r0 * g:r1 * g].cpu().numpy(), out.cpu().numpy(), job.rejected(), job.n_band
+
+    res = run_threads(3, rank_fn)
+    rows = res[0][0]
+    assert min(x[4] for x in res) == 0  # a band without samples
+    assert res[0][4] > 0  # band 0: the samples above the first row (counted out) beside valid ones
+    assert sum(x[3] for x in res) == bad.size
+    grid = np.zeros(g * g, np.complex64)
+    for rank, (_, band_rows, _, _, _) in enumerate(res):
+        grid[rows[rank] * g:rows[rank + 1] * g] = band_rows
+    keep = np.ones(iu.size, bool)
+    keep[bad] = False
+    ref = np.zeros(g * g, np.complex64)
+    orc.grid_f32(vis[keep], support, c, co[keep], iu[keep], iv[keep], ref, g)
+    assert orc.rel_l2(grid, ref) <= REL_L2_FP32
+    deg = np.concatenate([x[2] for x in res])
+    assert np.all(deg[bad] == 0)  # counted out: nothing degridded into them
+    plan = raw.Plan(*[torch.from_numpy(x).cuda() for x in (iu, iv, co)], support, g, c.size, tuning=(16, 32, 0, 0))
+    one = torch.empty(iu.size, dtype=torch.complex64, device="cuda")
+    plan.degrid(torch.from_numpy(grid).cuda(), dc, tcv.C64, one)
+    assert plan.rejected() == bad.size
+    assert np.array_equal(deg, one.cpu().numpy())
