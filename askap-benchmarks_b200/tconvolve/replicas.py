@@ -9,6 +9,8 @@ Here the replicas are torch.distributed processes: NCCL on GPUs, gloo on CPU (te
 * checksum        - order-independent 64-bit digest of a result array (bit pattern based)
 * cross_check     - every rank's digest must equal rank 0's (replicas of one problem are
                     bit-identical because the kernels are deterministic)
+* rank0_tunings   - every rank takes rank 0's plan tunings (each rank's autotuner may pick a
+                    different one, and a different gridding split changes the order of the sums)
 """
 from __future__ import annotations
 
@@ -56,3 +58,21 @@ def cross_check(digest: int, device="cpu") -> bool:
     dist.all_reduce(lo, op=dist.ReduceOp.MIN)
     dist.all_reduce(hi, op=dist.ReduceOp.MAX)
     return int(lo.item()) == int(hi.item())
+
+
+def rank0_tunings(tunings: dict, device="cpu") -> dict:
+    """{name: (tuning tuple of up to five ints, extra)} with every tuple replaced by rank 0's; the
+    same names on every rank.  A fifth entry of 0 is dropped (the kernel-bits field unset)."""
+    import torch
+    import torch.distributed as dist
+
+    _, n = world()
+    if n == 1:
+        return dict(tunings)
+    out = {}
+    for name in sorted(tunings):
+        t = torch.tensor((list(tunings[name][0]) + [0] * 5)[:5], dtype=torch.int64, device=device)
+        dist.broadcast(t, 0)
+        vals = [int(x) for x in t.cpu().tolist()]
+        out[name] = (tuple(vals[:4]) + ((vals[4],) if vals[4] else ()), tunings[name][1])
+    return out

@@ -280,6 +280,11 @@ def b200_arm(args):
         tunings[args.form] = b.tune(3)
     elif form != tconvolve.C64:
         b.set_ctype(form)
+    if world > 1 and tunings:
+        # every replica takes rank 0's choices: a different gridding split would change the order
+        # of the sums, and the replicas' results are compared bit for bit
+        tunings = replicas.rank0_tunings(tunings, device="cuda")
+        b.set_tuning(*tunings[args.form][0][:4])
     b.sync()
     bufs = b.device_buffers()
     support = b.getSupport()

@@ -45,7 +45,10 @@ def _worker(rank, world, port, plant, q):
         if plant and rank == 1:
             grid[1234] += np.complex64(1e-3)  # a planted disagreement on one replica
         same = replicas.cross_check(replicas.checksum(grid))
-        q.put((rank, mx, same))
+        # each rank's own autotuner choice; every rank ends with rank 0's
+        mine = {"r32": ((16, 64, 0, 64 * (rank + 1)), 1.0 + rank), "c64": ((8, 32, 128 * rank, 0, rank), None)}
+        agreed = replicas.rank0_tunings(mine)
+        q.put((rank, mx, same, agreed))
     finally:
         dist.destroy_process_group()
 
@@ -66,14 +69,17 @@ def _run(plant: bool):
 
 def test_replicas_agree_and_time_is_max():
     out = _run(plant=False)
-    for rank, mx, same in out:
+    for rank, mx, same, agreed in out:
         assert mx == [2.0, 5.0]
         assert same
+        # rank 0's tunings everywhere (its own "extra" value kept)
+        assert agreed["r32"][0] == (16, 64, 0, 64) and agreed["c64"][0] == (8, 32, 0, 0)
+        assert agreed["r32"][1] == 1.0 + rank
 
 
 def test_cross_check_detects_planted_mismatch():
     out = _run(plant=True)
-    assert all(not same for _, _, same in out)
+    assert all(not same for _, _, same, _ in out)
 
 
 def test_single_process_defaults():
@@ -85,3 +91,4 @@ def test_single_process_defaults():
     assert replicas.world() == (0, 1)
     assert replicas.max_over_ranks([3.0]) == [3.0]
     assert replicas.cross_check(123)
+    assert replicas.rank0_tunings({"r32": ((16, 64, 0, 64), 2.0)}) == {"r32": ((16, 64, 0, 64), 2.0)}
