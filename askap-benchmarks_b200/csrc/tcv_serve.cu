@@ -334,7 +334,7 @@ void tcv_server_config_default(tcv_server_config* c)
     c->max_batch = 32;
     c->batch_samples = 262144;
     c->hbm_budget = size_t(150e9);
-    c->tuning = tcv_tuning{16, 32, 64, 64};
+    c->tuning = tcv_tuning{16, 32, 32, 32};  // 32-sample work units: a request's busy tiles spread over the SMs
     c->device = 0;
 }
 

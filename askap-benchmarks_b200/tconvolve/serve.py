@@ -43,7 +43,7 @@ class Request:
 class Server:
     def __init__(self, g_size: int = 1024, w_size: int = 9, cell_size: float | None = None, baseline: int = 2000,
                  c_type: int | str = "r32", streams: int = 2, max_batch: int = 32, batch_samples: int = 262144,
-                 hbm_budget: float = 150e9, tuning=(16, 32, 64, 64), device: int = 0):
+                 hbm_budget: float = 150e9, tuning=(16, 32, 32, 32), device: int = 0):
         cfg = TcvServerConfig()
         lib().tcv_server_config_default(ctypes.byref(cfg))
         cfg.g_size, cfg.w_size, cfg.baseline = g_size, w_size, baseline

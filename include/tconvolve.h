@@ -265,7 +265,7 @@ typedef struct tcv_server_config {
     int32_t max_batch;     /* requests per batch (default 32, at most 128) */
     int64_t batch_samples; /* samples per batch; also the largest request (default 262144) */
     size_t hbm_budget;     /* device bytes the server may hold (default 150e9) */
-    tcv_tuning tuning;     /* tile shape / plane groups ({0, 0}: defaults) */
+    tcv_tuning tuning;     /* tile shape, plane groups, work units (default {16, 32, 32, 32}) */
     int32_t device;
 } tcv_server_config;
 
