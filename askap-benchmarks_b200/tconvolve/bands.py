@@ -294,3 +294,94 @@ class BandJob:
 
     def rejected(self) -> int:
         return self.plan.rejected() if self.plan is not None else 0
+
+
+def run(steps: int = 5, device="cuda", printer=print, problem: str = "c2", tuning=(16, 64, 0, 64)) -> dict:
+    """tConvolveMPI's flow (attic/tConvolveMPI/tConvolveMPI.cc:78-121) for ONE job split into row
+    bands over the ranks: every rank makes the reference's samples (u, v, w from its generator,
+    data 1+0i, attic/tConvolveMPI/Benchmark.cc:46-80), keeps its contiguous share and hands the
+    rest to their bands' ranks; then `steps` gridding passes and `steps` degridding passes of the
+    whole job, each timed on the device (the slowest rank's time); rank 0 prints the reference's
+    report lines with the job's rates."""
+    import torch
+
+    from . import raw
+    from .replicas import max_over_ranks, world
+    from .workload import PROBLEMS
+
+    rank, n = world()
+    prob = PROBLEMS[problem]
+    freq = torch.tensor([(1.4e9 - 2.0e5 * i / prob.n_chan) / 2.998e8 for i in range(prob.n_chan)],
+                        dtype=torch.float64, device=device)  # Benchmark.cc:86-90
+    u, v, w = raw.init_uvw(prob.n_samples, prob.baseline, 1, device=device)
+    support, os_, wcs, c_len = raw.c_geometry(float(freq[0].item()), prob.cell_size, prob.baseline, prob.w_size)
+    c64, _ = raw.init_c(float(freq[0].item()), prob.cell_size, prob.baseline, prob.w_size, device=device)
+    # the real form of the table: the attic table's imaginary parts are zero, so it gives the
+    # complex64 table's results bit for bit at half the table bytes
+    c, scale, _ = raw.convert_c(c64, _lib.R32)
+    iu, iv, coff = raw.init_offsets(u, v, w, freq, prob.cell_size, wcs, prob.w_size, prob.g_size, support, os_)
+    total = iu.numel()
+    a, e = rank * total // n, (rank + 1) * total // n
+    data = torch.ones(e - a, dtype=torch.complex64, device=device)  # Benchmark.cc:75-78
+    job = BandJob(data, iu[a:e].contiguous(), iv[a:e].contiguous(), coff[a:e].contiguous(), support, prob.g_size,
+                  c_len, comm=DistComm() if n > 1 else SoloComm(), ops=CudaBandOps(device), tuning=tuning)
+    grid = torch.zeros(prob.g_size * prob.g_size, dtype=torch.complex64, device=device)
+    out = torch.empty(e - a, dtype=torch.complex64, device=device)
+    R32 = _lib.R32
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3
+
+    job.grid(grid, c, R32, scale)  # warm-up: the specialised kernels are built at the first pass
+    job.degrid(grid, c, R32, out, scale)
+    torch.cuda.synchronize()
+    t_grid, t_degrid = max_over_ranks([timed(lambda: job.grid(grid, c, R32, scale)),
+                                       timed(lambda: job.degrid(grid, c, R32, out, scale))], device=device)
+    updates = float(total) * (2 * support + 1) ** 2 * steps
+    if rank == 0:
+        for title, t, what in (("Forward", t_grid, "Gridding"), ("Reverse", t_degrid, "Degridding")):
+            printer(f"+++++ {title} processing (row bands) +++++")
+            printer(f"    Number of processes: {n}")
+            printer(f"    Time {t} (s) ")
+            printer(f"    Time per visibility spectral sample {1e6 * t / (total * steps)} (us) ")
+            printer(f"    Time per {what.lower()}   {1e9 * t / updates} (ns) ")
+            printer(f"    {what} rate   {updates / t / 1e6} (million grid points per second)")
+        printer("Done")
+    return {"ranks": n, "rows": job.rows, "grid_s": t_grid, "degrid_s": t_degrid, "updates": updates,
+            "samples_per_rank": job.n_band, "rejected": job.rejected()}
+
+
+def main(argv=None) -> int:
+    """torchrun --nproc-per-node N -m tconvolve.bands [passes]"""
+    import datetime
+    import os
+    import sys
+
+    import torch
+    import torch.distributed as dist
+
+    args = sys.argv[1:] if argv is None else argv
+    if len(args) > 1 or (args and not args[0].isdigit()):
+        print("usage: python -m tconvolve.bands [# of passes]", file=sys.stderr)
+        return 1
+    steps = int(args[0]) if args else 5
+    if "RANK" in os.environ:
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0"))))
+    try:
+        run(steps)
+    finally:
+        if dist.is_initialized():
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

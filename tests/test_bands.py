@@ -478,3 +478,28 @@ def test_band_split_threads_empty_band_and_rejected(tcv, orc, cuda_ok):
     plan.degrid(torch.from_numpy(grid).cuda(), dc, tcv.C64, one)
     assert plan.rejected() == bad.size
     assert np.array_equal(deg, one.cpu().numpy())
+
+
+@pytest.mark.gpu
+def test_bands_program_one_rank(tcv, cuda_ok):
+    """`python -m tconvolve.bands` on one process (one band): the reference's report lines."""
+    import subprocess
+    import sys
+
+    out = subprocess.run([sys.executable, "-m", "tconvolve.bands", "2"], cwd=PKG, capture_output=True, text=True,
+                         timeout=600, check=True).stdout
+    for line in ("+++++ Forward processing (row bands) +++++", "    Number of processes: 1",
+                 "+++++ Reverse processing (row bands) +++++", "Done"):
+        assert line in out.splitlines(), line
+    rates = [float(ln.split()[2]) for ln in out.splitlines() if ln.strip().startswith(("Gridding rate",
+                                                                                     "Degridding rate"))]
+    assert len(rates) == 2 and min(rates) > 1e5  # million grid points per second
+
+
+def test_bands_program_usage():
+    import subprocess
+    import sys
+
+    r = subprocess.run([sys.executable, "-m", "tconvolve.bands", "x"], cwd=PKG, capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 1 and "usage" in r.stderr
