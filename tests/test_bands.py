@@ -503,3 +503,32 @@ def test_bands_program_usage():
     r = subprocess.run([sys.executable, "-m", "tconvolve.bands", "x"], cwd=PKG, capture_output=True, text=True,
                        timeout=120)
     assert r.returncode == 1 and "usage" in r.stderr
+
+
+def test_band_split_one_rank_without_a_process_group(orc):
+    """One band (SoloComm): the split reduces to the plain passes; the oracle stands in for the
+    device."""
+    import sys
+
+    import torch
+
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    from band_helpers import NumpyBandOps
+    from tconvolve.bands import BandJob, SoloComm
+
+    prob = PROBLEMS["g1"]
+    c, support, iu, iv, co = _setup(orc, prob)
+    vis = normal_vis(iu.size, VIS_SEED)
+    t = torch.from_numpy
+    job = BandJob(t(vis.copy()), t(iu.copy()), t(iv.copy()), t(co.copy()), support, prob.g_size, c.size,
+                  comm=SoloComm(), ops=NumpyBandOps(orc, c))
+    assert job.rows == [0, prob.g_size] and job.n_band == iu.size
+    assert job.halo == {"grid_send": [], "grid_recv": [], "fetch_send": [], "fetch_recv": []}
+    grid = torch.zeros(prob.g_size ** 2, dtype=torch.complex64)
+    job.grid(grid, None, 0)
+    ref = np.zeros(prob.g_size ** 2, np.complex64)
+    orc.grid_f32(vis, support, c, co, iu, iv, ref, prob.g_size)
+    assert np.array_equal(grid.numpy(), ref)  # one rank, samples in input order: the reference's sums
+    out = torch.empty(iu.size, dtype=torch.complex64)
+    job.degrid(grid, None, 0, out)
+    assert np.array_equal(out.numpy(), orc.degrid_f32(ref, prob.g_size, support, c, co, iu, iv))
