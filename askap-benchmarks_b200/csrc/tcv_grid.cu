@@ -53,7 +53,9 @@ tcv_status launch(const tcv_plan* p, const float2* data, const void* c, float c_
 {
     const PlanGeom& g = p->g;
     if (g.n == 0) return TCV_OK;
-    const void* spec = kVar ? nullptr : jit_tile_kernel(0, c_type, g.s, kR);
+    const void* spec = kVar ? nullptr
+                       : p->jit_cached_only ? jit_tile_kernel_cached(0, c_type, g.s, kR)
+                                            : jit_tile_kernel(0, c_type, g.s, kR);
     const void* generic = reinterpret_cast<const void*>(&grid_tile_kernel<Tab, 0, kR, kVar>);
     const void* kernel = spec ? spec : generic;
     const int ctas = resident_of(kernel);
@@ -80,7 +82,9 @@ tcv_status launch_adjoint(const tcv_plan* p, const float2* grid, const void* c, 
 {
     const PlanGeom& g = p->g;
     if (g.n == 0) return TCV_OK;
-    const void* spec = kVar ? nullptr : jit_tile_kernel(1, c_type, g.s, kR);
+    const void* spec = kVar ? nullptr
+                       : p->jit_cached_only ? jit_tile_kernel_cached(1, c_type, g.s, kR)
+                                            : jit_tile_kernel(1, c_type, g.s, kR);
     const void* generic = reinterpret_cast<const void*>(&degrid_tile_kernel<Tab, 0, kR, kVar>);
     const void* kernel = spec ? spec : generic;
     const int ctas = resident_of(kernel);

@@ -58,6 +58,8 @@ struct HogArgs {
     int width, psf_width, nblocks;
     long long n;  // width * width
     float gain, threshold;
+    unsigned long long wait_ns;  // persistent loop: limit of one grid-barrier wait
+    unsigned int withheld;       // persistent loop: arrivals the barrier counts that never come (test hook)
 };
 
 __device__ __forceinline__ unsigned int key_index(unsigned long long k) { return ~static_cast<unsigned int>(k); }
@@ -356,7 +358,7 @@ __global__ void __launch_bounds__(kHogThreads, 2) hog_persist_kernel(HogArgs a, 
             vals[blockIdx.x] = bv;
             __threadfence();
             atomicAdd(&st->arrived, 1u);
-            const unsigned int target = unsigned(it + 1) * unsigned(a.nblocks);
+            const unsigned int target = unsigned(it + 1) * unsigned(a.nblocks) + a.withheld;
             ok = 0;
             const unsigned long long t0 = global_ns();
             for (unsigned int spin = 0; spin < (1u << 24); ++spin) {
@@ -366,7 +368,7 @@ __global__ void __launch_bounds__(kHogThreads, 2) hog_persist_kernel(HogArgs a, 
                 }
                 if (*reinterpret_cast<volatile int*>(&st->error)) break;
                 __nanosleep(32);
-                if ((spin & 1023u) == 1023u && global_ns() - t0 > 2000000000ull) break;
+                if ((spin & 63u) == 63u && global_ns() - t0 >= a.wait_ns) break;
             }
             if (!ok) st->error = 1;
             __threadfence();
@@ -395,6 +397,9 @@ size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 // residual + PSF bytes up to which the persistent kernel is chosen (they stay in the 126 MB L2)
 constexpr size_t kPersistBytes = size_t(48) << 20;
 int g_hog_strategy = TCV_HOGBOM_AUTO;
+constexpr unsigned long long kDefaultWaitNs = 2000000000ull;  // 2 s
+unsigned long long g_wait_ns = kDefaultWaitNs;
+unsigned int g_withheld = 0;
 
 int hog_blocks(long long n)
 {
@@ -447,6 +452,8 @@ tcv_status tcv_hogbom_deconvolve(const float* d_dirty, int width, const float* d
     a.nblocks = hog_blocks(a.n);
     a.gain = gain;
     a.threshold = threshold;
+    a.wait_ns = g_wait_ns;
+    a.withheld = g_withheld;
     TCV_CUDA(cudaMemsetAsync(a.state, 0, sizeof(HogState), st));
     // the PSF's peak (HogbomGolden.cc:73-76), then residual = dirty with the first scan (:70)
     const long long np = (long long)psf_width * psf_width;
@@ -496,6 +503,14 @@ tcv_status tcv_hogbom_deconvolve(const float* d_dirty, int width, const float* d
 void tcv_hogbom_set_strategy(int strategy)
 {
     if (strategy >= TCV_HOGBOM_AUTO && strategy <= TCV_HOGBOM_PERSISTENT) g_hog_strategy = strategy;
+}
+
+tcv_status tcv_hogbom_set_wait(uint64_t limit_ns, uint32_t withheld_arrivals)
+{
+    if (limit_ns > kDefaultWaitNs || withheld_arrivals > 1024u) return TCV_ERR_ARG;
+    g_wait_ns = limit_ns;
+    g_withheld = withheld_arrivals;
+    return TCV_OK;
 }
 
 tcv_status tcv_hogbom_result(const void* d_work, int* iters_done, int* stopped_at, int64_t* skipped_rows,

@@ -106,6 +106,7 @@ struct tcv_plan {
     int degrid_variant;            // TCV_DEGRID_TILES or TCV_DEGRID_ANCHOR (reference-layout tables)
     bool batch;                    // jobs carry their own grids (tcv_batch_plan_create)
     bool binned;
+    bool jit_cached_only = false;  // launch specialised tile kernels only if already built (never compile)
     bool anchors_ready = false;    // the anchor binning matches the last binning
     bool anchors_stale = false;    // a captured binning skipped it: anchor degridding re-bins always
     std::vector<tcv::JobDesc> host_jobs;  // the job table (kept alive for its asynchronous copy)
@@ -142,6 +143,8 @@ tcv_status launch_degrid(const tcv_plan* p, const float2* grid, const void* c, i
 // nullptr when no specialised copy is available (the generic copy is used)
 // rows: grid rows per warp (the tile shape)
 const void* jit_tile_kernel(int kind, int c_type, int s, int rows);
+// the same, but only a copy built earlier: never compiles or loads a module (nullptr otherwise)
+const void* jit_tile_kernel_cached(int kind, int c_type, int s, int rows);
 // build both specialised tile kernels of (form, sSize, rows) ahead of a capture or a timing
 void jit_prepare(int c_type, int s, int rows);
 // FFT steps (tcv_fft.cu): fftExec in place; the inverse transform of a grid fused with fftFix into

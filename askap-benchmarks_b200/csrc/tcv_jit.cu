@@ -157,6 +157,14 @@ const void* jit_tile_kernel(int kind, int c_type, int s, int rows)
     return reinterpret_cast<const void*>(build(kind, c_type, s, rows));
 }
 
+const void* jit_tile_kernel_cached(int kind, int c_type, int s, int rows)
+{
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_enabled) return nullptr;
+    const auto it = g_cache.find(std::make_tuple(kind, c_type, s, rows));
+    return it == g_cache.end() ? nullptr : reinterpret_cast<const void*>(it->second);
+}
+
 void jit_prepare(int c_type, int s, int rows)
 {
     std::lock_guard<std::mutex> lock(g_mu);

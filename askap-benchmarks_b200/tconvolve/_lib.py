@@ -195,6 +195,7 @@ SIGNATURES = {
     "tcv_hogbom_deconvolve": (_I, [_P, _I, _P, _I, _P, _P, _I, _F, _F, _P, _P, _P, _S, _P]),
     "tcv_hogbom_result": (_I, [_P, _P, _P, _P, _P, _P]),
     "tcv_hogbom_set_strategy": (None, [_I]),
+    "tcv_hogbom_set_wait": (_I, [ctypes.c_uint64, ctypes.c_uint32]),
     "tcv_find_peak": (_I, [_P, _I64, _P, _P, _P, _S, _P]),
     "tcv_fft_exec": (_I, [_P, _I, _I, _P]),
     "tcv_probe_table_threads": (_I64, []),

@@ -358,11 +358,15 @@ tcv_status tcv_degrid_raw(const float *d_grid, int g_size, int support, const vo
  * reference (its gridders allocate per call, attic/tConvolveCuda/CudaGridder.cc:80-95).
  * Same arguments and result as tcv_grid_raw (grid += gridding of d_data), with the plan's
  * scratch in a fixed device array of tcv_static_scratch_bytes() (64 MiB) that every GPU loading
- * the library holds until exit.  Problems whose plan needs more (tcv_plan_workspace_bytes > that
- * size; about 277 k samples of a 129 x 129 footprint on a 4096 grid) return TCV_ERR_WORKSPACE
- * before any device work.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share the
- * array: calls that overlap on the GPU race and must be serialised by the caller. */
+ * the library holds until exit.  A problem fits when tcv_plan_workspace_bytes(n, support,
+ * g_size, c_len) <= tcv_static_scratch_bytes() (for a 129 x 129 footprint on a 4096 grid with
+ * the 33-plane table: n <= 269,745); larger ones return TCV_ERR_WORKSPACE before any device
+ * work.  The first call in a context of a device (the first on the device, and the first after
+ * a cudaDeviceReset) looks up the array's device address (cudaGetSymbolAddress) and loads the
+ * library's device code there: make it at set-up, before any stream capture.  The call never
+ * compiles or loads a footprint-specialised kernel: it uses one only if tcv_jit_prepare built it
+ * earlier, and the library's generic kernel otherwise (same sums).  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
 size_t tcv_static_scratch_bytes(void);
 tcv_status tcv_grid_raw_static(const float *d_data, int64_t n, int support, const void *d_c,
                                int c_type, float c_scale, int64_t c_len, const int32_t *d_coff,
@@ -574,6 +578,14 @@ tcv_status tcv_hogbom_deconvolve(const float *d_dirty, int width, const float *d
  * force either form.  Results are identical. */
 enum { TCV_HOGBOM_AUTO = 0, TCV_HOGBOM_PER_LAUNCH = 1, TCV_HOGBOM_PERSISTENT = 2 };
 void tcv_hogbom_set_strategy(int strategy);
+/* The bounded waits of the cooperative form (process-wide, for launches made after the call):
+ * limit_ns caps one grid-barrier wait (default and maximum 2e9 ns); withheld_arrivals (default 0)
+ * raises every barrier's arrival target by that many CTAs that never arrive, so that every wait
+ * runs out: a host-side hook that exercises the timeout path (the loop stops, every CTA returns,
+ * tcv_hogbom_result reports TCV_ERR_TIMEOUT) without faulting or hanging the GPU.  Restore (2e9, 0)
+ * afterwards.  The device-side counterpart of the reference's error accounting, which counts
+ * disagreeing values instead of failing (attic/tConvolveBurnIn/tConvolveBurnIn.cc:94-107). */
+tcv_status tcv_hogbom_set_wait(uint64_t limit_ns, uint32_t withheld_arrivals);
 /* After tcv_hogbom_deconvolve (synchronises): iterations done, the iteration that met the
  * threshold (-1 if none), PSF rows skipped, the PSF peak index.  Any output may be NULL.
  * TCV_ERR_TIMEOUT if a grid-barrier wait of the persistent form gave up (the loop stopped). */

@@ -48,8 +48,8 @@ def lib():
                                        _I32, _P, _P, _P]
         L.orc_grid_f32.argtypes = [_P, _I64, _I32, _P, _P, _P, _P, _P, _I32, _I32]
         L.orc_degrid_f32.argtypes = [_P, _I32, _I32, _P, _P, _P, _P, _P, _I64, _I32]
-        L.orc_grid_f64.argtypes = [_P, _I64, _I32, _P, _P, _P, _P, _P, _I32]
-        L.orc_degrid_f64.argtypes = [_P, _I32, _I32, _P, _P, _P, _P, _P, _I64]
+        L.orc_grid_f64.argtypes = [_P, _I64, _I32, _P, _P, _P, _P, _P, _I32, _I32]
+        L.orc_degrid_f64.argtypes = [_P, _I32, _I32, _P, _P, _P, _P, _P, _I64, _I32]
         L.orc_cur_geometry.argtypes = [_I32, _P]
         L.orc_cur_init_uvw.argtypes = [_I32, _P, _P, _P, _P]
         L.orc_cur_init_c.argtypes = [_I32, _P, _P, _P]
@@ -176,19 +176,21 @@ def degrid_f32(grid, g_size, support, c, coff, iu, iv, threads: int = 1):
     return out
 
 
-def grid_f64(data, support, c64, coff, iu, iv, grid64, g_size):
-    """FP64 gridding (complex128 data and grid, real float64 table). In place."""
+def grid_f64(data, support, c64, coff, iu, iv, grid64, g_size, threads: int = 1):
+    """FP64 gridding (complex128 data and grid, real float64 table). In place; the same result
+    for any thread count (each thread owns a band of rows and walks the samples in order)."""
     data = np.ascontiguousarray(data, np.complex128)
     assert grid64.dtype == np.complex128
     lib().orc_grid_f64(_p(data), data.size, support, _p(c64), _p(coff), _p(iu), _p(iv),
-                       _p(grid64), g_size)
+                       _p(grid64), g_size, threads)
     return grid64
 
 
-def degrid_f64(grid64, g_size, support, c64, coff, iu, iv):
+def degrid_f64(grid64, g_size, support, c64, coff, iu, iv, threads: int = 1):
     n = iu.size
     out = np.empty(n, np.complex128)
-    lib().orc_degrid_f64(_p(grid64), g_size, support, _p(c64), _p(coff), _p(iu), _p(iv), _p(out), n)
+    lib().orc_degrid_f64(_p(grid64), g_size, support, _p(c64), _p(coff), _p(iu), _p(iv), _p(out), n,
+                         threads)
     return out
 
 
@@ -209,10 +211,10 @@ def run_plain(cfg: Config, vis: np.ndarray | None = None, threads: int = 1, want
                sum_c=sum_c, iu=iu, iv=iv, coff=co, data=data, grid=grid, outdata=out)
     if want_f64:
         g64 = np.zeros(cfg.g_size * cfg.g_size, np.complex128)
-        grid_f64(data.astype(np.complex128), support, c64, co, iu, iv, g64, cfg.g_size)
+        grid_f64(data.astype(np.complex128), support, c64, co, iu, iv, g64, cfg.g_size, threads)
         res["C64"] = c64
         res["grid64"] = g64
-        res["outdata64"] = degrid_f64(g64, cfg.g_size, support, c64, co, iu, iv)
+        res["outdata64"] = degrid_f64(g64, cfg.g_size, support, c64, co, iu, iv, threads)
     return res
 
 

@@ -314,42 +314,82 @@ void orc_degrid_f32(const float *grid, int g_size, int support, const float *c,
  * Benchmark.cc:125-195, with a real double table (the attic table has zero imaginary part),
  * complex double data and a complex double grid (interleaved).
  * ------------------------------------------------------------------------------------------- */
-void orc_grid_f64(const double *data, int64_t n, int support, const double *c_real,
-                  const int32_t *coff, const int32_t *iu, const int32_t *iv,
-                  double *grid, int g_size)
+typedef struct {
+    const double *data, *c_real;
+    const int32_t *iu, *iv, *coff;
+    int64_t n;
+    int support, g_size;
+    double *grid;
+    int row_lo, row_hi;
+} orc_grid64_job;
+
+/* Rows [row_lo, row_hi) of the grid, every sample in input order (as orc_grid_rows): each point
+ * sees the same additions in the same order for any thread count. */
+static void *orc_grid64_rows(void *arg)
 {
-    const int s = 2 * support + 1;
-    const int64_t g = g_size;
-    for (int64_t d = 0; d < n; ++d) {
-        const double dr = data[2 * d], di = data[2 * d + 1];
-        int64_t gind = iu[d] + g * iv[d] - support;
-        int64_t cind = coff[d];
-        for (int sv = 0; sv < s; ++sv) {
-            double *gp = grid + 2 * gind;
-            const double *cp = c_real + cind;
+    const orc_grid64_job *jb = (const orc_grid64_job *)arg;
+    const int s = 2 * jb->support + 1;
+    const int64_t g = jb->g_size;
+    for (int64_t d = 0; d < jb->n; ++d) {
+        const double dr = jb->data[2 * d], di = jb->data[2 * d + 1];
+        const int iv = jb->iv[d];
+        int r0 = iv > jb->row_lo ? iv : jb->row_lo;
+        int r1 = iv + s < jb->row_hi ? iv + s : jb->row_hi;
+        for (int row = r0; row < r1; ++row) {
+            double *gp = jb->grid + 2 * ((int64_t)row * g + jb->iu[d] - jb->support);
+            const double *cp = jb->c_real + (int64_t)jb->coff[d] + (int64_t)(row - iv) * s;
             for (int x = 0; x < s; ++x) {
                 gp[2 * x] += dr * cp[x];
                 gp[2 * x + 1] += di * cp[x];
             }
-            gind += g;
-            cind += s;
         }
     }
+    return NULL;
 }
 
-void orc_degrid_f64(const double *grid, int g_size, int support, const double *c_real,
-                    const int32_t *coff, const int32_t *iu, const int32_t *iv,
-                    double *out, int64_t n)
+void orc_grid_f64(const double *data, int64_t n, int support, const double *c_real,
+                  const int32_t *coff, const int32_t *iu, const int32_t *iv,
+                  double *grid, int g_size, int n_threads)
 {
-    const int s = 2 * support + 1;
-    const int64_t g = g_size;
-    for (int64_t d = 0; d < n; ++d) {
+    if (n_threads < 1) n_threads = 1;
+    orc_grid64_job *jobs = (orc_grid64_job *)calloc((size_t)n_threads, sizeof(orc_grid64_job));
+    pthread_t *th = (pthread_t *)calloc((size_t)n_threads, sizeof(pthread_t));
+    for (int t = 0; t < n_threads; ++t) {
+        orc_grid64_job jb = {data, c_real, iu, iv, coff, n, support, g_size, grid,
+                             (int)((int64_t)g_size * t / n_threads),
+                             (int)((int64_t)g_size * (t + 1) / n_threads)};
+        jobs[t] = jb;
+    }
+    if (n_threads == 1) {
+        orc_grid64_rows(&jobs[0]);
+    } else {
+        for (int t = 0; t < n_threads; ++t) pthread_create(&th[t], NULL, orc_grid64_rows, &jobs[t]);
+        for (int t = 0; t < n_threads; ++t) pthread_join(th[t], NULL);
+    }
+    free(jobs);
+    free(th);
+}
+
+typedef struct {
+    const double *grid, *c_real;
+    const int32_t *iu, *iv, *coff;
+    int64_t lo, hi;
+    int support, g_size;
+    double *out;
+} orc_degrid64_job;
+
+static void *orc_degrid64_range(void *arg)
+{
+    const orc_degrid64_job *jb = (const orc_degrid64_job *)arg;
+    const int s = 2 * jb->support + 1;
+    const int64_t g = jb->g_size;
+    for (int64_t d = jb->lo; d < jb->hi; ++d) {
         double ar = 0.0, ai = 0.0;
-        int64_t gind = iu[d] + g * iv[d] - support;
-        int64_t cind = coff[d];
+        int64_t gind = jb->iu[d] + g * jb->iv[d] - jb->support;
+        int64_t cind = jb->coff[d];
         for (int sv = 0; sv < s; ++sv) {
-            const double *gp = grid + 2 * gind;
-            const double *cp = c_real + cind;
+            const double *gp = jb->grid + 2 * gind;
+            const double *cp = jb->c_real + cind;
             for (int x = 0; x < s; ++x) {
                 ar += gp[2 * x] * cp[x];
                 ai += gp[2 * x + 1] * cp[x];
@@ -357,7 +397,30 @@ void orc_degrid_f64(const double *grid, int g_size, int support, const double *c
             gind += g;
             cind += s;
         }
-        out[2 * d] = ar;
-        out[2 * d + 1] = ai;
+        jb->out[2 * d] = ar;
+        jb->out[2 * d + 1] = ai;
     }
+    return NULL;
+}
+
+void orc_degrid_f64(const double *grid, int g_size, int support, const double *c_real,
+                    const int32_t *coff, const int32_t *iu, const int32_t *iv,
+                    double *out, int64_t n, int n_threads)
+{
+    if (n_threads < 1) n_threads = 1;
+    orc_degrid64_job *jobs = (orc_degrid64_job *)calloc((size_t)n_threads, sizeof(orc_degrid64_job));
+    pthread_t *th = (pthread_t *)calloc((size_t)n_threads, sizeof(pthread_t));
+    for (int t = 0; t < n_threads; ++t) {
+        orc_degrid64_job jb = {grid, c_real, iu, iv, coff, n * t / n_threads, n * (t + 1) / n_threads,
+                               support, g_size, out};
+        jobs[t] = jb;
+    }
+    if (n_threads == 1) {
+        orc_degrid64_range(&jobs[0]);
+    } else {
+        for (int t = 0; t < n_threads; ++t) pthread_create(&th[t], NULL, orc_degrid64_range, &jobs[t]);
+        for (int t = 0; t < n_threads; ++t) pthread_join(th[t], NULL);
+    }
+    free(jobs);
+    free(th);
 }

@@ -134,3 +134,53 @@ def test_persistent_and_per_launch_forms_agree(tcv, orc, cuda_ok, width):
     assert np.array_equal(m1, m2) and np.array_equal(r1, r2) and np.array_equal(p1, p2) and np.array_equal(v1, v2)
     o = orc.hogbom(dirty, psf, 400, 0.1, 1e-5)
     assert np.array_equal(m2, o["model"]) and np.array_equal(r2, o["residual"])
+
+
+@pytest.mark.parametrize("limit_ns", [0, 1_000_000])
+def test_barrier_timeout_path(tcv, orc, cuda_ok, limit_ns):
+    """The cooperative loop's bounded grid-barrier wait, made to run out on purpose: the barrier
+    is told to expect one CTA more than the launch has (an arrival nothing makes), with a short
+    limit.  Every CTA must give up, flag the error and return (the launch ends), the loop must stop
+    after its first iteration and tcv_hogbom_result must report TCV_ERR_TIMEOUT.  With the default
+    wait restored, the next run on the same workspace is the oracle's bit for bit."""
+    import ctypes
+
+    import torch
+
+    from tconvolve._lib import lib
+    from tconvolve.hogbom import Workspace, deconvolve_device
+    from tconvolve.workload import synthetic_dirty, synthetic_psf
+
+    w = 1024
+    dirty, psf = synthetic_dirty(w, 15, 1e-3, seed=21), synthetic_psf(w)
+    d = torch.from_numpy(dirty.ravel()).cuda()
+    p = torch.from_numpy(psf.ravel()).cuda()
+    m = torch.zeros_like(d)
+    r = torch.empty_like(d)
+    ws = Workspace(w)
+    L = lib()
+    assert L.tcv_hogbom_set_wait(3_000_000_000, 0) == 1  # above the 2 s cap: TCV_ERR_ARG
+    try:
+        L.tcv_hogbom_set_strategy(2)  # TCV_HOGBOM_PERSISTENT
+        assert L.tcv_hogbom_set_wait(limit_ns, 1) == 0
+        deconvolve_device(d, w, p, w, m, r, 200, 0.1, 0.0, work=ws)
+        torch.cuda.synchronize()  # returns: every CTA left the kernel
+        done, stop = ctypes.c_int(), ctypes.c_int()
+        st = L.tcv_hogbom_result(ctypes.c_void_p(ws.buf.data_ptr()), ctypes.byref(done), ctypes.byref(stop), None,
+                                 None, None)
+        assert st == 5  # TCV_ERR_TIMEOUT
+        assert done.value == 1 and stop.value == -1
+    finally:
+        L.tcv_hogbom_set_wait(2_000_000_000, 0)
+        L.tcv_hogbom_set_strategy(0)
+    # the context is still usable and the next run is the reference's
+    L.tcv_hogbom_set_strategy(2)
+    try:
+        m.zero_()
+        deconvolve_device(d, w, p, w, m, r, 200, 0.1, 0.0, work=ws)
+        res = ws.result()
+    finally:
+        L.tcv_hogbom_set_strategy(0)
+    o = orc.hogbom(dirty, psf, 200, 0.1, 0.0)
+    assert res["done"] == o["done"] == 200
+    assert np.array_equal(m.cpu().numpy(), o["model"]) and np.array_equal(r.cpu().numpy(), o["residual"])
