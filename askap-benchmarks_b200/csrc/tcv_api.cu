@@ -111,7 +111,7 @@ tcv_status ensure_tables(tcv_ctx* c)
         c->c_pad_type = want;
         return TCV_OK;
     }
-    tcv::jit_prepare(t, 2 * c->support + 1, c->tuning.tile_rows);  // the direct path's tile kernels, specialised on sSize
+    tcv::jit_prepare(t, 2 * c->support + 1, c->tuning.tile_rows, tcv::tuning_stages(c->tuning));  // the direct path's tile kernels, specialised on sSize
     if (t == TCV_C_C64 || c->c_alt_type == t) return TCV_OK;
     if (c->c_alt) {
         CTX_CUDA(c, cudaStreamSynchronize(c->stream));

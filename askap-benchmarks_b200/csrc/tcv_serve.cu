@@ -395,7 +395,7 @@ tcv_status tcv_server_create(const tcv_server_config* cfg, tcv_server** out)
         free_server(s);
         return st;
     }
-    tcv::jit_prepare(ct, 2 * s->support + 1, c.tuning.tile_rows);
+    tcv::jit_prepare(ct, 2 * s->support + 1, c.tuning.tile_rows, tcv::tuning_stages(c.tuning));
     // batch slots, admitted against the budget
     const size_t work = slot_work_bytes(s);
     if (work == 0 || s->held + size_t(c.streams) * slot_bytes(c, work) > c.hbm_budget) {
