@@ -111,7 +111,7 @@ tcv_status ensure_tables(tcv_ctx* c)
         c->c_pad_type = want;
         return TCV_OK;
     }
-    tcv::jit_prepare(t, 2 * c->support + 1, c->tuning.tile_rows, tcv::tuning_stages(c->tuning));  // the direct path's tile kernels, specialised on sSize
+    tcv::jit_prepare(t, 2 * c->support + 1, c->tuning.tile_rows);  // the direct path's tile kernels, specialised on sSize
     if (t == TCV_C_C64 || c->c_alt_type == t) return TCV_OK;
     if (c->c_alt) {
         CTX_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -329,9 +329,10 @@ tcv_status tcv_set_tuning(tcv_ctx* c, const tcv_tuning* t)
 {
     if (!c || !t) return TCV_ERR_ARG;
     const tcv_tuning nt{t->tile_rows ? t->tile_rows : 16, t->group_mib ? t->group_mib : 32, t->split,
-                        t->degrid_split};
+                        t->degrid_split, t->kernel};
+    // the sample-parallel kernel bits belong to variable-width plans: a context's plan has one width
     if ((nt.tile_rows != 8 && nt.tile_rows != 16 && nt.tile_rows != 32) || nt.group_mib < -1 || nt.split < 0 ||
-        nt.degrid_split < 0)
+        nt.degrid_split < 0 || nt.kernel != 0)
         return TCV_ERR_ARG;
     const tcv_tuning prev = c->tuning;
     c->tuning = nt;

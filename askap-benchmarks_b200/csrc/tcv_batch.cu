@@ -86,8 +86,7 @@ tcv_status tcv_graph_capture(tcv_graph** graph_out, tcv_plan* plan, int passes, 
     if (!(passes & TCV_PASS_BIN) && !plan->binned) return TCV_ERR_STATE;
     if (plan->batch ? d_grid != nullptr : d_grid == nullptr) return TCV_ERR_ARG;
     if ((passes & TCV_PASS_DEGRID) && plan->g.n > 0 && !d_vis) return TCV_ERR_ARG;
-    if (!(c_type & (TCV_C_PADDED | TCV_C_PAIRED)))
-        jit_prepare(c_type, plan->g.s, plan->g.rows, plan->g.staged ? plan->g.stage_ns : 0);
+    if (!(c_type & (TCV_C_PADDED | TCV_C_PAIRED))) jit_prepare(c_type, plan->g.s, plan->g.rows);
     tcv_graph* g = new (std::nothrow) tcv_graph{};
     if (!g) return TCV_ERR_OOM;
     cudaStream_t cs = nullptr;
@@ -236,7 +235,7 @@ tcv_status tcv_autotune(const tcv_job* jobs, int n_jobs, const int32_t* d_iu, co
             if (a != TCV_OK) return a;
             have = need;
         }
-        jit_prepare(c_type, 2 * support + 1, t.tile_rows, tuning_stages(t));
+        jit_prepare(c_type, 2 * support + 1, t.tile_rows);
         tcv_plan* plan = nullptr;
         tcv_status r = tcv_batch_plan_create(&plan, sub.data(), int(sub.size()), support, c_len, &t, work.p, have, st);
         if (r != TCV_OK) return r;

@@ -78,22 +78,20 @@ struct TabC64 {
     static constexpr bool kReal = false;
     using elem = float2;
     __device__ __forceinline__ static float2 load(const elem* p) { return __ldg(p); }
-    __device__ __forceinline__ static float2 cvt(const elem e) { return e; }
 };
 struct TabR32 {
     static constexpr int kMinBlocks = 4;
     static constexpr bool kReal = true;
     using elem = float;
     __device__ __forceinline__ static float2 load(const elem* p) { return make_float2(__ldg(p), 0.f); }
-    __device__ __forceinline__ static float2 cvt(const elem e) { return make_float2(e, 0.f); }
 };
 struct TabCBF16 {
     static constexpr int kMinBlocks = 3;
     static constexpr bool kReal = false;
     using elem = u32;  // (re, im) bfloat16 pair, re in the low half
-    __device__ __forceinline__ static float2 load(const elem* p) { return cvt(__ldg(p)); }
-    __device__ __forceinline__ static float2 cvt(const elem u)
+    __device__ __forceinline__ static float2 load(const elem* p)
     {
+        const u32 u = __ldg(p);
         return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
     }
 };
@@ -176,6 +174,7 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
     __shared__ float4 sm_rec[2][kTileChunk];  // (data.re, data.im, first column, first row)
     __shared__ int sm_coff[2][kTileChunk];
     __shared__ int sm_w[kVar ? 2 : 1][kVar ? kTileChunk : 1];  // per-sample widths
+    __shared__ unsigned char sm_mask[2][kTileChunk];  // per sample: the warps whose blocks it meets
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
     const u32 i1 = group_ustart[a.group + 1];
@@ -184,11 +183,25 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
             const u32 k = order[c.start + c.base + threadIdx.x];
             const float2 d = data[k];
             const int sk = kVar ? int(a.ssz[k]) : s0;
-            sm_rec[buf][threadIdx.x] = make_float4(d.x * a.c_scale, d.y * a.c_scale,
-                                                   __int_as_float(iu[k] - (kVar ? sk / 2 : a.support)),
-                                                   __int_as_float(iv[k]));
+            const int fx = iu[k] - (kVar ? sk / 2 : a.support), fy = iv[k];
+            sm_rec[buf][threadIdx.x] = make_float4(d.x * a.c_scale, d.y * a.c_scale, __int_as_float(fx),
+                                                   __int_as_float(fy));
             sm_coff[buf][threadIdx.x] = coff[k];
             if (kVar) sm_w[kVar ? buf : 0][kVar ? threadIdx.x : 0] = sk;
+            // warp w's block: columns tx*64 + (w % 2)*32 + [0, 32), rows ty*kTH + (w / 2)*kR + [0, kR)
+            const int bx = rec_tx(c.ti) * kTileW - fx, by = rec_ty(c.ti) * kTH - fy;
+            u32 cols = 0, rows = 0;
+#pragma unroll
+            for (int h = 0; h < kTileW / 32; ++h)
+                cols |= u32(bx + h * 32 < sk && bx + h * 32 + 32 > 0) << h;
+#pragma unroll
+            for (int r = 0; r < kTileWarps / (kTileW / 32); ++r)
+                rows |= u32(by + r * kR < sk && by + r * kR + kR > 0) << r;
+            u32 m = 0;
+#pragma unroll
+            for (int w = 0; w < kTileWarps; ++w)
+                m |= (((cols >> (w % (kTileW / 32))) & (rows >> (w / (kTileW / 32)))) & 1u) << w;
+            sm_mask[buf][threadIdx.x] = (unsigned char)m;
         }
     };
     ChunkCursor cur;
@@ -208,13 +221,16 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
         const int bx0 = tx * kTileW + (warp % (kTileW / 32)) * 32;  // first column of this warp
         const int gx = bx0 + lane;
         const int gy0 = ty * kTH + (warp / (kTileW / 32)) * kR;
-        for (int j = 0; j < cur.m; ++j) {
+        // the chunk's samples that meet this warp's block, in order: one ballot per 32 samples
+        for (int e = 0; e < cur.m; e += 32) {
+            u32 bits = __ballot_sync(0xffffffffu, e + lane < cur.m && ((sm_mask[buf][e + lane] >> warp) & 1u));
+            while (bits) {
+            const int j = e + __ffs(bits) - 1;
+            bits &= bits - 1;
             const float4 q = sm_rec[buf][j];
             const int s = kVar ? sm_w[kVar ? buf : 0][kVar ? j : 0] : s0;
             const int fx = __float_as_int(q.z), fy = __float_as_int(q.w);
-            const int dy0 = gy0 - fy;  // footprint row of this warp's first row
-            if (dy0 >= s || dy0 + kR <= 0) continue;      // warp-uniform
-            if (fx > bx0 + 31 || fx + s <= bx0) continue;  // warp-uniform
+            const int dy0 = gy0 - fy;  // footprint row of this warp's first row (the block meets the footprint)
             const int dx = gx - fx;
             const bool colok = unsigned(dx) < unsigned(s);
             const float2 dv = make_float2(q.x, q.y);
@@ -234,6 +250,7 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
                         cmac<Tab::kReal>(acc[r], dv, c);
                     }
                 }
+            }
             }
         }
         if ((nxt.it != cur.it || nxt.m == 0) && cur.pslot != kDirect) {

@@ -9,13 +9,12 @@ namespace tcv {
 namespace {
 
 // CTAs of a persistent launch: every SM filled to the kernel's occupancy
-int resident_of(const void* kernel, int smem = 0)
+int resident_of(const void* kernel)
 {
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTileThreads, size_t(smem)) != cudaSuccess ||
-        per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTileThreads, 0) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     return per_sm * sms;
 }
@@ -77,46 +76,6 @@ tcv_status launch(const tcv_plan* p, const float2* data, const void* c, float c_
     return TCV_OK;
 }
 
-// Staged gridding (grid_stage_kernel): the same launches and folds, with the rings in dynamic
-// shared memory.
-template <class Tab, int kR, int kNS>
-tcv_status launch_staged(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
-                         cudaStream_t st, int c_type)
-{
-    const PlanGeom& g = p->g;
-    if (g.n == 0) return TCV_OK;
-    const void* spec = p->jit_cached_only ? jit_tile_kernel_cached(2, c_type, g.s, kR, kNS)
-                                          : jit_tile_kernel(2, c_type, g.s, kR, kNS);
-    const void* generic = reinterpret_cast<const void*>(&grid_stage_kernel<Tab, 0, kR, kNS>);
-    const void* kernel = spec ? spec : generic;
-    constexpr int smem = stage_smem_bytes<Tab, kR, kNS>();
-    TCV_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    TCV_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    const int ctas = resident_of(kernel, smem);
-    const typename Tab::elem* tab = static_cast<const typename Tab::elem*>(c);
-    const unsigned int* order = p->vals[p->sel];
-    for (int grp = 0; grp < g.n_groups; ++grp) {
-        GridArgs a = make_args(p, grp, c_scale, grid);
-        void* args[] = {&data, &tab, const_cast<const int32_t**>(&p->iu), const_cast<const int32_t**>(&p->iv),
-                        const_cast<const int32_t**>(&p->coff), &order, const_cast<uint4**>(&p->units),
-                        const_cast<uint32_t**>(&p->group_ustart), &a};
-        TCV_CUDA(cudaLaunchKernel(kernel, dim3(ctas), dim3(kTileThreads), args, size_t(smem), st));
-        if (g.split) {
-            fold_kernel<kR><<<fold_ctas(), kTileThreads, 0, st>>>(p->items, p->group_start, p->nunits, p->pstart, a);
-            TCV_CUDA(cudaGetLastError());
-        }
-    }
-    return TCV_OK;
-}
-
-template <class Tab, int kR>
-tcv_status launch_staged_ns(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
-                            cudaStream_t st, int c_type)
-{
-    if (p->g.stage_ns == 3) return launch_staged<Tab, kR, 3>(p, data, c, c_scale, grid, st, c_type);
-    return launch_staged<Tab, kR, 2>(p, data, c, c_scale, grid, st, c_type);
-}
-
 template <class Tab, int kR, bool kVar = false>
 tcv_status launch_adjoint(const tcv_plan* p, const float2* grid, const void* c, float c_scale, float2* out,
                           cudaStream_t st, int c_type)
@@ -167,16 +126,6 @@ tcv_status grid_rows(const tcv_plan* p, const float2* data, const void* c, float
         return TCV_ERR_UNSUPPORTED;
     }
     if (p->g.dense || p->g.ddense) return TCV_ERR_UNSUPPORTED;  // sample-parallel kernels: variable-width plans only
-    if (p->g.staged) {
-        if constexpr (sizeof(typename Tab::elem) == 4 || sizeof(typename Tab::elem) == 8) {
-            switch (p->g.rows) {
-                case 8: return launch_staged_ns<Tab, 8>(p, data, c, c_scale, grid, st, c_type);
-                case 16: return launch_staged_ns<Tab, 16>(p, data, c, c_scale, grid, st, c_type);
-                default: return TCV_ERR_UNSUPPORTED;
-            }
-        }
-        return TCV_ERR_UNSUPPORTED;  // 2-byte table entries: cp.async copies 4, 8 or 16 bytes
-    }
     switch (p->g.rows) {
         case 8: return launch<Tab, 8>(p, data, c, c_scale, grid, st, c_type);
         case 16: return launch<Tab, 16>(p, data, c, c_scale, grid, st, c_type);

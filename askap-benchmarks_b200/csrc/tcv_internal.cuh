@@ -20,7 +20,6 @@ struct TabCF16 {
     static constexpr bool kReal = false;
     using elem = __half2;
     __device__ __forceinline__ static float2 load(const elem* p) { return __half22float2(__ldg(p)); }
-    __device__ __forceinline__ static float2 cvt(const elem e) { return __half22float2(e); }
 };
 struct TabRF16 {
     static constexpr int kMinBlocks = 4;
@@ -49,8 +48,6 @@ struct PlanGeom {
     int dsplit;         // the same for degridding
     bool dense;         // variable-width plans: sample-parallel gridding kernel (tcv_dense.cu)
     bool ddense;        // variable-width plans: sample-parallel degridding kernel
-    bool staged;        // fixed-width plans: gridding through cp.async shared-memory rings
-    int stage_ns;       // stages per warp ring of the staged kernels (2 or 3)
     int ntx, nty;       // tiles per row / column of a one-job plan
     int64_t ntiles;     // tiles of all jobs
     int max_tiles;      // tiles one footprint can touch
@@ -145,17 +142,16 @@ tcv_status launch_degrid(const tcv_plan* p, const float2* grid, const void* c, i
 // tile kernels specialised on the footprint width (tcv_jit.cu): kind 0 gridding, 1 degridding;
 // nullptr when no specialised copy is available (the generic copy is used)
 // rows: grid rows per warp (the tile shape)
-// kind 0 gridding, 1 degridding, 2 staged gridding (stages: its ring depth)
-const void* jit_tile_kernel(int kind, int c_type, int s, int rows, int stages = 0);
+const void* jit_tile_kernel(int kind, int c_type, int s, int rows);
 // the same, but only a copy built earlier: never compiles or loads a module (nullptr otherwise)
-const void* jit_tile_kernel_cached(int kind, int c_type, int s, int rows, int stages = 0);
+const void* jit_tile_kernel_cached(int kind, int c_type, int s, int rows);
 // build both specialised tile kernels of (form, sSize, rows) ahead of a capture or a timing
-void jit_prepare(int c_type, int s, int rows, int stages = 0);
-// ring depth of the staged gridding kernel a tuning selects (0: not staged)
-inline int tuning_stages(const tcv_tuning& t) { return (t.kernel & 4) ? ((t.kernel & 16) ? 3 : 2) : 0; }
+void jit_prepare(int c_type, int s, int rows);
 // FFT steps (tcv_fft.cu): fftExec in place; the inverse transform of a grid fused with fftFix into
 // a float image (and/or a complex one); the forward transform of a real image into a grid.
 tcv_status fft_exec(float2* d_grid, int n, bool forward, cudaStream_t st);
+// the set-up of the transforms of size n (twiddle table; allocates): before any capture
+tcv_status fft_prepare(int n);
 tcv_status image_from_grid(float2* d_grid, int n, float scale, float* d_image, float2* d_image_c, cudaStream_t st);
 tcv_status grid_from_image(const float* d_image, int n, float2* d_grid, cudaStream_t st);
 // Sample-parallel kernels of variable-width plans on 64 x 32 tiles (tcv_dense.cu).

@@ -46,8 +46,8 @@ NvrtcApi g_api;
 bool g_api_tried = false;
 bool g_enabled = true;
 std::string g_info = "no specialised kernel built yet";
-std::map<std::tuple<int, int, int, int, int>, cudaKernel_t> g_cache;  // (kind, c_type, sSize, rows, stages) -> kernel
-std::map<std::tuple<int, int, int, int, int>, bool> g_failed;
+std::map<std::tuple<int, int, int, int>, cudaKernel_t> g_cache;  // (kind, c_type, sSize, rows) -> kernel
+std::map<std::tuple<int, int, int, int>, bool> g_failed;
 
 bool load_api()
 {
@@ -89,22 +89,19 @@ const char* tab_name(int c_type)
 }
 
 // Build (or fetch) the specialised kernel; nullptr if unavailable.  Caller holds g_mu.
-cudaKernel_t build(int kind, int c_type, int s, int rows, int stages = 0)
+cudaKernel_t build(int kind, int c_type, int s, int rows)
 {
-    if (kind != 2) stages = 0;
-    const auto key = std::make_tuple(kind, c_type, s, rows, stages);
+    const auto key = std::make_tuple(kind, c_type, s, rows);
     auto it = g_cache.find(key);
     if (it != g_cache.end()) return it->second;
     if (g_failed.count(key)) return nullptr;
     const char* tab = tab_name(c_type);
-    if (!tab || s < 1 || s > 4096 || (rows != 8 && rows != 16 && rows != 32) || kind < 0 || kind > 2 ||
-        (kind == 2 && stages != 2 && stages != 3) || (kind == 2 && c_type == TCV_C_RBF16) || !load_api()) {
+    if (!tab || s < 1 || s > 4096 || (rows != 8 && rows != 16 && rows != 32) || !load_api()) {
         g_failed[key] = true;
         return nullptr;
     }
-    static const char* const kNames[] = {"tcv::grid_tile_kernel<", "tcv::degrid_tile_kernel<", "tcv::grid_stage_kernel<"};
-    const std::string expr = std::string(kNames[kind]) + tab + ", " + std::to_string(s) + ", " + std::to_string(rows) +
-                             (kind == 2 ? ", " + std::to_string(stages) : std::string()) + ">";
+    const std::string expr = std::string(kind == 0 ? "tcv::grid_tile_kernel<" : "tcv::degrid_tile_kernel<") + tab +
+                             ", " + std::to_string(s) + ", " + std::to_string(rows) + ">";
     const std::string body = "#include \"tcv_device.cuh\"\n";
     const char* hdr_src[] = {kDeviceSrc};
     const char* hdr_name[] = {"tcv_device.cuh"};
@@ -153,28 +150,27 @@ cudaKernel_t build(int kind, int c_type, int s, int rows, int stages = 0)
 
 }  // namespace
 
-const void* jit_tile_kernel(int kind, int c_type, int s, int rows, int stages)
+const void* jit_tile_kernel(int kind, int c_type, int s, int rows)
 {
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_enabled) return nullptr;
-    return reinterpret_cast<const void*>(build(kind, c_type, s, rows, stages));
+    return reinterpret_cast<const void*>(build(kind, c_type, s, rows));
 }
 
-const void* jit_tile_kernel_cached(int kind, int c_type, int s, int rows, int stages)
+const void* jit_tile_kernel_cached(int kind, int c_type, int s, int rows)
 {
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_enabled) return nullptr;
-    const auto it = g_cache.find(std::make_tuple(kind, c_type, s, rows, kind == 2 ? stages : 0));
+    const auto it = g_cache.find(std::make_tuple(kind, c_type, s, rows));
     return it == g_cache.end() ? nullptr : reinterpret_cast<const void*>(it->second);
 }
 
-void jit_prepare(int c_type, int s, int rows, int stages)
+void jit_prepare(int c_type, int s, int rows)
 {
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_enabled) return;
     build(0, c_type & 0xff, s, rows);
     build(1, c_type & 0xff, s, rows);
-    if (stages) build(2, c_type & 0xff, s, rows, stages);
 }
 
 }  // namespace tcv

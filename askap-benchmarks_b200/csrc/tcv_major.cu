@@ -265,6 +265,7 @@ tcv_status tcv_major_init(tcv_major_ctx* c)
     c->plan_bytes = tcv_plan_workspace_bytes_tuned(c->n, c->support, N, c->c_len, &g.tuning);
     if (c->plan_bytes == 0) return mfail(c, TCV_ERR_UNSUPPORTED, "plan geometry");
     MAJ_CUDA(c, cudaMalloc(&c->plan_work, c->plan_bytes));
+    MAJ_TRY(c, tcv::fft_prepare(N));  // the transforms' twiddle table, made here rather than mid-cycle
     MAJ_TRY(c, tcv_plan_build_tuned(&c->plan, c->iu, c->iv, c->coff, c->n, c->support, N, c->c_len, &g.tuning,
                                     c->plan_work, c->plan_bytes, st));
     int64_t rej = 0;

@@ -661,10 +661,7 @@ bool valid_tuning(const tcv_tuning* t)
 {
     if (!t) return true;
     const bool rows_ok = t->tile_rows == 0 || t->tile_rows == 8 || t->tile_rows == 16 || t->tile_rows == 32;
-    // bits 1, 2: sample-parallel kernels of variable-width plans (8-row tiles); 4: staged gridding
-    // of fixed-width plans, 16: with three-stage rings
-    const bool kernel_ok = (t->kernel & ~(1 | 2 | 4 | 16)) == 0 && (!(t->kernel & 3) || t->tile_rows == 8) &&
-                           (!(t->kernel & 16) || (t->kernel & 4));
+    const bool kernel_ok = t->kernel == 0 || (t->kernel >= 1 && t->kernel <= 3 && t->tile_rows == 8);
     return rows_ok && kernel_ok && t->group_mib >= -1 && t->split >= 0 && t->split <= (1 << 24) &&
            t->degrid_split >= 0 && t->degrid_split <= (1 << 24);
 }
@@ -814,8 +811,6 @@ PlanGeom make_geom(int64_t n, int support, const int* g_sizes, int n_jobs, int64
     g.dsplit = t ? t->degrid_split : 0;
     g.dense = t && (t->kernel & 1);
     g.ddense = t && (t->kernel & 2);
-    g.staged = t && (t->kernel & 4);
-    g.stage_ns = (t && (t->kernel & 16)) ? 3 : 2;
     g.tw = kTileW;
     g.th = tile_height(g.rows);
     g.ntiles = 0;

@@ -6,8 +6,10 @@
 // (the sample's oversampling offset and w-plane).  The HBM copy bandwidth is not their ceiling;
 // this probe measures the one that is: warps reading random 128-byte row segments, 16 rows of one
 // "kernel" each with a 129-entry stride, from a buffer that fits in L2, 16 loads in flight per lane.
+// Built as its own library (libtcvprobe.so): a measurement tool, not part of the gridding ABI.
 // No counterpart in the reference.
 #include "tcv_internal.cuh"
+#include "tcv_probe.h"
 
 namespace tcv {
 namespace {

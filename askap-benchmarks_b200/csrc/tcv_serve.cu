@@ -47,13 +47,14 @@ using ReqPtr = std::shared_ptr<ServeReq>;
 struct Slot {
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
-    double *du = nullptr, *dv = nullptr, *dw = nullptr;
+    unsigned char* din = nullptr;         // one batch's inputs, packed: u, v, w, then the gridding data
+    unsigned char* hin = nullptr;         // their pinned host staging copy (one H2D copy per batch)
+    double *du = nullptr, *dv = nullptr, *dw = nullptr;  // the current batch's arrays inside din
     float2 *dvis = nullptr, *dout = nullptr;
     int32_t *diu = nullptr, *div = nullptr, *dco = nullptr;
     void* work = nullptr;
     size_t work_bytes = 0;
-    double *hu = nullptr, *hv = nullptr, *hw = nullptr;
-    float2 *hvis = nullptr, *hout = nullptr;
+    float2* hout = nullptr;
     unsigned long long* hrej = nullptr;  // rejected counts of the grid and degrid plans
     std::vector<ReqPtr> reqs;           // the batch in flight (grid requests first)
     int64_t n_grid = 0;                 // samples of its grid requests
@@ -147,23 +148,29 @@ tcv_status launch(tcv_server* s, Slot& sl)
         total += r->r.n;
     }
     sl.n_grid = n_grid;
+    // pack the batch's inputs (u, v, w of every request, then the gridding requests' data) so that
+    // one copy moves them
+    double* hu = reinterpret_cast<double*>(sl.hin);
+    double *hv = hu + total, *hw = hv + total;
+    float2* hvis = reinterpret_cast<float2*>(hw + total);
+    sl.du = reinterpret_cast<double*>(sl.din);
+    sl.dv = sl.du + total;
+    sl.dw = sl.dv + total;
+    sl.dvis = reinterpret_cast<float2*>(sl.dw + total);
     int64_t at = 0;
     for (const ReqPtr& r : reqs) {
         const size_t b = size_t(r->r.n) * 8;
         if (r->r.n) {
-            std::memcpy(sl.hu + at, r->r.u, b);
-            std::memcpy(sl.hv + at, r->r.v, b);
-            std::memcpy(sl.hw + at, r->r.w, b);
-            if (r->r.kind == TCV_REQ_GRID) std::memcpy(sl.hvis + at, r->r.vis, b);
+            std::memcpy(hu + at, r->r.u, b);
+            std::memcpy(hv + at, r->r.v, b);
+            std::memcpy(hw + at, r->r.w, b);
+            if (r->r.kind == TCV_REQ_GRID) std::memcpy(hvis + at, r->r.vis, b);
         }
         at += r->r.n;
     }
     sl.hrej[0] = sl.hrej[1] = 0;
     if (total > 0) {
-        TCV_CUDA(cudaMemcpyAsync(sl.du, sl.hu, size_t(total) * 8, cudaMemcpyHostToDevice, sl.st));
-        TCV_CUDA(cudaMemcpyAsync(sl.dv, sl.hv, size_t(total) * 8, cudaMemcpyHostToDevice, sl.st));
-        TCV_CUDA(cudaMemcpyAsync(sl.dw, sl.hw, size_t(total) * 8, cudaMemcpyHostToDevice, sl.st));
-        if (n_grid) TCV_CUDA(cudaMemcpyAsync(sl.dvis, sl.hvis, size_t(n_grid) * 8, cudaMemcpyHostToDevice, sl.st));
+        TCV_CUDA(cudaMemcpyAsync(sl.din, sl.hin, size_t(3 * total + n_grid) * 8, cudaMemcpyHostToDevice, sl.st));
         tcv_status st = tcv_init_offsets_raw(sl.du, sl.dv, sl.dw, total, s->dfreq, 1, s->cfg.cell_size, s->w_cell,
                                              s->cfg.w_size, s->cfg.g_size, s->support, s->over_sample, sl.diu, sl.div,
                                              sl.dco, sl.st);
@@ -297,10 +304,10 @@ void free_server(tcv_server* s)
 {
     for (auto& sl : s->slots) {
         if (sl->st) cudaStreamSynchronize(sl->st);
-        void* d[] = {sl->du, sl->dv, sl->dw, sl->dvis, sl->dout, sl->diu, sl->div, sl->dco, sl->work};
+        void* d[] = {sl->din, sl->dout, sl->diu, sl->div, sl->dco, sl->work};
         for (void* p : d)
             if (p) cudaFree(p);
-        void* h[] = {sl->hu, sl->hv, sl->hw, sl->hvis, sl->hout, sl->hrej};
+        void* h[] = {sl->hin, sl->hout, sl->hrej};
         for (void* p : h)
             if (p) cudaFreeHost(p);
         if (sl->done) cudaEventDestroy(sl->done);
@@ -395,7 +402,7 @@ tcv_status tcv_server_create(const tcv_server_config* cfg, tcv_server** out)
         free_server(s);
         return st;
     }
-    tcv::jit_prepare(ct, 2 * s->support + 1, c.tuning.tile_rows, tcv::tuning_stages(c.tuning));
+    tcv::jit_prepare(ct, 2 * s->support + 1, c.tuning.tile_rows);
     // batch slots, admitted against the budget
     const size_t work = slot_work_bytes(s);
     if (work == 0 || s->held + size_t(c.streams) * slot_bytes(c, work) > c.hbm_budget) {
@@ -408,10 +415,7 @@ tcv_status tcv_server_create(const tcv_server_config* cfg, tcv_server** out)
         Slot& sl = *s->slots.back();
         e = cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
-        if (e == cudaSuccess) e = dmalloc(&sl.du, cap, s->held);
-        if (e == cudaSuccess) e = dmalloc(&sl.dv, cap, s->held);
-        if (e == cudaSuccess) e = dmalloc(&sl.dw, cap, s->held);
-        if (e == cudaSuccess) e = dmalloc(&sl.dvis, cap, s->held);
+        if (e == cudaSuccess) e = dmalloc(&sl.din, 32 * cap, s->held);
         if (e == cudaSuccess) e = dmalloc(&sl.dout, cap, s->held);
         if (e == cudaSuccess) e = dmalloc(&sl.diu, cap, s->held);
         if (e == cudaSuccess) e = dmalloc(&sl.div, cap, s->held);
@@ -423,10 +427,7 @@ tcv_status tcv_server_create(const tcv_server_config* cfg, tcv_server** out)
                 s->held += work;
             }
         }
-        if (e == cudaSuccess) e = hmalloc(&sl.hu, cap);
-        if (e == cudaSuccess) e = hmalloc(&sl.hv, cap);
-        if (e == cudaSuccess) e = hmalloc(&sl.hw, cap);
-        if (e == cudaSuccess) e = hmalloc(&sl.hvis, cap);
+        if (e == cudaSuccess) e = hmalloc(&sl.hin, 32 * cap);
         if (e == cudaSuccess) e = hmalloc(&sl.hout, cap);
         if (e == cudaSuccess) e = hmalloc(&sl.hrej, 2);
     }

@@ -13,6 +13,7 @@ PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BUILD_DIR = os.path.join(PKG_ROOT, "_build")
 CSRC_DIR = os.path.join(PKG_ROOT, "csrc")
 LIB_PATH = os.path.join(BUILD_DIR, "libtconvolve.so")
+PROBE_LIB_PATH = os.path.join(BUILD_DIR, "libtcvprobe.so")
 
 TCV_OK = 0
 STATUS_NAMES = {
@@ -198,8 +199,6 @@ SIGNATURES = {
     "tcv_hogbom_set_wait": (_I, [ctypes.c_uint64, ctypes.c_uint32]),
     "tcv_find_peak": (_I, [_P, _I64, _P, _P, _P, _S, _P]),
     "tcv_fft_exec": (_I, [_P, _I, _I, _P]),
-    "tcv_probe_table_threads": (_I64, []),
-    "tcv_probe_table_stream": (_I, [_P, _I64, _I, _I, _P, _P, _P]),
     "tcv_band_histogram": (_I, [_P, _I64, _I, _I, _P, _P]),
     "tcv_band_bounds": (_I, [_P, _I, _I, _I, _P]),
     "tcv_band_workspace_bytes": (_S, [_I64, _I]),
@@ -315,6 +314,29 @@ def lib() -> ctypes.CDLL:
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+# the L2 table-stream probe (include/tcv_probe.h): a measurement tool in a library of its own
+PROBE_SIGNATURES = {
+    "tcv_probe_table_threads": (_I64, []),
+    "tcv_probe_table_stream": (_I, [_P, _I64, _I, _I, _P, _P, _P]),
+}
+_probe = None
+
+
+def probe_lib() -> ctypes.CDLL:
+    """libtcvprobe.so, loaded with its signatures (built beside libtconvolve.so)."""
+    global _probe
+    if _probe is None:
+        if not os.path.exists(PROBE_LIB_PATH):
+            raise RuntimeError(f"libtcvprobe.so not built ({PROBE_LIB_PATH}); run build() first")
+        P = ctypes.CDLL(PROBE_LIB_PATH)
+        for name, (res, args) in PROBE_SIGNATURES.items():
+            fn = getattr(P, name)
+            fn.restype = res
+            fn.argtypes = args
+        _probe = P
+    return _probe
 
 
 def check(status: int, what: str, ctx=None) -> None:

@@ -731,7 +731,8 @@ def batched_section(args, torch, stream, world):
     as one captured CUDA graph (bin + grid + degrid of every job) per step, with the tile shape and
     plane groups from the autotuner.  The grids (5 GB) are far larger than L2.  Measured for the
     chosen form, the plain c64 form and the bf16 form; the bf16 result's relative L2 distance from
-    the plain result is measured here (the FP64-oracle errors are in the precision tests)."""
+    the plain result, and every form's distance from the FP64 oracle on three of the jobs (the
+    smallest of each grid size and the median job), are measured here."""
     import tconvolve
     from tconvolve import raw
     from tconvolve._lib import PASS_BIN, PASS_DEGRID, PASS_GRID
@@ -748,6 +749,16 @@ def batched_section(args, torch, stream, world):
            "forms": {}}
     outs = {}
     rejected = None
+    # the FP64 oracle on a few jobs (the smallest of each grid size and the median job): every form's
+    # grid and degridded samples there against it
+    fp64 = {}
+    first = np.concatenate([[0], np.cumsum([n for n, _ in sizes])]).astype(np.int64)
+    check_jobs = None
+    if not args.no_precision:
+        order_n = sorted(range(len(sizes)), key=lambda j: sizes[j][0])
+        check_jobs = sorted({min((j for j in order_n if sizes[j][1] == 2048), key=lambda j: sizes[j][0]),
+                             min((j for j in order_n if sizes[j][1] == 4096), key=lambda j: sizes[j][0]),
+                             order_n[len(order_n) // 2]})
     for name in dict.fromkeys([args.form, "c64", "rbf16"]):
         ct = tconvolve.CTYPE_BY_NAME[name]
         c, scale, _ = (p["c64"], 1.0, 0) if ct == tconvolve.C64 else raw.convert_c(p["c64"], ct)
@@ -785,6 +796,9 @@ def batched_section(args, torch, stream, world):
         graph.launch(stream)
         torch.cuda.synchronize()
         outs[name] = out.clone()
+        if check_jobs is not None:
+            fp64[name] = [(grids[j].cpu().numpy(), out[first[j]:first[j] + sizes[j][0]].cpu().numpy())
+                          for j in check_jobs]
         upd = (p["total"] - rejected) * s2
         res["forms"][name] = {"value": world * 2 * upd / (step_ms * 1e-3), "unit": UNIT, "ms_per_step": step_ms,
                               "steps": k, "tuning": list(best), "autotune_s": tune_s,
@@ -797,37 +811,142 @@ def batched_section(args, torch, stream, world):
         a, r = outs["rbf16"], outs["c64"]
         res["forms"]["rbf16"]["rel_l2_vs_plain"] = float(torch.linalg.vector_norm(a - r) /
                                                          torch.linalg.vector_norm(r))
+    if check_jobs is not None:
+        res["precision_vs_fp64"] = batched_fp64_errors(p, sizes, first, check_jobs, fp64)
     res["rejected_samples"] = rejected
     res["rejected_note"] = ("samples whose footprint (rows iv..iv+128) leaves a 2048 grid; skipped and counted, "
                             "not in the update count")
     return res
 
 
+def batched_fp64_errors(p, sizes, first, jobs, results):
+    """Relative L2 of each form's grid and degridded samples against the FP64 oracle, on the
+    given jobs (their in-bounds samples; the reference would write out of bounds for the others):
+    the oracle's double gridding and degridding with the real double table of the same geometry
+    and the reference's normalisation."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as orc
+
+    threads = host_threads()
+    cfg = orc.Config(160000, 33, 1, 4096, 5.0)
+    _, c_f64, support, _, _, _ = orc.init_c(cfg, want_f64=True)
+    s = 2 * support + 1
+    iu, iv, co, data = (p[k].cpu().numpy() for k in ("iu", "iv", "coff", "data"))
+    out = {"jobs": [{"job": int(j), "samples": int(sizes[j][0]), "g_size": int(sizes[j][1])} for j in jobs],
+           "forms": {name: {"grid_rel_l2": [], "degrid_rel_l2": []} for name in results}}
+    for k, j in enumerate(jobs):
+        g = int(sizes[j][1])
+        sl = slice(int(first[j]), int(first[j] + sizes[j][0]))
+        keep = (iu[sl] - support >= 0) & (iu[sl] - support + s <= g) & (iv[sl] >= 0) & (iv[sl] + s <= g)
+        a = [np.ascontiguousarray(x[sl][keep]) for x in (iu, iv, co)]
+        ref = np.zeros(g * g, np.complex128)
+        orc.grid_f64(data[sl][keep].astype(np.complex128), support, c_f64, a[2], a[0], a[1], ref, g, threads)
+        ref_o = orc.degrid_f64(ref, g, support, c_f64, a[2], a[0], a[1], threads)
+        for name, per_job in results.items():
+            grid_j, out_j = per_job[k]
+            out["forms"][name]["grid_rel_l2"].append(orc.rel_l2(grid_j, ref))
+            out["forms"][name]["degrid_rel_l2"].append(orc.rel_l2(out_j[keep], ref_o))
+    for e in out["forms"].values():
+        e["grid_rel_l2_max"] = max(e["grid_rel_l2"])
+        e["degrid_rel_l2_max"] = max(e["degrid_rel_l2"])
+    return out
+
+
 def serving_section(args, device):
     """Serving: Poisson arrivals of gridding and degridding requests (half each) of 16000 samples
-    on the 1024^2-grid, 9-plane, 5 arcsec problem (32.4e6 updates each) at 50, 100, 200 and 500
-    requests/s, over 64 resident grids, under a 150 GB device-memory budget; latency is submission
-    to result-ready, measured by the server."""
+    on the 1024^2-grid, 9-plane, 5 arcsec problem (32.4e6 updates each) over 64 resident grids,
+    under a 150 GB device-memory budget; latency is submission to result-ready, measured by the
+    server.  The chosen form runs at 50, 100, 200 and 500 requests/s (light load: batches of about
+    one request) and at a saturating open-loop rate and a burst of 256 requests (continuous
+    batching: batches of many requests); the bf16 form runs the saturating load and the burst
+    beside it.  Each form's served results are checked against the FP64 oracle: one gridding
+    request into a fresh grid, then one degridding request of that grid."""
     from tconvolve.serve import Server, poisson_run, request_pool
 
-    srv = Server(c_type=args.form if args.form in ("r32", "c64", "rbf16", "cbf16") else "r32", streams=2,
-                 max_batch=32, batch_samples=32 * 16000, hbm_budget=150e9, device=device)
-    grids = [srv.grid_alloc() for _ in range(64)]
+    chosen = args.form if args.form in ("r32", "c64", "rbf16", "cbf16") else "r32"
     pool = request_pool(32, 16000, seed=7)
-    poisson_run(srv, rate=200, duration=0.3, pool=pool, grids=grids, seed=99)  # warm-up
     upd = 16000 * 45 * 45
-    rates = []
-    for rate in (50, 100, 200, 500):
-        r = poisson_run(srv, rate=rate, duration=args.serve_seconds, pool=pool, grids=grids, seed=rate)
-        r["updates_per_s"] = r["throughput_req_s"] * upd if r["throughput_req_s"] else None
-        rates.append(r)
-    st = srv.stats()
-    srv.close()
-    return {"workload": "Poisson arrivals, half gridding / half degridding requests of 16000 samples "
-                        "(1024^2 grid, 9 w-planes, support 22: 32.4e6 updates each), 64 resident grids",
-            "form": args.form if args.form in ("r32", "c64", "rbf16", "cbf16") else "r32",
-            "hbm_budget_bytes": int(150e9), "bytes_held": st["bytes_held"], "slots": 2, "max_batch": 32,
-            "latency": "submission to result-ready (server clock)", "rates": rates}
+    out = {"workload": "Poisson arrivals, half gridding / half degridding requests of 16000 samples "
+                       "(1024^2 grid, 9 w-planes, support 22: 32.4e6 updates each), 64 resident grids",
+           "form": chosen, "hbm_budget_bytes": int(150e9), "slots": 2, "max_batch": 32,
+           "latency": "submission to result-ready (server clock)", "forms": {}}
+    for form in dict.fromkeys([chosen, "rbf16"]):
+        srv = Server(c_type=form, streams=2, max_batch=32, batch_samples=32 * 16000, hbm_budget=150e9, device=device)
+        grids = [srv.grid_alloc() for _ in range(64)]
+        poisson_run(srv, rate=200, duration=0.3, pool=pool, grids=grids, seed=99)  # warm-up
+        rates = []
+        loads = ([("poisson", r, args.serve_seconds) for r in (50, 100, 200, 500)] if form == chosen else [])
+        loads += [("poisson", 20000, 1.0), ("burst", 256, None)]
+        for kind, rate, dur in loads:
+            if kind == "poisson":
+                r = poisson_run(srv, rate=rate, duration=dur, pool=pool, grids=grids, seed=rate)
+            else:
+                r = burst_run(srv, rate, pool, grids, seed=5)
+            r["load"] = kind
+            r["updates_per_s"] = r["throughput_req_s"] * upd if r["throughput_req_s"] else None
+            rates.append(r)
+        entry = {"rates": rates, "bytes_held": srv.stats()["bytes_held"]}
+        if not args.no_precision:
+            entry["precision_vs_fp64"] = served_precision(srv, pool[0])
+        srv.close()
+        out["forms"][form] = entry
+    out["rates"] = out["forms"][chosen]["rates"]
+    return out
+
+
+def burst_run(server, n: int, pool, grids, seed: int = 0) -> dict:
+    """n requests submitted back to back (half gridding, half degridding, random resident grids):
+    the server batches them as slots free up; latency and throughput as poisson_run reports."""
+    from tconvolve import _lib
+
+    rng = np.random.default_rng(seed)
+    kinds = rng.random(n) < 0.5
+    picks = rng.integers(0, len(pool), n)
+    gsel = rng.integers(0, len(grids), n)
+    t0 = time.perf_counter()
+    reqs = []
+    for i in range(n):
+        u, v, w, vis = pool[picks[i]]
+        kind = _lib.REQ_DEGRID if kinds[i] else _lib.REQ_GRID
+        reqs.append(server.submit(kind, grids[gsel[i]], u, v, w, vis if kind == _lib.REQ_GRID else None))
+    submit_s = time.perf_counter() - t0
+    infos = [r.wait() for r in reqs]
+    lat = np.array([i.t_done - i.t_submit for i in infos]) * 1e3
+    span = max(i.t_done for i in infos) - min(i.t_submit for i in infos)
+    return {"requests": n, "submit_span_s": submit_s, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+            "throughput_req_s": n / span if span > 0 else None,
+            "mean_batch": float(np.mean([i.batch_requests for i in infos])),
+            "errors": int(sum(1 for i in infos if i.status != 0))}
+
+
+def served_precision(srv, inputs) -> dict:
+    """One gridding request into a fresh resident grid and one degridding request of that grid,
+    through the server, against the FP64 oracle of the same samples (the 1024^2, 9-plane, 5 arcsec
+    problem's real double table with the reference's normalisation)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as orc
+    from tconvolve import _lib
+
+    u, v, w, vis = inputs
+    g = srv.grid_alloc()
+    srv.submit(_lib.REQ_GRID, g, u, v, w, vis).wait()
+    grid = srv.grid_read(g)
+    r = srv.submit(_lib.REQ_DEGRID, g, u, v, w)
+    r.wait()
+    srv.grid_free(g)
+    cfg = orc.CONFIGS["c1"]
+    _, c_f64, support, os_, wcs, _ = orc.init_c(cfg, want_f64=True)
+    iu, iv, co = orc.init_offsets(orc.Config(u.size, cfg.w_size, 1, cfg.g_size, cfg.cell_size), u, v, w, wcs,
+                                  support, os_)
+    gs = cfg.g_size
+    grid64 = np.zeros(gs * gs, np.complex128)
+    orc.grid_f64(vis.astype(np.complex128), support, c_f64, co, iu, iv, grid64, gs, host_threads())
+    out64 = orc.degrid_f64(grid64, gs, support, c_f64, co, iu, iv, host_threads())
+    # the degridding request read the served grid: its FP64 reference degrids that same grid
+    served64 = orc.degrid_f64(grid.astype(np.complex128), gs, support, c_f64, co, iu, iv, host_threads())
+    return {"grid_rel_l2": orc.rel_l2(grid, grid64), "degrid_rel_l2_same_grid": orc.rel_l2(r.vis_out, served64),
+            "degrid_rel_l2_end_to_end": orc.rel_l2(r.vis_out, out64), "samples": int(u.size)}
 
 
 def current_section(args, torch, world):
@@ -1090,10 +1209,11 @@ def l2_table_ceiling(torch, stream, updates, g_ms, d_ms, form):
     from tconvolve.raw import _ptr
 
     L = tconvolve.lib()
+    P = tconvolve._lib.probe_lib()
     buf = torch.rand(16 << 20, dtype=torch.float32, device="cuda")
-    out = torch.empty(int(L.tcv_probe_table_threads()), dtype=torch.float32, device="cuda")
+    out = torch.empty(int(P.tcv_probe_table_threads()), dtype=torch.float32, device="cuda")
     nbytes = ctypes.c_int64()
-    launch = lambda: L.tcv_probe_table_stream(_ptr(buf), buf.numel(), 129, 256, _ptr(out), ctypes.byref(nbytes),
+    launch = lambda: P.tcv_probe_table_stream(_ptr(buf), buf.numel(), 129, 256, _ptr(out), ctypes.byref(nbytes),
                                               ctypes.c_void_p(stream.cuda_stream))
     for _ in range(3):
         if launch() != 0:

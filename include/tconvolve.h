@@ -601,7 +601,9 @@ tcv_status tcv_find_peak(const float *d_image, int64_t n, float *val_out, int64_
  * complex64 of even size g_size (odd sizes: TCV_ERR_UNSUPPORTED, as the reference refuses them).
  * ---------------------------------------------------------------------------------------- */
 /* fftExec / fftExecGPU: in place, rotate by half the size in both axes, unnormalised 2-D C2C
- * transform (forward: exp(-i..), else exp(+i..)), rotate back.  Single precision (cuFFT). */
+ * transform (forward: exp(-i..), else exp(+i..)), rotate back.  Single precision: this library's
+ * own two-pass transform for power-of-two sizes 128 .. 8192 (the first call of a size on a device
+ * makes its twiddle table: set-up, allocates), cuFFT for other even sizes. */
 tcv_status tcv_fft_exec(float *d_grid, int g_size, int forward, void *stream);
 /* fftFix / fftFixGPU: grid[i] = (Re grid[i] * scale, 0) for n complex values. */
 tcv_status tcv_fft_fix(float *d_grid, int64_t n, float scale, void *stream);
@@ -696,19 +698,6 @@ tcv_status tcv_band_scatter(const float *d_src, const int32_t *d_perm, int64_t n
                             void *stream);
 /* d_dst += d_src over n_complex complex64 values (a received halo into the owner's rows). */
 tcv_status tcv_rows_add(float *d_dst, const float *d_src, int64_t n_complex, void *stream);
-
-/* ------------------------------------------------------------------------------------------
- * A measurement, not part of the path: the L2-to-SM bandwidth of this GPU for the tile kernels'
- * table reads (random 128-byte row segments, 16 rows at a row stride, from an L2-resident
- * buffer), the ceiling those kernels are bound by.  No counterpart in the reference.
- * ---------------------------------------------------------------------------------------- */
-/* Threads of one probe launch (d_out must hold as many floats). */
-int64_t tcv_probe_table_threads(void);
-/* One launch over d_buf (n_floats, ideally a few tens of MB so that it stays in L2), each warp
- * reading `samples` random 16-row windows of `stride` floats; *bytes_out receives the bytes the
- * warps read (128 per row segment).  Asynchronous on the stream: time it with events. */
-tcv_status tcv_probe_table_stream(const float *d_buf, int64_t n_floats, int stride, int samples,
-                                  float *d_out, int64_t *bytes_out, void *stream);
 
 #ifdef __cplusplus
 }

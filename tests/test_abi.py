@@ -34,6 +34,21 @@ def test_library_exports_every_declared_symbol(tcv):
     assert not missing, f"declared but not exported: {missing}"
 
 
+def test_probe_library_exports_its_header(tcv):
+    """The L2 table-stream probe is a measurement tool in a library of its own (libtcvprobe.so,
+    include/tcv_probe.h); libtconvolve.so does not export it."""
+    from tconvolve._lib import LIB_PATH, PROBE_LIB_PATH, PROBE_SIGNATURES
+
+    text = re.sub(r"/\*.*?\*/", "", open(os.path.join(REPO, "include", "tcv_probe.h")).read(), flags=re.S)
+    declared = sorted(set(re.findall(r"\b(tcv_[a-z0-9_]+)\s*\(", text)))
+    assert declared == sorted(PROBE_SIGNATURES)
+    out = subprocess.run(["nm", "-D", "--defined-only", PROBE_LIB_PATH], check=True, capture_output=True,
+                         text=True).stdout
+    assert all(f" T {f}" in out for f in declared)
+    main = subprocess.run(["nm", "-D", "--defined-only", LIB_PATH], check=True, capture_output=True, text=True).stdout
+    assert "tcv_probe" not in main
+
+
 def test_binding_covers_header(tcv):
     from tconvolve._lib import SIGNATURES
 

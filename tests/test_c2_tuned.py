@@ -74,3 +74,4 @@ def test_tuned_plans_match_reference(c2_bench, c2_reference, orc, tuning):
     assert np.array_equal(g64, g32) and np.array_equal(o64, o32)
     g2, o2 = _run(c2_bench, "r32", tuning)
     assert np.array_equal(g2, g32) and np.array_equal(o2, o32)
+

@@ -23,8 +23,10 @@ def _fft_case(n, seed):
     return (rng.standard_normal(n * n) + 1j * rng.standard_normal(n * n)).astype(np.complex64)
 
 
-@pytest.mark.parametrize("n", [256, 1034, 4096])
+@pytest.mark.parametrize("n", [128, 256, 512, 1034, 2048, 4096, 8192])
 def test_fft_steps(tcv, orc, cuda_ok, n):
+    """Power-of-two sizes 128 .. 8192 run the library's own two-pass transform (an odd power of
+    two takes one radix-2 stage), 1034 runs cuFFT; both against numpy's double transform."""
     import torch
 
     from tconvolve import major

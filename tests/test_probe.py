@@ -8,7 +8,7 @@ import pytest
 
 
 def test_probe_argument_validation(tcv):
-    from tconvolve._lib import lib
+    from tconvolve._lib import probe_lib as lib
 
     L = lib()
     fake = ctypes.c_void_p(0x1000)  # never dereferenced: the calls fail their argument checks first
@@ -23,7 +23,7 @@ def test_probe_argument_validation(tcv):
 def test_probe_measures(tcv, cuda_ok):
     import torch
 
-    from tconvolve._lib import lib
+    from tconvolve._lib import probe_lib as lib
     from tconvolve.raw import _ptr
 
     L = lib()
