@@ -602,8 +602,9 @@ tcv_status tcv_find_peak(const float *d_image, int64_t n, float *val_out, int64_
  * ---------------------------------------------------------------------------------------- */
 /* fftExec / fftExecGPU: in place, rotate by half the size in both axes, unnormalised 2-D C2C
  * transform (forward: exp(-i..), else exp(+i..)), rotate back.  Single precision: this library's
- * own two-pass transform for power-of-two sizes 128 .. 8192 (the first call of a size on a device
- * makes its twiddle table: set-up, allocates), cuFFT for other even sizes. */
+ * own three-pass transform for power-of-two sizes 128 .. 8192 (the first call of a size on a device
+ * makes its twiddle table and a g_size^2 complex scratch grid: set-up, allocates), cuFFT for other
+ * even sizes. */
 tcv_status tcv_fft_exec(float *d_grid, int g_size, int forward, void *stream);
 /* fftFix / fftFixGPU: grid[i] = (Re grid[i] * scale, 0) for n complex values. */
 tcv_status tcv_fft_fix(float *d_grid, int64_t n, float scale, void *stream);
