@@ -94,175 +94,241 @@ __device__ __forceinline__ DenseRec prepare(int coffk, int s, int fx, int fy, in
     return d;
 }
 
-// A staged sample for gridding: its rectangle in tile coordinates (first column and row, width,
-// height) and the table index of the rectangle's first element.  Each warp clips it to its half.
-struct GridRec {
-    int c0;     // table index of the rectangle's first element
-    int s;      // table row stride
-    int shape;  // first tile column | first tile row << 8 | w << 16 | h << 24 (h = 0: no overlap)
-};
-
-__device__ __forceinline__ GridRec prepare_grid(int coffk, int s, int fx, int fy, int tx0, int ty0)
+// Gridding lane table: for a rectangle width w (1 .. 32) and a lane, the lane's row in the step
+// (lane / w), its column (lane % w) and the rows per step (floor(32 / w)), as
+// row | column << 5 | rows << 10.
+__device__ __forceinline__ void build_grid_lut(unsigned short (&gl)[33][32], int tid, int nthreads)
 {
-    const Rect R = clip(fx, fy, s, tx0, ty0);
-    const int w = R.c1 - R.c0, h = R.r1 - R.r0;
-    GridRec g;
-    g.s = s;
-    if (w <= 0 || h <= 0) {  // no overlap (a binned sample always has one)
-        g.c0 = 0;
-        g.shape = 0;
-        return g;
+    for (int i = tid; i < 33 * 32; i += nthreads) {
+        const int w = i / 32 < 1 ? 1 : i / 32, lane = i % 32;
+        gl[i / 32][lane] = (unsigned short)((lane / w) | (lane % w) << 5 | (32 / w) << 10);
     }
-    g.c0 = coffk + R.r0 * s + R.c0;
-    g.shape = (fx + R.c0 - tx0) | ((fy + R.r0 - ty0) << 8) | (w << 16) | (h << 24);
-    return g;
 }
 
-// Gridding: the tile's two 32-column halves each have kGWarps / 2 warps; sample j goes to warp
-// j mod (kGWarps / 2) of each half it meets, which adds it into its private copy of that half.
+// The gridding kernel's position in its work: unit list position, first sample of the chunk in
+// that unit, the unit's sample range, tile record and partial tile, and the chunk's sample count
+// (0: no more work).  Chunks are kGChunk samples.
+constexpr int kGChunk = 128;
+struct DChunk {
+    u32 it, base, cnt, start, ti, pslot;
+    int m;
+};
+__device__ __forceinline__ void dchunk_load(DChunk& c, u32 it, u32 i1, const uint4* __restrict__ units,
+                                            const GridArgs& a)
+{
+    c.it = it;
+    c.base = 0;
+    c.m = 0;
+    if (it < i1) {
+        const uint4 u = units[it];
+        c.start = u.y;
+        c.cnt = u.z;
+        c.pslot = u.w;
+        c.ti = a.tinfo[u.x - u32(a.group) * u32(a.ntiles)];
+        c.m = int(c.cnt < u32(kGChunk) ? c.cnt : u32(kGChunk));
+    }
+}
+__device__ __forceinline__ void dchunk_next(DChunk& c, u32 i1, const uint4* __restrict__ units, const GridArgs& a)
+{
+    if (c.base + u32(kGChunk) < c.cnt) {
+        c.base += u32(kGChunk);
+        const u32 left = c.cnt - c.base;
+        c.m = int(left < u32(kGChunk) ? left : u32(kGChunk));
+    } else {
+        dchunk_load(c, c.it + gridDim.x, i1, units, a);
+    }
+}
+
+// Gridding.  The tile's two 32-column halves each have kGWarps / 2 warps with private copies of the
+// half.  A chunk of kGChunk samples is staged as jobs, one per (sample, half it meets): thread t
+// prepares sample t % kGChunk for half t / kGChunk, and the jobs of a staging warp are packed in
+// sample order into its 32-entry segment of the half's list (ballot), so a half's warps see only
+// the samples that meet it.  A job is the table index of the first element of the sample's
+// rectangle in the half, and first point | (width - 1) << 10 | (height - 1) << 15 | table row
+// stride << 20, and the scaled data value.  Warp j of a half takes jobs j, j + 4, ... of the
+// half's list (segments in order).  The next chunk is staged while this one is added (two
+// buffers, one barrier per chunk); each warp keeps the next job's first table loads in flight
+// while it adds the current one.
 template <class Tab>
-__global__ void __launch_bounds__(kGThreads)
+__global__ void __launch_bounds__(kGThreads, 3)
 dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
                   const int* __restrict__ iu, const int* __restrict__ iv, const int* __restrict__ coff,
                   const u32* __restrict__ order, const uint4* __restrict__ units,
                   const u32* __restrict__ group_ustart, GridArgs a)
 {
+    using E = typename Tab::elem;
     constexpr int kHalf = kDTW / 2;            // 32 columns
     constexpr int kHPts = kHalf * kDTH;        // 1024 points per half
     constexpr int kPerHalf = kGWarps / 2;      // warps per half
-    extern __shared__ float2 dsm[];
-    float2* acc_all = dsm;                                               // [kGWarps][kHPts]
-    GridRec* rec = reinterpret_cast<GridRec*>(dsm + kGWarps * kHPts);   // [kGThreads]
-    float2* rdv = reinterpret_cast<float2*>(rec + kGThreads);            // scaled data
-    __shared__ DenseLut L;
+    constexpr int kSegs = kGChunk / 32;        // staging warps per half
+    constexpr int U = 4;                       // table loads of a job issued together
+    static_assert(kSegs == 4 && 2 * kGChunk == kGThreads, "one staging thread per (sample, half)");
+    extern __shared__ __align__(16) float2 dsm[];
+    float2* acc_all = dsm;                                                    // [kGWarps][kHPts]
+    int4* jobs = reinterpret_cast<int4*>(dsm + kGWarps * kHPts);             // [2][2][kGChunk]
+    __shared__ int jcnt[2][2][kSegs];
+    __shared__ unsigned short gl[33][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int half = warp / kPerHalf, sub = warp % kPerHalf, hx0 = half * kHalf;
-    build_lut(L, threadIdx.x, kGThreads);
+    const int half = warp / kPerHalf, sub = warp % kPerHalf;
+    build_grid_lut(gl, threadIdx.x, kGThreads);
     float2* acc = acc_all + warp * kHPts;
     for (int i = lane; i < kHPts; i += 32) acc[i] = make_float2(0.f, 0.f);
-    const u32 i1 = group_ustart[a.group + 1];
-    for (u32 it = group_ustart[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
-        const uint4 u = units[it];
-        const u32 start = u.y, cnt = u.z, pslot = u.w;
-        const u32 ti = a.tinfo[u.x - u32(a.group) * u32(a.ntiles)];
-        const int tx0 = rec_tx(ti) * kDTW, ty0 = rec_ty(ti) * kDTH;
-        for (u32 base = 0; base < cnt; base += kGThreads) {
-            const int m = int(cnt - base < u32(kGThreads) ? cnt - base : u32(kGThreads));
-            __syncthreads();  // the previous chunk's records are consumed (and the lane table built)
-            if (int(threadIdx.x) < m) {
-                const u32 k = order[start + base + threadIdx.x];
+
+    const int si = threadIdx.x % kGChunk, sh = threadIdx.x / kGChunk;
+    auto stage = [&](const DChunk& c, int buf) {
+        bool has = false;
+        int4 jb = make_int4(0, 0, 0, 0);
+        if (si < c.m) {
+            const u32 k = order[c.start + c.base + si];
+            const int sk = int(a.ssz[k]);
+            const int fx = iu[k] - sk / 2, fy = iv[k];
+            const int tx0 = rec_tx(c.ti) * kDTW, ty0 = rec_ty(c.ti) * kDTH;
+            const Rect R = clip(fx, fy, sk, tx0, ty0);
+            const int tc = fx + R.c0 - tx0, h = R.r1 - R.r0, hx0 = sh * kHalf;
+            const int lo = max(tc, hx0), hi = min(fx + R.c1 - tx0, hx0 + kHalf);
+            has = h > 0 && lo < hi;
+            if (has) {
                 const float2 d = data[k];
-                const int sk = int(a.ssz[k]);
-                rec[threadIdx.x] = prepare_grid(coff[k], sk, iu[k] - sk / 2, iv[k], tx0, ty0);
-                rdv[threadIdx.x] = make_float2(d.x * a.c_scale, d.y * a.c_scale);
+                jb.x = coff[k] + R.r0 * sk + R.c0 + (lo - tc);
+                jb.y = int(u32((fy + R.r0 - ty0) * kHalf + lo - hx0) | u32(hi - lo - 1) << 10 | u32(h - 1) << 15 |
+                           u32(sk) << 20);
+                jb.z = __float_as_int(d.x * a.c_scale);
+                jb.w = __float_as_int(d.y * a.c_scale);
             }
-            __syncthreads();
-            // Software pipeline over this warp's samples: the next sample's first U steps of table
-            // loads are in flight while the current sample updates the copy.
-            constexpr int U = 4;
-            struct Job {
-                int h, hf, kk, s, cbase, pbase;  // h: rows from the lane's first; hf: the rectangle's
-                bool lane_ok;
-                float2 dv;
-            };
-            // the next sample from index j on that meets this half; false when there is none
-            auto setup = [&](int& j, Job& jb) -> bool {
-                for (; j < m; j += kPerHalf) {
-                    const GridRec g = rec[j];
-                    const int tc = g.shape & 255, tr = (g.shape >> 8) & 255, w = (g.shape >> 16) & 255,
-                              h = g.shape >> 24;
-                    const int lo = max(tc, hx0), hi = min(tc + w, hx0 + kHalf);
-                    if (h == 0 || lo >= hi) continue;  // warp-uniform
-                    const int wc = hi - lo;
-                    jb.kk = L.k[wc];
-                    const int qq = L.q[wc][lane], rr = L.r[wc][lane];
-                    jb.lane_ok = qq < jb.kk;
-                    jb.h = h - qq;  // rows left for this lane, from its first
-                    jb.hf = h;
-                    jb.s = g.s;
-                    jb.cbase = g.c0 + (lo - tc) + qq * g.s + rr;
-                    jb.pbase = (tr + qq) * kHalf + (lo - hx0) + rr;
-                    jb.dv = rdv[j];
-                    return true;
-                }
-                return false;
-            };
-            auto load = [&](const Job& jb, int row0, float2 (&cv)[U]) {
+        }
+        const u32 b = __ballot_sync(0xffffffffu, has);
+        if (has) jobs[(buf * 2 + sh) * kGChunk + (si & ~31) + __popc(b & ((1u << lane) - 1u))] = jb;
+        if (lane == 0) jcnt[buf][sh][si >> 5] = __popc(b);
+    };
+
+    struct Job {
+        const E* tp;   // the lane's first table entry
+        int ap;        // the lane's first point in the copy
+        int rem, h;    // rows of the lane (from its first, in steps of kk) and of the rectangle
+        int kk, kks;   // rows per step, and table entries per step
+        float2 dv;
+    };
+    auto consume = [&](int buf) {
+        const int4* jl = jobs + (buf * 2 + half) * kGChunk;
+        const int c0 = jcnt[buf][half][0], c1 = jcnt[buf][half][1], c2 = jcnt[buf][half][2];
+        const int p1 = c0, p2 = p1 + c1, p3 = p2 + c2, n = p3 + jcnt[buf][half][3];
+        auto setup = [&](int i, Job& J) {
+            int sl = i;  // list position -> slot of its segment
+            if (i >= p1) sl += 32 - c0;
+            if (i >= p2) sl += 32 - c1;
+            if (i >= p3) sl += 32 - c2;
+            const int4 jb = jl[sl];
+            const u32 meta = u32(jb.y);
+            const int wc = int((meta >> 10) & 31u) + 1, s = int(meta >> 20);
+            const u32 lu = gl[wc][lane];
+            const int q = int(lu & 31u), r = int((lu >> 5) & 31u);
+            J.h = int((meta >> 15) & 31u) + 1;
+            J.kk = int(lu >> 10);
+            J.rem = q < J.kk ? J.h - q : 0;
+            J.tp = ctab + (jb.x + q * s + r);
+            J.ap = int(meta & 1023u) + q * kHalf + r;
+            J.kks = J.kk * s;
+            J.dv = make_float2(__int_as_float(jb.z), __int_as_float(jb.w));
+        };
+        auto load = [&](const Job& J, int e0, float2 (&cv)[U]) {
 #pragma unroll
-                for (int e = 0; e < U; ++e) {
-                    const int ro = row0 + e * jb.kk;
-                    cv[e] = (jb.lane_ok && ro < jb.h) ? Tab::load(ctab + (jb.cbase + ro * jb.s)) : make_float2(0.f, 0.f);
-                }
-            };
-            auto apply = [&](const Job& jb, int row0, const float2 (&cv)[U]) {
+            for (int e = 0; e < U; ++e) {
+                const int ro = (e0 + e) * J.kk;
+                if (ro >= J.h) break;  // warp-uniform
+                cv[e] = ro < J.rem ? Tab::load(J.tp + (e0 + e) * J.kks) : make_float2(0.f, 0.f);
+            }
+        };
+        auto apply = [&](const Job& J, int e0, const float2 (&cv)[U]) {
 #pragma unroll
-                for (int e = 0; e < U; ++e) {
-                    const int ro = row0 + e * jb.kk;
-                    if (jb.lane_ok && ro < jb.h) {
-                        float2& gp = acc[jb.pbase + ro * kHalf];
-                        float2 t = gp;
-                        cmac<Tab::kReal>(t, jb.dv, cv[e]);
-                        gp = t;
+            for (int e = 0; e < U; ++e) {
+                const int ro = (e0 + e) * J.kk;
+                if (ro >= J.h) break;  // warp-uniform
+                if (ro < J.rem) {
+                    float2& gp = acc[J.ap + ro * kHalf];
+                    float2 t = gp;
+                    cmac<Tab::kReal>(t, J.dv, cv[e]);
+                    gp = t;
+                }
+            }
+        };
+        int i = sub;
+        if (i >= n) return;
+        Job cur;
+        float2 cv[U];
+        setup(i, cur);
+        load(cur, 0, cv);
+        for (;;) {
+            const int inx = i + kPerHalf;
+            const bool more = inx < n;
+            Job nx;
+            float2 nv[U];
+            if (more) {  // in flight during the updates below
+                setup(inx, nx);
+                load(nx, 0, nv);
+            }
+            apply(cur, 0, cv);
+            for (int e0 = U; e0 * cur.kk < cur.h; e0 += U) {  // tall rectangles (warp-uniform)
+                float2 t[U];
+                load(cur, e0, t);
+                apply(cur, e0, t);
+            }
+            __syncwarp();  // this job's updates land before another lane reads them for the next
+            if (!more) break;
+            cur = nx;
+            i = inx;
+#pragma unroll
+            for (int e = 0; e < U; ++e) cv[e] = nv[e];
+        }
+    };
+
+    const u32 i1 = group_ustart[a.group + 1];
+    DChunk cur;
+    dchunk_load(cur, group_ustart[a.group] + blockIdx.x, i1, units, a);
+    stage(cur, 0);
+    __syncthreads();  // the first chunk is staged (and the lane table built)
+    int buf = 0;
+    while (cur.m > 0) {
+        DChunk nxt = cur;
+        dchunk_next(nxt, i1, units, a);
+        stage(nxt, buf ^ 1);  // the next chunk, while this one is added
+        consume(buf);
+        if (nxt.it != cur.it || nxt.m == 0) {  // the unit is done (block-uniform)
+            __syncthreads();  // every warp's copy is complete
+            // each half's copies in warp order, into the grid (a whole cell) or the unit's partial tile
+            const JobDesc& jd = a.jobs[rec_job(cur.ti)];
+            const int gs = jd.g_size;
+            float2* grid = a.grid ? a.grid : jd.grid;
+            const int tx0 = rec_tx(cur.ti) * kDTW, ty0 = rec_ty(cur.ti) * kDTH;
+            for (int p = threadIdx.x; p < kDPts; p += kGThreads) {
+                const int px = p % kDTW, py = p / kDTW;
+                const int hh = px / kHalf, hp = py * kHalf + (px % kHalf);
+                float2* c = acc_all + hh * kPerHalf * kHPts + hp;
+                float2 v = c[0];
+#pragma unroll
+                for (int w = 1; w < kPerHalf; ++w) {
+                    const float2 o = c[w * kHPts];
+                    v.x += o.x;
+                    v.y += o.y;
+                }
+#pragma unroll
+                for (int w = 0; w < kPerHalf; ++w) c[w * kHPts] = make_float2(0.f, 0.f);
+                if (cur.pslot != kDirect) {
+                    a.partial[(unsigned long long)(cur.pslot) * kDPts + p] = v;
+                } else {
+                    const int gx = tx0 + px, gy = ty0 + py;
+                    if (gx < gs && gy < gs) {
+                        float2* gp = grid + ((unsigned long long)(gy) * gs + gx);
+                        float2 o = *gp;
+                        o.x += v.x;
+                        o.y += v.y;
+                        *gp = o;
                     }
                 }
-            };
-            int j = sub;
-            Job cur;
-            float2 cvc[U];
-            bool have = setup(j, cur);
-            if (have) load(cur, 0, cvc);
-            while (have) {
-                int jn = j + kPerHalf;
-                Job nxt;
-                float2 cvn[U];
-                const bool more = setup(jn, nxt);
-                if (more) load(nxt, 0, cvn);  // in flight during the updates below
-                apply(cur, 0, cvc);
-                for (int row0 = U * cur.kk; row0 < cur.hf; row0 += U * cur.kk) {  // tall rectangles (warp-uniform)
-                    float2 cv[U];
-                    load(cur, row0, cv);
-                    apply(cur, row0, cv);
-                }
-                __syncwarp();  // this sample's updates land before another lane reads them for the next
-                if (!more) break;
-                cur = nxt;
-                j = jn;
-#pragma unroll
-                for (int e = 0; e < U; ++e) cvc[e] = cvn[e];
             }
         }
-        __syncthreads();  // every warp's copy is complete
-        // each half's copies in warp order, into the grid (a whole cell) or the unit's partial tile
-        const JobDesc& jd = a.jobs[rec_job(ti)];
-        const int gs = jd.g_size;
-        float2* grid = a.grid ? a.grid : jd.grid;
-        for (int p = threadIdx.x; p < kDPts; p += kGThreads) {
-            const int px = p % kDTW, py = p / kDTW;
-            const int hh = px / kHalf, hp = py * kHalf + (px % kHalf);
-            float2* c = acc_all + hh * kPerHalf * kHPts + hp;
-            float2 v = c[0];
-#pragma unroll
-            for (int w = 1; w < kPerHalf; ++w) {
-                const float2 o = c[w * kHPts];
-                v.x += o.x;
-                v.y += o.y;
-            }
-#pragma unroll
-            for (int w = 0; w < kPerHalf; ++w) c[w * kHPts] = make_float2(0.f, 0.f);
-            if (pslot != kDirect) {
-                a.partial[(unsigned long long)(pslot) * kDPts + p] = v;
-            } else {
-                const int gx = tx0 + px, gy = ty0 + py;
-                if (gx < gs && gy < gs) {
-                    float2* gp = grid + ((unsigned long long)(gy) * gs + gx);
-                    float2 o = *gp;
-                    o.x += v.x;
-                    o.y += v.y;
-                    *gp = o;
-                }
-            }
-        }
-        // the zeroed copies are rewritten only after the next unit's first barrier
+        __syncthreads();  // the next chunk is staged; this chunk's jobs are free; the copies are zero
+        cur = nxt;
+        buf ^= 1;
     }
 }
 
@@ -352,7 +418,7 @@ int resident(const void* kernel, int threads, size_t smem)
     return per_sm * sms;
 }
 
-constexpr size_t kGridSmem = size_t(kGWarps) * (kDPts / 2) * sizeof(float2) + size_t(kGThreads) * (sizeof(GridRec) + sizeof(float2));
+constexpr size_t kGridSmem = size_t(kGWarps) * (kDPts / 2) * sizeof(float2) + size_t(2 * 2 * kGChunk) * sizeof(int4);
 
 GridArgs dense_args(const tcv_plan* p, int grp, float c_scale, float2* grid)
 {
@@ -379,7 +445,7 @@ tcv_status launch_dense_grid(const tcv_plan* p, const float2* data, const void* 
 {
     const PlanGeom& g = p->g;
     if (g.n == 0) return TCV_OK;
-    if (!g.var || g.tw != kDTW || g.th != kDTH) return TCV_ERR_UNSUPPORTED;
+    if (!g.var || g.tw != kDTW || g.th != kDTH || g.s > 4095) return TCV_ERR_UNSUPPORTED;  // widths: 12 bits of a job
     const void* kernel = reinterpret_cast<const void*>(&dense_grid_kernel<Tab>);
     TCV_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGridSmem)));
     const int ctas = resident(kernel, kGThreads, kGridSmem);

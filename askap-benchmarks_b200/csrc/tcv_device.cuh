@@ -410,209 +410,6 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
     }
 }
 
-// ------------------------------------------------------------------------------------------
-// Staged gridding.  The same output-stationary tiles, work units and results as grid_tile_kernel,
-// but a warp's table rows travel through a private ring of kNS shared-memory stages filled by
-// asynchronous copies (cp.async, 4 or 8 bytes per lane and row, zero-filled outside the
-// footprint) instead of through registers: while the warp multiplies-adds one sample's rows out
-// of shared memory, the rows of the next kNS - 1 samples it meets are in flight, without the
-// registers a second set of loaded values would take.  Each lane copies and reads back only its
-// own column, so a lane waits on its own copies and needs no warp barrier.  Zero-filled entries
-// add fma(d, 0, acc) = acc: the sums are bit-identical to grid_tile_kernel's.
-// ------------------------------------------------------------------------------------------
-__device__ __forceinline__ u32 smem_addr(const void* p)
-{
-    unsigned long long a;
-    asm("cvta.to.shared.u64 %0, %1;" : "=l"(a) : "l"(p));
-    return u32(a);
-}
-
-// copy kBytes from global to shared, or write kBytes of zeros when src_bytes == 0
-template <int kBytes>
-__device__ __forceinline__ void cp_async_zfill(u32 dst, const void* src, int src_bytes)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(src), "n"(kBytes), "r"(src_bytes)
-                 : "memory");
-}
-// the same with compile-time byte offsets added to both addresses (one base register per sample)
-template <int kBytes, int kDstOff, int kSrcOff>
-__device__ __forceinline__ void cp_async_zfill_imm(u32 dst, const void* src, int src_bytes)
-{
-    asm volatile("cp.async.ca.shared.global [%0+%3], [%1+%4], %2, %5;\n" ::"r"(dst), "l"(src), "n"(kBytes), "n"(kDstOff),
-                 "n"(kSrcOff), "r"(src_bytes)
-                 : "memory");
-}
-// rows r .. kR-1 of a full-row sample: row r of the lane's column at row0 + r * kS entries, into
-// ring row r (32 entries apart)
-template <class E, int kS, int kR, int r>
-struct StageRows {
-    __device__ __forceinline__ static void issue(u32 dst, const E* row0, int nb)
-    {
-        cp_async_zfill_imm<int(sizeof(E)), r * 32 * int(sizeof(E)), r * kS * int(sizeof(E))>(dst, row0, nb);
-        StageRows<E, kS, kR, r + 1>::issue(dst, row0, nb);
-    }
-};
-template <class E, int kS, int kR>
-struct StageRows<E, kS, kR, kR> {
-    __device__ __forceinline__ static void issue(u32, const E*, int) {}
-};
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int kPending>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(kPending) : "memory"); }
-
-// dynamic shared memory of the staged kernels: kTileWarps rings of kNS stages of kR rows x 32 entries
-template <class Tab, int kR, int kNS>
-__host__ __device__ constexpr int stage_smem_bytes() { return kTileWarps * kNS * kR * 32 * int(sizeof(typename Tab::elem)); }
-
-// CTAs per SM the staged kernel's registers are sized for: two-stage rings at four CTAs (64
-// registers), three-stage rings at three (85 registers; the rings then take the shared memory)
-template <int kR, int kNS>
-__host__ __device__ constexpr int stage_min_blocks() { return kR >= 16 ? (kNS >= 3 ? 3 : 4) : 6; }
-
-template <class Tab, int kS, int kR, int kNS>
-__global__ void __launch_bounds__(kTileThreads, stage_min_blocks<kR, kNS>())
-grid_stage_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
-                  const int* __restrict__ iu, const int* __restrict__ iv,
-                  const int* __restrict__ coff, const u32* __restrict__ order,
-                  const uint4* __restrict__ units, const u32* __restrict__ group_ustart, GridArgs a)
-{
-    using E = typename Tab::elem;
-    constexpr int kTH = tile_height(kR);
-    constexpr int kStage = kR * 32;  // entries of one stage
-    extern __shared__ __align__(16) unsigned char stage_sm[];
-    __shared__ float4 sm_rec[2][kTileChunk];  // (data.re, data.im, first column, first row)
-    __shared__ int sm_coff[2][kTileChunk];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s0 = kS > 0 ? kS : a.s;
-    const u32 i1 = group_ustart[a.group + 1];
-    E* ring = reinterpret_cast<E*>(stage_sm) + warp * (kNS * kStage);
-    const u32 ring_sa = smem_addr(ring) + u32(lane * int(sizeof(E)));
-    auto stage = [&](const ChunkCursor& c, int buf) {
-        if (int(threadIdx.x) < c.m) {
-            const u32 k = order[c.start + c.base + threadIdx.x];
-            const float2 d = data[k];
-            sm_rec[buf][threadIdx.x] = make_float4(d.x * a.c_scale, d.y * a.c_scale, __int_as_float(iu[k] - a.support),
-                                                   __int_as_float(iv[k]));
-            sm_coff[buf][threadIdx.x] = coff[k];
-        }
-    };
-    ChunkCursor cur;
-    cursor_load(cur, group_ustart[a.group] + blockIdx.x, i1, units, a);
-    stage(cur, 0);
-    __syncthreads();
-    float2 acc[kR];
-#pragma unroll
-    for (int r = 0; r < kR; ++r) acc[r] = make_float2(0.f, 0.f);
-    // samples in flight (issued, not yet added): nq of them from ring slot qhead on; each lane
-    // keeps their data values beside its own column of the ring
-    __shared__ float2 sm_dv[kTileWarps][kNS][32];
-    int nq = 0, qhead = 0;
-    auto add_oldest = [&]() {
-        const E* sp = ring + qhead * kStage + lane;
-        const float2 dv = sm_dv[warp][qhead][lane];
-        // in groups of 8 rows: the compiler may not hoist every row's load above the first adds
-        // (the loaded values would otherwise take as many registers as the accumulators)
-#pragma unroll
-        for (int r0 = 0; r0 < kR; r0 += 8) {
-#pragma unroll
-            for (int r = r0; r < r0 + 8 && r < kR; ++r) cmac<Tab::kReal>(acc[r], dv, Tab::cvt(sp[r * 32]));
-            asm volatile("" ::: "memory");
-        }
-        qhead = qhead + 1 == kNS ? 0 : qhead + 1;
-        --nq;
-    };
-    int buf = 0;
-    while (cur.m > 0) {
-        ChunkCursor nxt = cur;
-        cursor_next(nxt, i1, units, a);
-        stage(nxt, buf ^ 1);  // overlaps with the work below
-
-        const int tx = rec_tx(cur.ti), ty = rec_ty(cur.ti);
-        const int bx0 = tx * kTileW + (warp % (kTileW / 32)) * 32;
-        const int gx = bx0 + lane;
-        const int gy0 = ty * kTH + (warp / (kTileW / 32)) * kR;
-        for (int j = 0; j < cur.m; ++j) {
-            const float4 q = sm_rec[buf][j];
-            const int s = s0;
-            const int fx = __float_as_int(q.z), fy = __float_as_int(q.w);
-            const int dy0 = gy0 - fy;
-            if (dy0 >= s || dy0 + kR <= 0) continue;      // warp-uniform
-            if (fx > bx0 + 31 || fx + s <= bx0) continue;  // warp-uniform
-            if (nq == kNS) {
-                cp_async_wait<kNS - 1>();
-                add_oldest();
-            }
-            int slot = qhead + nq;
-            slot = slot >= kNS ? slot - kNS : slot;
-            const int dx = gx - fx;
-            const bool colok = unsigned(dx) < unsigned(s);
-            // lanes outside the footprint copy zeros; their source address is kept inside the
-            // sample's kernel (column clamped to the footprint) although nothing is read from it
-            const int dxc = dx < 0 ? 0 : (dx >= s ? s - 1 : dx);
-            const E* src = ctab + (sm_coff[buf][j] + dxc);
-            const u32 dst = ring_sa + u32(slot * kStage * int(sizeof(E)));
-            const int nb = colok ? int(sizeof(E)) : 0;
-            if (dy0 >= 0 && dy0 + kR <= s) {
-                const E* row0 = src + dy0 * s;
-                if constexpr (kS > 0) {
-                    StageRows<E, kS, kR, 0>::issue(dst, row0, nb);
-                } else {
-#pragma unroll
-                    for (int r = 0; r < kR; ++r)
-                        cp_async_zfill<int(sizeof(E))>(dst + u32(r * 32 * int(sizeof(E))), row0 + r * s, nb);
-                }
-            } else {
-#pragma unroll
-                for (int r = 0; r < kR; ++r) {
-                    const int fr = dy0 + r;  // footprint row, clamped likewise
-                    const bool ok = unsigned(fr) < unsigned(s);
-                    cp_async_zfill<int(sizeof(E))>(dst + u32(r * 32 * int(sizeof(E))),
-                                                   src + (fr < 0 ? 0 : (fr >= s ? s - 1 : fr)) * s, ok ? nb : 0);
-                }
-            }
-            cp_async_commit();
-            sm_dv[warp][slot][lane] = make_float2(q.x, q.y);
-            ++nq;
-        }
-        const bool unit_done = nxt.it != cur.it || nxt.m == 0;
-        if (unit_done) {
-            cp_async_wait<0>();
-            while (nq > 0) add_oldest();
-        }
-        if (unit_done && cur.pslot != kDirect) {
-            float2* pt = a.partial + (unsigned long long)(cur.pslot) * (kTileW * kTH) +
-                         ((warp / (kTileW / 32)) * kR) * kTileW + (warp % (kTileW / 32)) * 32 + lane;
-#pragma unroll
-            for (int r = 0; r < kR; ++r) {
-                pt[r * kTileW] = acc[r];
-                acc[r] = make_float2(0.f, 0.f);
-            }
-        } else if (unit_done) {
-            const JobDesc& jd = a.jobs[rec_job(cur.ti)];
-            const int gs = jd.g_size;
-            float2* grid = a.grid ? a.grid : jd.grid;
-            if (gx < gs) {
-#pragma unroll
-                for (int r = 0; r < kR; ++r) {
-                    const int gy = gy0 + r;
-                    if (gy < gs) {
-                        float2* gp = grid + ((unsigned long long)(gy) * gs + gx);
-                        float2 v = *gp;
-                        v.x += acc[r].x;
-                        v.y += acc[r].y;
-                        *gp = v;
-                    }
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < kR; ++r) acc[r] = make_float2(0.f, 0.f);
-        }
-        __syncthreads();  // the next chunk is staged; this chunk's records are free
-        cur = nxt;
-        buf ^= 1;
-    }
-}
-
 // Fold the partial tiles of the split cells of one plane group into the grid: for every point,
 // the units' partial sums in unit order, then one add into the grid (deterministic).  Work items
 // are (cell, 256-point slice of its tile), block-stride over the group's non-empty cells; cells
