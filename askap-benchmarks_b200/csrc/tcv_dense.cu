@@ -10,14 +10,16 @@
 // of its first element, rows per step), so a warp only walks it.
 //
 // Gridding: each 32-column half of the 64 x 32 tile has four warps with private copies of the
-// half in shared memory (8 KB each, no two warps write one copy: no atomics); sample j is added by
-// warp j mod 4 of each half it meets.  A warp keeps the next sample's first table loads in flight
-// while it updates its copy with the current one (a two-stage software pipeline).  At the end of
-// the unit the copies are added in warp order into the grid, or into the unit's partial tile for
-// a split cell (fold_kernel then adds those in unit order, as for the tile kernels).
-// Degridding: the grid tile is staged in shared memory once per unit; sample j is taken by warp
-// j mod 8, which reduces its products across the warp into the sample's slot for the tile
-// (slot_reduce_kernel adds the slots in tile order).
+// half in shared memory (8 KB each, no two warps write one copy: no atomics).  A chunk of samples
+// is staged as jobs, one per (sample, half it meets), packed per half so that a half's warps see
+// only the samples that meet it; job i of a half is added by warp i mod 4 of that half.  A warp
+// keeps the next job's first table loads in flight while it updates its copy with the current one
+// (a two-stage software pipeline), and the next chunk is staged while this one is added.  At the
+// end of the unit the copies are added in warp order into the grid, or into the unit's partial
+// tile for a split cell (fold_kernel then adds those in unit order, as for the tile kernels).
+// Degridding: the grid tile is staged in shared memory once per unit; a warp takes four samples
+// at a time and reduces their products across the warp together (one transposing reduction) into
+// the samples' slots for the tile (slot_reduce_kernel adds the slots in tile order).
 //
 // Every sum is taken in a fixed order, so results are deterministic; they group the reference's
 // per-point sums differently (by warp), which moves them by FP32 rounding only.  Tiles are the
@@ -105,14 +107,14 @@ __device__ __forceinline__ void build_grid_lut(unsigned short (&gl)[33][32], int
     }
 }
 
-// The gridding kernel's position in its work: unit list position, first sample of the chunk in
-// that unit, the unit's sample range, tile record and partial tile, and the chunk's sample count
-// (0: no more work).  Chunks are kGChunk samples.
-constexpr int kGChunk = 128;
+// A kernel's position in its work: unit list position, first sample of the chunk in that unit, the
+// unit's sample range, tile record and partial tile, and the chunk's sample count (0: no more
+// work).  Chunks are kChunk samples.
 struct DChunk {
     u32 it, base, cnt, start, ti, pslot;
     int m;
 };
+template <int kChunk>
 __device__ __forceinline__ void dchunk_load(DChunk& c, u32 it, u32 i1, const uint4* __restrict__ units,
                                             const GridArgs& a)
 {
@@ -125,19 +127,21 @@ __device__ __forceinline__ void dchunk_load(DChunk& c, u32 it, u32 i1, const uin
         c.cnt = u.z;
         c.pslot = u.w;
         c.ti = a.tinfo[u.x - u32(a.group) * u32(a.ntiles)];
-        c.m = int(c.cnt < u32(kGChunk) ? c.cnt : u32(kGChunk));
+        c.m = int(c.cnt < u32(kChunk) ? c.cnt : u32(kChunk));
     }
 }
+template <int kChunk>
 __device__ __forceinline__ void dchunk_next(DChunk& c, u32 i1, const uint4* __restrict__ units, const GridArgs& a)
 {
-    if (c.base + u32(kGChunk) < c.cnt) {
-        c.base += u32(kGChunk);
+    if (c.base + u32(kChunk) < c.cnt) {
+        c.base += u32(kChunk);
         const u32 left = c.cnt - c.base;
-        c.m = int(left < u32(kGChunk) ? left : u32(kGChunk));
+        c.m = int(left < u32(kChunk) ? left : u32(kChunk));
     } else {
-        dchunk_load(c, c.it + gridDim.x, i1, units, a);
+        dchunk_load<kChunk>(c, c.it + gridDim.x, i1, units, a);
     }
 }
+constexpr int kGChunk = 128;  // gridding: samples staged per round
 
 // Gridding.  The tile's two 32-column halves each have kGWarps / 2 warps with private copies of the
 // half.  A chunk of kGChunk samples is staged as jobs, one per (sample, half it meets): thread t
@@ -161,7 +165,7 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
     constexpr int kHPts = kHalf * kDTH;        // 1024 points per half
     constexpr int kPerHalf = kGWarps / 2;      // warps per half
     constexpr int kSegs = kGChunk / 32;        // staging warps per half
-    constexpr int U = 4;                       // table loads of a job issued together
+    constexpr int U = 3;                       // table loads of a job issued together
     static_assert(kSegs == 4 && 2 * kGChunk == kGThreads, "one staging thread per (sample, half)");
     extern __shared__ __align__(16) float2 dsm[];
     float2* acc_all = dsm;                                                    // [kGWarps][kHPts]
@@ -283,13 +287,13 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
 
     const u32 i1 = group_ustart[a.group + 1];
     DChunk cur;
-    dchunk_load(cur, group_ustart[a.group] + blockIdx.x, i1, units, a);
+    dchunk_load<kGChunk>(cur, group_ustart[a.group] + blockIdx.x, i1, units, a);
     stage(cur, 0);
     __syncthreads();  // the first chunk is staged (and the lane table built)
     int buf = 0;
     while (cur.m > 0) {
         DChunk nxt = cur;
-        dchunk_next(nxt, i1, units, a);
+        dchunk_next<kGChunk>(nxt, i1, units, a);
         stage(nxt, buf ^ 1);  // the next chunk, while this one is added
         consume(buf);
         if (nxt.it != cur.it || nxt.m == 0) {  // the unit is done (block-uniform)
@@ -332,6 +336,12 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
     }
 }
 
+// Degridding.  The unit's grid tile is staged in shared memory; a chunk of kDThreads samples is
+// staged as rectangles (prepare) with their slot indices, the next chunk while this one is read
+// (two buffers, one barrier per chunk).  Warp w takes samples 4g .. 4g + 3 for g = w, w + 8, ...:
+// each lane's partial products of the four, then one transposing warp reduction for all four
+// (6 complex shuffles instead of 20), which sums each sample over the lanes in the same tree as a
+// plain butterfly.
 template <class Tab>
 __global__ void __launch_bounds__(kDThreads)
 dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int* __restrict__ iu,
@@ -340,71 +350,101 @@ dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int* __re
                     float2* __restrict__ slots, int max_tiles, GridArgs a)
 {
     __shared__ float2 gt[kDPts];           // the grid tile
-    __shared__ DenseRec rec[kDThreads];
-    __shared__ unsigned long long rslot[kDThreads];  // slot index of (sample, this tile)
+    __shared__ DenseRec rec[2][kDThreads];
+    __shared__ unsigned long long rslot[2][kDThreads];  // slot index of (sample, this tile)
     __shared__ DenseLut L;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     build_lut(L, threadIdx.x, kDThreads);
-    const u32 i1 = group_ustart[a.group + 1];
-    for (u32 it = group_ustart[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
-        const uint4 u = units[it];
-        const u32 start = u.y, cnt = u.z;
-        const u32 ti = a.tinfo[u.x - u32(a.group) * u32(a.ntiles)];
-        const int tx = rec_tx(ti), ty = rec_ty(ti);
-        const int tx0 = tx * kDTW, ty0 = ty * kDTH;
+    __syncthreads();  // the lane table is built (the staging reads it)
+    auto stage = [&](const DChunk& c, int buf) {
+        if (int(threadIdx.x) < c.m) {
+            const u32 k = order[c.start + c.base + threadIdx.x];
+            const int sk = int(a.ssz[k]);
+            const int fx = iu[k] - sk / 2, fy = iv[k];
+            const int tx = rec_tx(c.ti), ty = rec_ty(c.ti);
+            rec[buf][threadIdx.x] = prepare(coff[k], sk, fx, fy, tx * kDTW, ty * kDTH, L);
+            const int sx0 = fx / kDTW, sx1 = (fx + sk - 1) / kDTW, sy0 = fy / kDTH;
+            rslot[buf][threadIdx.x] = (unsigned long long)(k) * max_tiles + (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0);
+        }
+    };
+    auto load_tile = [&](u32 ti) {
         const JobDesc& jd = a.jobs[rec_job(ti)];
         const int gs = jd.g_size;
         const float2* grid = a.grid ? a.grid : jd.grid;
-        __syncthreads();  // the previous unit is done with gt and the records
+        const int tx0 = rec_tx(ti) * kDTW, ty0 = rec_ty(ti) * kDTH;
         for (int p = threadIdx.x; p < kDPts; p += kDThreads) {
             const int gx = tx0 + (p % kDTW), gy = ty0 + (p / kDTW);
             gt[p] = (gx < gs && gy < gs) ? grid[(unsigned long long)(gy) * gs + gx] : make_float2(0.f, 0.f);
         }
-        for (u32 base = 0; base < cnt; base += kDThreads) {
-            const int m = int(cnt - base < u32(kDThreads) ? cnt - base : u32(kDThreads));
-            __syncthreads();
-            if (int(threadIdx.x) < m) {
-                const u32 k = order[start + base + threadIdx.x];
-                const int sk = int(a.ssz[k]);
-                const int fx = iu[k] - sk / 2, fy = iv[k];
-                rec[threadIdx.x] = prepare(coff[k], sk, fx, fy, tx0, ty0, L);
-                const int sx0 = fx / kDTW, sx1 = (fx + sk - 1) / kDTW, sy0 = fy / kDTH;
-                rslot[threadIdx.x] = (unsigned long long)(k) * max_tiles + (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0);
+    };
+    // the partial dot product of this lane with sample j's rectangle
+    auto partial = [&](int buf, int j) -> float2 {
+        const DenseRec d = rec[buf][j];
+        const int w = d.shape & 255, h = (d.shape >> 8) & 255, kk = d.shape >> 16;
+        float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);  // two FMA chains
+        if (h > 0 && w <= 32) {
+            const int qq = L.q[w][lane], rr = L.r[w][lane];
+            const bool lane_ok = qq < kk;
+            const int cbase = d.c0 + qq * d.s + rr, pbase = d.p0 + qq * kDTW + rr;
+            for (int row0 = 0; row0 < h; row0 += 2 * kk) {
+                const bool oka = lane_ok && row0 + qq < h, okb = lane_ok && row0 + kk + qq < h;
+                if (oka) cmac<Tab::kReal>(p0, gt[pbase + row0 * kDTW], Tab::load(ctab + (cbase + row0 * d.s)));
+                if (okb)
+                    cmac<Tab::kReal>(p1, gt[pbase + (row0 + kk) * kDTW], Tab::load(ctab + (cbase + (row0 + kk) * d.s)));
             }
-            __syncthreads();
-            for (int j = warp; j < m; j += kDWarps) {
-                const DenseRec d = rec[j];
-                const int w = d.shape & 255, h = (d.shape >> 8) & 255, kk = d.shape >> 16;
-                float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);  // two FMA chains
-                if (h > 0 && w <= 32) {
-                    const int qq = L.q[w][lane], rr = L.r[w][lane];
-                    const bool lane_ok = qq < kk;
-                    const int cbase = d.c0 + qq * d.s + rr, pbase = d.p0 + qq * kDTW + rr;
-                    for (int row0 = 0; row0 < h; row0 += 2 * kk) {
-                        const bool oka = lane_ok && row0 + qq < h, okb = lane_ok && row0 + kk + qq < h;
-                        if (oka) cmac<Tab::kReal>(p0, gt[pbase + row0 * kDTW], Tab::load(ctab + (cbase + row0 * d.s)));
-                        if (okb)
-                            cmac<Tab::kReal>(p1, gt[pbase + (row0 + kk) * kDTW],
-                                             Tab::load(ctab + (cbase + (row0 + kk) * d.s)));
-                    }
-                } else if (h > 0) {
-                    const bool oka = lane < w, okb = lane + 32 < w;
-                    for (int row = 0; row < h; ++row) {
-                        if (oka) cmac<Tab::kReal>(p0, gt[d.p0 + row * kDTW + lane], Tab::load(ctab + (d.c0 + row * d.s + lane)));
-                        if (okb)
-                            cmac<Tab::kReal>(p1, gt[d.p0 + row * kDTW + lane + 32],
-                                             Tab::load(ctab + (d.c0 + row * d.s + lane + 32)));
-                    }
-                }
-                float2 v = make_float2(p0.x + p1.x, p0.y + p1.y);
-#pragma unroll
-                for (int o = 16; o; o >>= 1) {
-                    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-                    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-                }
-                if (lane == 0) slots[rslot[j]] = v;  // an empty overlap writes its empty slot
+        } else if (h > 0) {
+            const bool oka = lane < w, okb = lane + 32 < w;
+            for (int row = 0; row < h; ++row) {
+                if (oka) cmac<Tab::kReal>(p0, gt[d.p0 + row * kDTW + lane], Tab::load(ctab + (d.c0 + row * d.s + lane)));
+                if (okb)
+                    cmac<Tab::kReal>(p1, gt[d.p0 + row * kDTW + lane + 32],
+                                     Tab::load(ctab + (d.c0 + row * d.s + lane + 32)));
             }
         }
+        return make_float2(p0.x + p1.x, p0.y + p1.y);
+    };
+    const u32 i1 = group_ustart[a.group + 1];
+    DChunk cur;
+    dchunk_load<kDThreads>(cur, group_ustart[a.group] + blockIdx.x, i1, units, a);
+    stage(cur, 0);
+    if (cur.m > 0) load_tile(cur.ti);
+    __syncthreads();
+    int buf = 0;
+    while (cur.m > 0) {
+        DChunk nxt = cur;
+        dchunk_next<kDThreads>(nxt, i1, units, a);
+        stage(nxt, buf ^ 1);  // the next chunk, while this one is read
+        for (int g0 = warp * 4; g0 < cur.m; g0 += kDWarps * 4) {
+            float2 v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) v[e] = g0 + e < cur.m ? partial(buf, g0 + e) : make_float2(0.f, 0.f);  // warp-uniform
+            // exchange over lane bit 4 (lanes keep samples 0,1 or 2,3) and bit 3 (one sample each):
+            // lane holds sample (lane >> 3) & 3 summed over 4 lanes; butterflies over bits 2..0 finish
+            const bool h16 = (lane & 16) != 0, h8 = (lane & 8) != 0;
+            const float2 s0 = h16 ? v[0] : v[2], k0 = h16 ? v[2] : v[0];
+            const float2 s1 = h16 ? v[1] : v[3], k1 = h16 ? v[3] : v[1];
+            const float2 w0 = make_float2(k0.x + __shfl_xor_sync(0xffffffffu, s0.x, 16),
+                                          k0.y + __shfl_xor_sync(0xffffffffu, s0.y, 16));
+            const float2 w1 = make_float2(k1.x + __shfl_xor_sync(0xffffffffu, s1.x, 16),
+                                          k1.y + __shfl_xor_sync(0xffffffffu, s1.y, 16));
+            const float2 sd = h8 ? w0 : w1, kp = h8 ? w1 : w0;
+            float2 y = make_float2(kp.x + __shfl_xor_sync(0xffffffffu, sd.x, 8),
+                                   kp.y + __shfl_xor_sync(0xffffffffu, sd.y, 8));
+#pragma unroll
+            for (int o = 4; o; o >>= 1) {
+                y.x += __shfl_xor_sync(0xffffffffu, y.x, o);
+                y.y += __shfl_xor_sync(0xffffffffu, y.y, o);
+            }
+            const int js = g0 + (lane >> 3);
+            if ((lane & 7) == 0 && js < cur.m) slots[rslot[buf][js]] = y;  // an empty overlap writes its empty slot
+        }
+        if (nxt.m > 0 && nxt.it != cur.it) {  // a new unit: its grid tile (block-uniform)
+            __syncthreads();  // every warp is done with this tile
+            load_tile(nxt.ti);
+        }
+        __syncthreads();  // the next chunk (and tile) is staged; this chunk's records are free
+        cur = nxt;
+        buf ^= 1;
     }
 }
 
