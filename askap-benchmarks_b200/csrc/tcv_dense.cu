@@ -10,13 +10,13 @@
 // of its first element, rows per step), so a warp only walks it.
 //
 // Gridding: each 32-column half of the 64 x 32 tile has four warps with private copies of the
-// half in shared memory (8 KB each, no two warps write one copy: no atomics).  A chunk of samples
-// is staged as jobs, one per (sample, half it meets), packed per half so that a half's warps see
-// only the samples that meet it; job i of a half is added by warp i mod 4 of that half.  A warp
-// keeps the next job's first table loads in flight while it updates its copy with the current one
-// (a two-stage software pipeline), and the next chunk is staged while this one is added.  At the
-// end of the unit the copies are added in warp order into the grid, or into the unit's partial
-// tile for a split cell (fold_kernel then adds those in unit order, as for the tile kernels).
+// half in shared memory (8 KB each, no two warps write one copy: no atomics).  The warps work
+// independently: each takes every fourth group of 32 samples of the unit, stages them as jobs
+// for its half (one per sample that meets the half) and adds them into its copy, keeping the next
+// job's first table loads in flight while it adds the current one (a two-stage software
+// pipeline).  At the end of the unit the four warps of a half meet (a named barrier) and add
+// their copies in warp order into the grid, or into the unit's partial tile for a split cell
+// (fold_kernel then adds those in unit order, as for the tile kernels).
 // Degridding: the grid tile is staged in shared memory once per unit; a warp takes four samples
 // at a time and reduces their products across the warp together (one transposing reduction) into
 // the samples' slots for the tile (slot_reduce_kernel adds the slots in tile order).
@@ -141,18 +141,29 @@ __device__ __forceinline__ void dchunk_next(DChunk& c, u32 i1, const uint4* __re
         dchunk_load<kChunk>(c, c.it + gridDim.x, i1, units, a);
     }
 }
-constexpr int kGChunk = 128;  // gridding: samples staged per round
-
 // Gridding.  The tile's two 32-column halves each have kGWarps / 2 warps with private copies of the
-// half.  A chunk of kGChunk samples is staged as jobs, one per (sample, half it meets): thread t
-// prepares sample t % kGChunk for half t / kGChunk, and the jobs of a staging warp are packed in
-// sample order into its 32-entry segment of the half's list (ballot), so a half's warps see only
-// the samples that meet it.  A job is the table index of the first element of the sample's
-// rectangle in the half, and first point | (width - 1) << 10 | (height - 1) << 15 | table row
-// stride << 20, and the scaled data value.  Warp j of a half takes jobs j, j + 4, ... of the
-// half's list (segments in order).  The next chunk is staged while this one is added (two
-// buffers, one barrier per chunk); each warp keeps the next job's first table loads in flight
-// while it adds the current one.
+// half.  The warps work independently: warp j of a half takes samples 32 j + 128 i + [0, 32) of
+// the unit (i = 0, 1, ...), stages them as jobs for its half (one per sample that meets it: the
+// table index of the first element of the sample's rectangle in the half, and first point |
+// (width - 1) << 10 | (height - 1) << 15 | table row stride << 20, and the scaled data value),
+// packed in sample order by ballot into its own 32-entry list, and adds them into its copy,
+// keeping the next job's first table loads in flight while it adds the current one.  Only the
+// four warps of a half meet, at the end of each unit (a named barrier per half), to add their
+// copies in warp order into the grid or the unit's partial tile.
+// the sorted-order entry at position pos of a unit (0 past its end)
+__device__ __forceinline__ u32 base0_k(const u32* __restrict__ order, u32 start, u32 cnt, u32 pos)
+{
+    return pos < cnt ? order[start + pos] : 0u;
+}
+
+__device__ __forceinline__ void half_barrier(int half)
+{
+    if (half == 0)
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+    else
+        asm volatile("bar.sync 2, 128;" ::: "memory");
+}
+
 template <class Tab>
 __global__ void __launch_bounds__(kGThreads, 3)
 dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
@@ -164,46 +175,19 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
     constexpr int kHalf = kDTW / 2;            // 32 columns
     constexpr int kHPts = kHalf * kDTH;        // 1024 points per half
     constexpr int kPerHalf = kGWarps / 2;      // warps per half
-    constexpr int kSegs = kGChunk / 32;        // staging warps per half
     constexpr int U = 3;                       // table loads of a job issued together
-    static_assert(kSegs == 4 && 2 * kGChunk == kGThreads, "one staging thread per (sample, half)");
+    static_assert(kPerHalf * 32 == 128, "a half's warps meet at a 128-thread named barrier");
     extern __shared__ __align__(16) float2 dsm[];
     float2* acc_all = dsm;                                                    // [kGWarps][kHPts]
-    int4* jobs = reinterpret_cast<int4*>(dsm + kGWarps * kHPts);             // [2][2][kGChunk]
-    __shared__ int jcnt[2][2][kSegs];
+    int4* jobs_all = reinterpret_cast<int4*>(dsm + kGWarps * kHPts);         // [kGWarps][32]
     __shared__ unsigned short gl[33][32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int half = warp / kPerHalf, sub = warp % kPerHalf;
+    const int half = warp / kPerHalf, sub = warp % kPerHalf, hx0 = half * kHalf;
     build_grid_lut(gl, threadIdx.x, kGThreads);
     float2* acc = acc_all + warp * kHPts;
+    int4* jl = jobs_all + warp * 32;
     for (int i = lane; i < kHPts; i += 32) acc[i] = make_float2(0.f, 0.f);
-
-    const int si = threadIdx.x % kGChunk, sh = threadIdx.x / kGChunk;
-    auto stage = [&](const DChunk& c, int buf) {
-        bool has = false;
-        int4 jb = make_int4(0, 0, 0, 0);
-        if (si < c.m) {
-            const u32 k = order[c.start + c.base + si];
-            const int sk = int(a.ssz[k]);
-            const int fx = iu[k] - sk / 2, fy = iv[k];
-            const int tx0 = rec_tx(c.ti) * kDTW, ty0 = rec_ty(c.ti) * kDTH;
-            const Rect R = clip(fx, fy, sk, tx0, ty0);
-            const int tc = fx + R.c0 - tx0, h = R.r1 - R.r0, hx0 = sh * kHalf;
-            const int lo = max(tc, hx0), hi = min(fx + R.c1 - tx0, hx0 + kHalf);
-            has = h > 0 && lo < hi;
-            if (has) {
-                const float2 d = data[k];
-                jb.x = coff[k] + R.r0 * sk + R.c0 + (lo - tc);
-                jb.y = int(u32((fy + R.r0 - ty0) * kHalf + lo - hx0) | u32(hi - lo - 1) << 10 | u32(h - 1) << 15 |
-                           u32(sk) << 20);
-                jb.z = __float_as_int(d.x * a.c_scale);
-                jb.w = __float_as_int(d.y * a.c_scale);
-            }
-        }
-        const u32 b = __ballot_sync(0xffffffffu, has);
-        if (has) jobs[(buf * 2 + sh) * kGChunk + (si & ~31) + __popc(b & ((1u << lane) - 1u))] = jb;
-        if (lane == 0) jcnt[buf][sh][si >> 5] = __popc(b);
-    };
+    __syncthreads();  // the lane table is built
 
     struct Job {
         const E* tp;   // the lane's first table entry
@@ -212,127 +196,137 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
         int kk, kks;   // rows per step, and table entries per step
         float2 dv;
     };
-    auto consume = [&](int buf) {
-        const int4* jl = jobs + (buf * 2 + half) * kGChunk;
-        const int c0 = jcnt[buf][half][0], c1 = jcnt[buf][half][1], c2 = jcnt[buf][half][2];
-        const int p1 = c0, p2 = p1 + c1, p3 = p2 + c2, n = p3 + jcnt[buf][half][3];
-        auto setup = [&](int i, Job& J) {
-            int sl = i;  // list position -> slot of its segment
-            if (i >= p1) sl += 32 - c0;
-            if (i >= p2) sl += 32 - c1;
-            if (i >= p3) sl += 32 - c2;
-            const int4 jb = jl[sl];
-            const u32 meta = u32(jb.y);
-            const int wc = int((meta >> 10) & 31u) + 1, s = int(meta >> 20);
-            const u32 lu = gl[wc][lane];
-            const int q = int(lu & 31u), r = int((lu >> 5) & 31u);
-            J.h = int((meta >> 15) & 31u) + 1;
-            J.kk = int(lu >> 10);
-            J.rem = q < J.kk ? J.h - q : 0;
-            J.tp = ctab + (jb.x + q * s + r);
-            J.ap = int(meta & 1023u) + q * kHalf + r;
-            J.kks = J.kk * s;
-            J.dv = make_float2(__int_as_float(jb.z), __int_as_float(jb.w));
-        };
-        auto load = [&](const Job& J, int e0, float2 (&cv)[U]) {
+    auto setup = [&](int i, Job& J) {
+        const int4 jb = jl[i];
+        const u32 meta = u32(jb.y);
+        const int wc = int((meta >> 10) & 31u) + 1, s = int(meta >> 20);
+        const u32 lu = gl[wc][lane];
+        const int q = int(lu & 31u), r = int((lu >> 5) & 31u);
+        J.h = int((meta >> 15) & 31u) + 1;
+        J.kk = int(lu >> 10);
+        J.rem = q < J.kk ? J.h - q : 0;
+        J.tp = ctab + (jb.x + q * s + r);
+        J.ap = int(meta & 1023u) + q * kHalf + r;
+        J.kks = J.kk * s;
+        J.dv = make_float2(__int_as_float(jb.z), __int_as_float(jb.w));
+    };
+    auto load = [&](const Job& J, int e0, float2 (&cv)[U]) {
 #pragma unroll
-            for (int e = 0; e < U; ++e) {
-                const int ro = (e0 + e) * J.kk;
-                if (ro >= J.h) break;  // warp-uniform
-                cv[e] = ro < J.rem ? Tab::load(J.tp + (e0 + e) * J.kks) : make_float2(0.f, 0.f);
-            }
-        };
-        auto apply = [&](const Job& J, int e0, const float2 (&cv)[U]) {
+        for (int e = 0; e < U; ++e) {
+            const int ro = (e0 + e) * J.kk;
+            cv[e] = ro < J.rem ? Tab::load(J.tp + (e0 + e) * J.kks) : make_float2(0.f, 0.f);
+        }
+    };
+    auto apply = [&](const Job& J, int e0, const float2 (&cv)[U]) {
+        // the steps' points are distinct: all their reads first, then the adds and writes
+        float2 t[U];
 #pragma unroll
-            for (int e = 0; e < U; ++e) {
-                const int ro = (e0 + e) * J.kk;
-                if (ro >= J.h) break;  // warp-uniform
-                if (ro < J.rem) {
-                    float2& gp = acc[J.ap + ro * kHalf];
-                    float2 t = gp;
-                    cmac<Tab::kReal>(t, J.dv, cv[e]);
-                    gp = t;
-                }
-            }
-        };
-        int i = sub;
-        if (i >= n) return;
-        Job cur;
-        float2 cv[U];
-        setup(i, cur);
-        load(cur, 0, cv);
-        for (;;) {
-            const int inx = i + kPerHalf;
-            const bool more = inx < n;
-            Job nx;
-            float2 nv[U];
-            if (more) {  // in flight during the updates below
-                setup(inx, nx);
-                load(nx, 0, nv);
-            }
-            apply(cur, 0, cv);
-            for (int e0 = U; e0 * cur.kk < cur.h; e0 += U) {  // tall rectangles (warp-uniform)
-                float2 t[U];
-                load(cur, e0, t);
-                apply(cur, e0, t);
-            }
-            __syncwarp();  // this job's updates land before another lane reads them for the next
-            if (!more) break;
-            cur = nx;
-            i = inx;
+        for (int e = 0; e < U; ++e) {
+            const int ro = (e0 + e) * J.kk;
+            if (ro < J.rem) t[e] = acc[J.ap + ro * kHalf];
+        }
 #pragma unroll
-            for (int e = 0; e < U; ++e) cv[e] = nv[e];
+        for (int e = 0; e < U; ++e) {
+            const int ro = (e0 + e) * J.kk;
+            if (ro < J.rem) {
+                cmac<Tab::kReal>(t[e], J.dv, cv[e]);
+                acc[J.ap + ro * kHalf] = t[e];
+            }
         }
     };
 
     const u32 i1 = group_ustart[a.group + 1];
-    DChunk cur;
-    dchunk_load<kGChunk>(cur, group_ustart[a.group] + blockIdx.x, i1, units, a);
-    stage(cur, 0);
-    __syncthreads();  // the first chunk is staged (and the lane table built)
-    int buf = 0;
-    while (cur.m > 0) {
-        DChunk nxt = cur;
-        dchunk_next<kGChunk>(nxt, i1, units, a);
-        stage(nxt, buf ^ 1);  // the next chunk, while this one is added
-        consume(buf);
-        if (nxt.it != cur.it || nxt.m == 0) {  // the unit is done (block-uniform)
-            __syncthreads();  // every warp's copy is complete
-            // each half's copies in warp order, into the grid (a whole cell) or the unit's partial tile
-            const JobDesc& jd = a.jobs[rec_job(cur.ti)];
-            const int gs = jd.g_size;
-            float2* grid = a.grid ? a.grid : jd.grid;
-            const int tx0 = rec_tx(cur.ti) * kDTW, ty0 = rec_ty(cur.ti) * kDTH;
-            for (int p = threadIdx.x; p < kDPts; p += kGThreads) {
-                const int px = p % kDTW, py = p / kDTW;
-                const int hh = px / kHalf, hp = py * kHalf + (px % kHalf);
-                float2* c = acc_all + hh * kPerHalf * kHPts + hp;
-                float2 v = c[0];
-#pragma unroll
-                for (int w = 1; w < kPerHalf; ++w) {
-                    const float2 o = c[w * kHPts];
-                    v.x += o.x;
-                    v.y += o.y;
+    for (u32 it = group_ustart[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
+        const uint4 u = units[it];
+        const u32 start = u.y, cnt = u.z, pslot = u.w;
+        const u32 ti = a.tinfo[u.x - u32(a.group) * u32(a.ntiles)];
+        const int tx0 = rec_tx(ti) * kDTW, ty0 = rec_ty(ti) * kDTH;
+        u32 kn = base0_k(order, start, cnt, u32(sub) * 32u + u32(lane));
+        for (u32 base = u32(sub) * 32u; base < cnt; base += u32(kPerHalf) * 32u) {
+            bool has = false;
+            int4 jb = make_int4(0, 0, 0, 0);
+            const u32 k = kn;
+            // the next samples' indices are read while this chunk is added
+            kn = base0_k(order, start, cnt, base + u32(kPerHalf) * 32u + u32(lane));
+            if (base + u32(lane) < cnt) {
+                const int sk = int(a.ssz[k]);
+                const int fx = iu[k] - sk / 2, fy = iv[k];
+                const Rect R = clip(fx, fy, sk, tx0, ty0);
+                const int tc = fx + R.c0 - tx0, h = R.r1 - R.r0;
+                const int lo = max(tc, hx0), hi = min(fx + R.c1 - tx0, hx0 + kHalf);
+                has = h > 0 && lo < hi;
+                if (has) {
+                    const float2 d = data[k];
+                    jb.x = coff[k] + R.r0 * sk + R.c0 + (lo - tc);
+                    jb.y = int(u32((fy + R.r0 - ty0) * kHalf + lo - hx0) | u32(hi - lo - 1) << 10 |
+                               u32(h - 1) << 15 | u32(sk) << 20);
+                    jb.z = __float_as_int(d.x * a.c_scale);
+                    jb.w = __float_as_int(d.y * a.c_scale);
                 }
-#pragma unroll
-                for (int w = 0; w < kPerHalf; ++w) c[w * kHPts] = make_float2(0.f, 0.f);
-                if (cur.pslot != kDirect) {
-                    a.partial[(unsigned long long)(cur.pslot) * kDPts + p] = v;
-                } else {
-                    const int gx = tx0 + px, gy = ty0 + py;
-                    if (gx < gs && gy < gs) {
-                        float2* gp = grid + ((unsigned long long)(gy) * gs + gx);
-                        float2 o = *gp;
-                        o.x += v.x;
-                        o.y += v.y;
-                        *gp = o;
+            }
+            const u32 b = __ballot_sync(0xffffffffu, has);
+            if (has) jl[__popc(b & ((1u << lane) - 1u))] = jb;
+            __syncwarp();
+            const int n = __popc(b);
+            if (n > 0) {
+                Job cur;
+                float2 cv[U];
+                setup(0, cur);
+                load(cur, 0, cv);
+                for (int i = 0;; ++i) {
+                    const bool more = i + 1 < n;
+                    Job nx;
+                    float2 nv[U];
+                    if (more) {  // in flight during the updates below
+                        setup(i + 1, nx);
+                        load(nx, 0, nv);
                     }
+                    apply(cur, 0, cv);
+                    for (int e0 = U; e0 * cur.kk < cur.h; e0 += U) {  // tall rectangles (warp-uniform)
+                        float2 t[U];
+                        load(cur, e0, t);
+                        apply(cur, e0, t);
+                    }
+                    __syncwarp();  // this job's updates land before another lane reads them for the next
+                    if (!more) break;
+                    cur = nx;
+#pragma unroll
+                    for (int e = 0; e < U; ++e) cv[e] = nv[e];
+                }
+            }
+            __syncwarp();  // the list is read before the next samples are packed into it
+        }
+        // the unit is done in this half: its copies in warp order into the grid or the partial tile
+        half_barrier(half);
+        const JobDesc& jd = a.jobs[rec_job(ti)];
+        const int gs = jd.g_size;
+        float2* grid = a.grid ? a.grid : jd.grid;
+        for (int p = int(threadIdx.x) & 127; p < kHPts; p += 128) {
+            float2* c = acc_all + half * kPerHalf * kHPts + p;
+            float2 v = c[0];
+#pragma unroll
+            for (int w = 1; w < kPerHalf; ++w) {
+                const float2 o = c[w * kHPts];
+                v.x += o.x;
+                v.y += o.y;
+            }
+#pragma unroll
+            for (int w = 0; w < kPerHalf; ++w) c[w * kHPts] = make_float2(0.f, 0.f);
+            const int px = hx0 + p % kHalf, py = p / kHalf;  // point in the tile
+            if (pslot != kDirect) {
+                a.partial[(unsigned long long)(pslot) * kDPts + py * kDTW + px] = v;
+            } else {
+                const int gx = tx0 + px, gy = ty0 + py;
+                if (gx < gs && gy < gs) {
+                    float2* gp = grid + ((unsigned long long)(gy) * gs + gx);
+                    float2 o = *gp;
+                    o.x += v.x;
+                    o.y += v.y;
+                    *gp = o;
                 }
             }
         }
-        __syncthreads();  // the next chunk is staged; this chunk's jobs are free; the copies are zero
-        cur = nxt;
-        buf ^= 1;
+        half_barrier(half);  // the copies are zero again before the next unit's adds
     }
 }
 
@@ -458,7 +452,7 @@ int resident(const void* kernel, int threads, size_t smem)
     return per_sm * sms;
 }
 
-constexpr size_t kGridSmem = size_t(kGWarps) * (kDPts / 2) * sizeof(float2) + size_t(2 * 2 * kGChunk) * sizeof(int4);
+constexpr size_t kGridSmem = size_t(kGWarps) * (kDPts / 2) * sizeof(float2) + size_t(kGWarps * 32) * sizeof(int4);
 
 GridArgs dense_args(const tcv_plan* p, int grp, float c_scale, float2* grid)
 {

@@ -293,7 +293,8 @@ grid_tile_kernel(const float2* __restrict__ data, const typename Tab::elem* __re
 // points in registers; for each sample of the cell a warp whose block meets the footprint forms
 // the partial dot product of its block with the table, four samples at a time reduced together
 // with shuffles, and the CTA adds its 8 warp partials in warp order into the sample's slot for
-// this tile.  A final pass
+// this tile.  The sample's staging thread marks the warps whose blocks meet the footprint and
+// those whose rows lie wholly inside it, so a warp tests one bit per sample.  A final pass
 // (slot_reduce_kernel) adds each sample's tile slots in tile order: no atomics, deterministic.
 template <class Tab, int kS, int kR, bool kVar = false>
 __global__ void __launch_bounds__(kTileThreads, degrid_min_blocks<Tab, kR>())
@@ -307,6 +308,9 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
     __shared__ int4 sm_rec[kTileChunk];              // (sample, first column, first row, cOffset)
     __shared__ float2 sm_part[kTileChunk][kTileWarps];
     __shared__ int sm_w[kVar ? kTileChunk : 1];      // per-sample widths
+    // per sample: the warps whose blocks it meets (bits 0..7) and those whose rows all lie
+    // inside its footprint (bits 8..15)
+    __shared__ unsigned short sm_mk[kTileChunk];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = kS > 0 ? kS : a.s;  // compile-time footprint width when specialised
     const u32 i1 = group_ustart[a.group + 1];
@@ -332,8 +336,26 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
             if (threadIdx.x < m) {
                 const u32 k = order[start + base + threadIdx.x];
                 const int sk = kVar ? int(a.ssz[k]) : s0;
-                sm_rec[threadIdx.x] = make_int4(int(k), iu[k] - (kVar ? sk / 2 : a.support), iv[k], coff[k]);
+                const int fx = iu[k] - (kVar ? sk / 2 : a.support), fy = iv[k];
+                sm_rec[threadIdx.x] = make_int4(int(k), fx, fy, coff[k]);
                 if (kVar) sm_w[kVar ? threadIdx.x : 0] = sk;
+                // warp w's block: columns tx*64 + (w % 2)*32 + [0, 32), rows ty*kTH + (w / 2)*kR + [0, kR)
+                const int bx = tx * kTileW - fx, by = ty * kTH - fy;
+                u32 cols = 0, rows = 0, full = 0;
+#pragma unroll
+                for (int h = 0; h < kTileW / 32; ++h) cols |= u32(bx + h * 32 < sk && bx + h * 32 + 32 > 0) << h;
+#pragma unroll
+                for (int r = 0; r < kTileWarps / (kTileW / 32); ++r) {
+                    rows |= u32(by + r * kR < sk && by + r * kR + kR > 0) << r;
+                    full |= u32(by + r * kR >= 0 && by + r * kR + kR <= sk) << r;
+                }
+                u32 mk = 0;
+#pragma unroll
+                for (int w = 0; w < kTileWarps; ++w) {
+                    mk |= (((cols >> (w % (kTileW / 32))) & (rows >> (w / (kTileW / 32)))) & 1u) << w;
+                    mk |= ((full >> (w / (kTileW / 32))) & 1u) << (8 + w);
+                }
+                sm_mk[threadIdx.x] = (unsigned short)mk;
             }
             __syncthreads();
             // four samples at a time: each lane's partial dot products of the four, then one
@@ -345,16 +367,17 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                     v[e] = make_float2(0.f, 0.f);
                     const int j = jg + e;
                     if (j >= m) continue;  // warp-uniform
+                    const u32 mk = sm_mk[j];
+                    if (!((mk >> warp) & 1u)) continue;  // warp-uniform: the block misses the footprint
                     const int4 q = sm_rec[j];
                     const int s = kVar ? sm_w[kVar ? j : 0] : s0;
                     const int fx = q.y, fy = q.z;
                     const int dy0 = gy0 - fy;
-                    if (dy0 >= s || dy0 + kR <= 0 || fx > bx0 + 31 || fx + s <= bx0) continue;  // warp-uniform
                     const int dx = gx - fx;
                     const bool colok = unsigned(dx) < unsigned(s);
                     const int ci = q.w + dy0 * s + dx;
                     float2 p0 = make_float2(0.f, 0.f), p1 = make_float2(0.f, 0.f);  // two FMA chains
-                    if (dy0 >= 0 && dy0 + kR <= s) {
+                    if ((mk >> (8 + warp)) & 1u) {  // every row of the block is inside the footprint
                         if (colok) {
 #pragma unroll
                             for (int r = 0; r < kR; r += 2) {
