@@ -392,7 +392,7 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                                 cmac<Tab::kReal>((r & 1) ? p1 : p0, gv[r], Tab::load(ctab + (ci + r * s)));
                         }
                     }
-                    v[e] = make_float2(p0.x + p1.x, p0.y + p1.y);
+                    v[e] = __fadd2_rn(p0, p1);
                 }
                 // exchange over lane bit 4 (lanes keep samples 0,1 or 2,3) and bit 3 (one sample
                 // each): lane holds sample (lane >> 3) & 3 summed over 4 lanes; butterflies over
@@ -400,18 +400,17 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                 const bool h16 = (lane & 16) != 0, h8 = (lane & 8) != 0;
                 const float2 s0 = h16 ? v[0] : v[2], k0 = h16 ? v[2] : v[0];
                 const float2 s1 = h16 ? v[1] : v[3], k1 = h16 ? v[3] : v[1];
-                const float2 w0 = make_float2(k0.x + __shfl_xor_sync(0xffffffffu, s0.x, 16),
-                                              k0.y + __shfl_xor_sync(0xffffffffu, s0.y, 16));
-                const float2 w1 = make_float2(k1.x + __shfl_xor_sync(0xffffffffu, s1.x, 16),
-                                              k1.y + __shfl_xor_sync(0xffffffffu, s1.y, 16));
+                // (paired adds: one instruction for the real and imaginary lanes, each rounded as fadd)
+                const float2 w0 = __fadd2_rn(k0, make_float2(__shfl_xor_sync(0xffffffffu, s0.x, 16),
+                                                             __shfl_xor_sync(0xffffffffu, s0.y, 16)));
+                const float2 w1 = __fadd2_rn(k1, make_float2(__shfl_xor_sync(0xffffffffu, s1.x, 16),
+                                                             __shfl_xor_sync(0xffffffffu, s1.y, 16)));
                 const float2 sd = h8 ? w0 : w1, kp = h8 ? w1 : w0;
-                float2 y = make_float2(kp.x + __shfl_xor_sync(0xffffffffu, sd.x, 8),
-                                       kp.y + __shfl_xor_sync(0xffffffffu, sd.y, 8));
+                float2 y = __fadd2_rn(kp, make_float2(__shfl_xor_sync(0xffffffffu, sd.x, 8),
+                                                      __shfl_xor_sync(0xffffffffu, sd.y, 8)));
 #pragma unroll
-                for (int o = 4; o; o >>= 1) {
-                    y.x += __shfl_xor_sync(0xffffffffu, y.x, o);
-                    y.y += __shfl_xor_sync(0xffffffffu, y.y, o);
-                }
+                for (int o = 4; o; o >>= 1)
+                    y = __fadd2_rn(y, make_float2(__shfl_xor_sync(0xffffffffu, y.x, o), __shfl_xor_sync(0xffffffffu, y.y, o)));
                 const int js = jg + (lane >> 3);
                 if ((lane & 7) == 0 && js < m) sm_part[js][warp] = y;
             }
@@ -420,10 +419,7 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                 const int4 q = sm_rec[threadIdx.x];
                 float2 v = sm_part[threadIdx.x][0];
 #pragma unroll
-                for (int w = 1; w < kTileWarps; ++w) {
-                    v.x += sm_part[threadIdx.x][w].x;
-                    v.y += sm_part[threadIdx.x][w].y;
-                }
+                for (int w = 1; w < kTileWarps; ++w) v = __fadd2_rn(v, sm_part[threadIdx.x][w]);
                 const int s = kVar ? sm_w[kVar ? threadIdx.x : 0] : s0;
                 const int sx0 = q.y / kTileW, sx1 = (q.y + s - 1) / kTileW, sy0 = q.z / kTH;
                 const int slot = (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0);
