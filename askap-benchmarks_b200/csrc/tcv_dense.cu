@@ -141,6 +141,22 @@ __device__ __forceinline__ void dchunk_next(DChunk& c, u32 i1, const uint4* __re
         dchunk_load<kChunk>(c, c.it + gridDim.x, i1, units, a);
     }
 }
+
+// the sorted-order entry at position pos of a unit (0 past its end)
+__device__ __forceinline__ u32 order_at(const u32* __restrict__ order, u32 start, u32 cnt, u32 pos)
+{
+    return pos < cnt ? order[start + pos] : 0u;
+}
+
+// the named barrier of one tile half's four gridding warps (barrier 0 is the CTA's)
+__device__ __forceinline__ void half_barrier(int half)
+{
+    if (half == 0)
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+    else
+        asm volatile("bar.sync 2, 128;" ::: "memory");
+}
+
 // Gridding.  The tile's two 32-column halves each have kGWarps / 2 warps with private copies of the
 // half.  The warps work independently: warp j of a half takes samples 32 j + 128 i + [0, 32) of
 // the unit (i = 0, 1, ...), stages them as jobs for its half (one per sample that meets it: the
@@ -150,20 +166,6 @@ __device__ __forceinline__ void dchunk_next(DChunk& c, u32 i1, const uint4* __re
 // keeping the next job's first table loads in flight while it adds the current one.  Only the
 // four warps of a half meet, at the end of each unit (a named barrier per half), to add their
 // copies in warp order into the grid or the unit's partial tile.
-// the sorted-order entry at position pos of a unit (0 past its end)
-__device__ __forceinline__ u32 base0_k(const u32* __restrict__ order, u32 start, u32 cnt, u32 pos)
-{
-    return pos < cnt ? order[start + pos] : 0u;
-}
-
-__device__ __forceinline__ void half_barrier(int half)
-{
-    if (half == 0)
-        asm volatile("bar.sync 1, 128;" ::: "memory");
-    else
-        asm volatile("bar.sync 2, 128;" ::: "memory");
-}
-
 template <class Tab>
 __global__ void __launch_bounds__(kGThreads, 3)
 dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
@@ -241,13 +243,13 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
         const u32 start = u.y, cnt = u.z, pslot = u.w;
         const u32 ti = a.tinfo[u.x - u32(a.group) * u32(a.ntiles)];
         const int tx0 = rec_tx(ti) * kDTW, ty0 = rec_ty(ti) * kDTH;
-        u32 kn = base0_k(order, start, cnt, u32(sub) * 32u + u32(lane));
+        u32 kn = order_at(order, start, cnt, u32(sub) * 32u + u32(lane));
         for (u32 base = u32(sub) * 32u; base < cnt; base += u32(kPerHalf) * 32u) {
             bool has = false;
             int4 jb = make_int4(0, 0, 0, 0);
             const u32 k = kn;
             // the next samples' indices are read while this chunk is added
-            kn = base0_k(order, start, cnt, base + u32(kPerHalf) * 32u + u32(lane));
+            kn = order_at(order, start, cnt, base + u32(kPerHalf) * 32u + u32(lane));
             if (base + u32(lane) < cnt) {
                 const int sk = int(a.ssz[k]);
                 const int fx = iu[k] - sk / 2, fy = iv[k];
