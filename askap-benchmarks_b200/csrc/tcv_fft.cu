@@ -280,7 +280,7 @@ enum { kFftOutGrid = 0, kFftOutRotated = 1, kFftOutImage = 2 };    // last pass 
 // both axes and signed, (-1)^(x+y) image[y + n/2][x + n/2].  With kRot the row's half of the
 // fftshift and sign is applied on the way out: value p = (-1)^p Z[p + n/2].
 template <bool kInverse, int kIn, bool kRot, int kThreads, int kLog>
-__global__ void __launch_bounds__(kThreads, kThreads <= 256 ? 3 : 1)
+__global__ void __launch_bounds__(kThreads, kThreads <= 256 ? 4 : 1)
 fft_rows_kernel(const float2* __restrict__ src, const float* __restrict__ image, float2* __restrict__ dst,
                 const float2* __restrict__ tw)
 {
