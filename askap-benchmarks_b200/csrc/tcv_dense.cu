@@ -142,12 +142,6 @@ __device__ __forceinline__ void dchunk_next(DChunk& c, u32 i1, const uint4* __re
     }
 }
 
-// the sorted-order entry at position pos of a unit (0 past its end)
-__device__ __forceinline__ u32 order_at(const u32* __restrict__ order, u32 start, u32 cnt, u32 pos)
-{
-    return pos < cnt ? order[start + pos] : 0u;
-}
-
 // the named barrier of one tile half's four gridding warps (barrier 0 is the CTA's)
 __device__ __forceinline__ void half_barrier(int half)
 {
@@ -168,9 +162,8 @@ __device__ __forceinline__ void half_barrier(int half)
 // copies in warp order into the grid or the unit's partial tile.
 template <class Tab>
 __global__ void __launch_bounds__(kGThreads, 3)
-dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __restrict__ ctab,
-                  const int* __restrict__ iu, const int* __restrict__ iv, const int* __restrict__ coff,
-                  const u32* __restrict__ order, const uint4* __restrict__ units,
+dense_grid_kernel(const float2* __restrict__ pdata, const typename Tab::elem* __restrict__ ctab,
+                  const int4* __restrict__ grec, const uint4* __restrict__ units,
                   const u32* __restrict__ group_ustart, GridArgs a)
 {
     using E = typename Tab::elem;
@@ -243,27 +236,23 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
         const u32 start = u.y, cnt = u.z, pslot = u.w;
         const u32 ti = a.tinfo[u.x - u32(a.group) * u32(a.ntiles)];
         const int tx0 = rec_tx(ti) * kDTW, ty0 = rec_ty(ti) * kDTH;
-        u32 kn = order_at(order, start, cnt, u32(sub) * 32u + u32(lane));
         for (u32 base = u32(sub) * 32u; base < cnt; base += u32(kPerHalf) * 32u) {
             bool has = false;
             int4 jb = make_int4(0, 0, 0, 0);
-            const u32 k = kn;
-            // the next samples' indices are read while this chunk is added
-            kn = order_at(order, start, cnt, base + u32(kPerHalf) * 32u + u32(lane));
             if (base + u32(lane) < cnt) {
-                const int sk = int(a.ssz[k]);
-                const int fx = iu[k] - sk / 2, fy = iv[k];
+                const int4 pr = grec[start + base + u32(lane)];  // (first column, first row, cOffset, width)
+                const int fx = pr.x, fy = pr.y, sk = pr.w;
                 const Rect R = clip(fx, fy, sk, tx0, ty0);
                 const int tc = fx + R.c0 - tx0, h = R.r1 - R.r0;
                 const int lo = max(tc, hx0), hi = min(fx + R.c1 - tx0, hx0 + kHalf);
                 has = h > 0 && lo < hi;
                 if (has) {
-                    const float2 d = data[k];
-                    jb.x = coff[k] + R.r0 * sk + R.c0 + (lo - tc);
+                    const float2 d = pdata[start + base + u32(lane)];  // scaled
+                    jb.x = pr.z + R.r0 * sk + R.c0 + (lo - tc);
                     jb.y = int(u32((fy + R.r0 - ty0) * kHalf + lo - hx0) | u32(hi - lo - 1) << 10 |
                                u32(h - 1) << 15 | u32(sk) << 20);
-                    jb.z = __float_as_int(d.x * a.c_scale);
-                    jb.w = __float_as_int(d.y * a.c_scale);
+                    jb.z = __float_as_int(d.x);
+                    jb.w = __float_as_int(d.y);
                 }
             }
             const u32 b = __ballot_sync(0xffffffffu, has);
@@ -340,10 +329,9 @@ dense_grid_kernel(const float2* __restrict__ data, const typename Tab::elem* __r
 // plain butterfly.
 template <class Tab>
 __global__ void __launch_bounds__(kDThreads)
-dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int* __restrict__ iu,
-                    const int* __restrict__ iv, const int* __restrict__ coff, const u32* __restrict__ order,
-                    const uint4* __restrict__ units, const u32* __restrict__ group_ustart,
-                    float2* __restrict__ slots, int max_tiles, GridArgs a)
+dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int4* __restrict__ grec,
+                    const u32* __restrict__ order, const uint4* __restrict__ units,
+                    const u32* __restrict__ group_ustart, float2* __restrict__ slots, int max_tiles, GridArgs a)
 {
     __shared__ float2 gt[kDPts];           // the grid tile
     __shared__ DenseRec rec[2][kDThreads];
@@ -354,11 +342,12 @@ dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int* __re
     __syncthreads();  // the lane table is built (the staging reads it)
     auto stage = [&](const DChunk& c, int buf) {
         if (int(threadIdx.x) < c.m) {
-            const u32 k = order[c.start + c.base + threadIdx.x];
-            const int sk = int(a.ssz[k]);
-            const int fx = iu[k] - sk / 2, fy = iv[k];
+            const u32 pos = c.start + c.base + threadIdx.x;
+            const u32 k = order[pos];
+            const int4 pr = grec[pos];  // (first column, first row, cOffset, width)
+            const int fx = pr.x, fy = pr.y, sk = pr.w;
             const int tx = rec_tx(c.ti), ty = rec_ty(c.ti);
-            rec[buf][threadIdx.x] = prepare(coff[k], sk, fx, fy, tx * kDTW, ty * kDTH, L);
+            rec[buf][threadIdx.x] = prepare(pr.z, sk, fx, fy, tx * kDTW, ty * kDTH, L);
             const int sx0 = fx / kDTW, sx1 = (fx + sk - 1) / kDTW, sy0 = fy / kDTH;
             rslot[buf][threadIdx.x] = (unsigned long long)(k) * max_tiles + (ty - sy0) * (sx1 - sx0 + 1) + (tx - sx0);
         }
@@ -444,6 +433,49 @@ dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int* __re
     }
 }
 
+// The footprint of every sorted (sample, tile) pair, in pair order, so that the sample-parallel
+// kernels stage a sample with one coalesced load instead of gathering its fields by sample index.
+// Blocks stride over the work units, which cover every pair of every non-empty cell.
+__global__ void pair_records_kernel(const uint4* __restrict__ units, const u32* __restrict__ group_ustart,
+                                    int n_groups, const u32* __restrict__ order, const int* __restrict__ iu,
+                                    const int* __restrict__ iv, const int* __restrict__ coff,
+                                    const unsigned short* __restrict__ ssz, int4* __restrict__ grec)
+{
+    const u32 nu = group_ustart[n_groups];
+    for (u32 it = blockIdx.x; it < nu; it += gridDim.x) {
+        const uint4 u = units[it];
+        for (u32 r = threadIdx.x; r < u.z; r += blockDim.x) {
+            const u32 pos = u.y + r, k = order[pos];
+            const int sk = int(ssz[k]);
+            grec[pos] = make_int4(iu[k] - sk / 2, iv[k], coff[k], sk);
+        }
+    }
+}
+
+// The scaled data values of the pairs, in pair order (gridding; per pass, as the data change)
+__global__ void pair_data_kernel(const uint4* __restrict__ units, const u32* __restrict__ group_ustart, int n_groups,
+                                 const u32* __restrict__ order, const float2* __restrict__ data, float c_scale,
+                                 float2* __restrict__ pdata)
+{
+    const u32 nu = group_ustart[n_groups];
+    for (u32 it = blockIdx.x; it < nu; it += gridDim.x) {
+        const uint4 u = units[it];
+        for (u32 r = threadIdx.x; r < u.z; r += blockDim.x) {
+            const u32 pos = u.y + r;
+            const float2 d = data[order[pos]];
+            pdata[pos] = make_float2(d.x * c_scale, d.y * c_scale);
+        }
+    }
+}
+
+int sm_count()
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
 int resident(const void* kernel, int threads, size_t smem)
 {
     int dev = 0, sms = 148, per_sm = 0;
@@ -485,13 +517,19 @@ tcv_status launch_dense_grid(const tcv_plan* p, const float2* data, const void* 
     const void* kernel = reinterpret_cast<const void*>(&dense_grid_kernel<Tab>);
     TCV_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGridSmem)));
     const int ctas = resident(kernel, kGThreads, kGridSmem);
+    if (!p->grec) return TCV_ERR_UNSUPPORTED;
     const typename Tab::elem* tab = static_cast<const typename Tab::elem*>(c);
     const unsigned int* order = p->vals[p->sel];
+    // the pairs' scaled data, in pair order, in the plan's degridding slots (unused while gridding)
+    const float2* pdata = p->slots;
+    pair_data_kernel<<<unsigned(8 * sm_count()), 256, 0, st>>>(p->units, p->group_ustart, g.n_groups, order, data,
+                                                               c_scale, p->slots);
+    TCV_CUDA(cudaGetLastError());
+    const int4* grec = p->grec;
     for (int grp = 0; grp < g.n_groups; ++grp) {
         GridArgs a = dense_args(p, grp, c_scale, grid);
-        void* args[] = {&data, &tab, const_cast<const int32_t**>(&p->iu), const_cast<const int32_t**>(&p->iv),
-                        const_cast<const int32_t**>(&p->coff), &order, const_cast<uint4**>(&p->units),
-                        const_cast<uint32_t**>(&p->group_ustart), &a};
+        void* args[] = {&pdata, &tab, &grec, const_cast<uint4**>(&p->units), const_cast<uint32_t**>(&p->group_ustart),
+                        &a};
         TCV_CUDA(cudaLaunchKernel(kernel, dim3(ctas), dim3(kGThreads), args, kGridSmem, st));
         if (g.split) TCV_CHECK(launch_fold8(p, a, st));
     }
@@ -506,19 +544,30 @@ tcv_status launch_dense_degrid(const tcv_plan* p, const float2* grid, const void
     if (g.n == 0) return TCV_OK;
     if (!g.var || g.tw != kDTW || g.th != kDTH) return TCV_ERR_UNSUPPORTED;
     const void* kernel = reinterpret_cast<const void*>(&dense_degrid_kernel<Tab>);
+    if (!p->grec) return TCV_ERR_UNSUPPORTED;
     const int ctas = resident(kernel, kDThreads, 0);
     const typename Tab::elem* tab = static_cast<const typename Tab::elem*>(c);
     const unsigned int* order = p->vals[p->sel];
+    const int4* grec = p->grec;
     int max_tiles = g.max_tiles;
     float2* gridp = const_cast<float2*>(grid);
     for (int grp = 0; grp < g.n_groups; ++grp) {
         GridArgs a = dense_args(p, grp, c_scale, gridp);
-        void* args[] = {&tab, const_cast<const int32_t**>(&p->iu), const_cast<const int32_t**>(&p->iv),
-                        const_cast<const int32_t**>(&p->coff), &order, const_cast<uint4**>(&p->d_units),
+        void* args[] = {&tab, &grec, &order, const_cast<uint4**>(&p->d_units),
                         const_cast<uint32_t**>(&p->d_group_ustart), const_cast<float2**>(&p->slots), &max_tiles, &a};
         TCV_CUDA(cudaLaunchKernel(kernel, dim3(ctas), dim3(kDThreads), args, 0, st));
     }
     return slot_reduce(p, c_scale, out, st);
+}
+
+tcv_status gather_pair_records(const tcv_plan* p, cudaStream_t st)
+{
+    const PlanGeom& g = p->g;
+    if (!p->grec || g.n == 0) return TCV_OK;
+    pair_records_kernel<<<unsigned(8 * sm_count()), 256, 0, st>>>(p->units, p->group_ustart, g.n_groups, p->vals[p->sel],
+                                                                  p->iu, p->iv, p->coff, p->ssz, p->grec);
+    TCV_CUDA(cudaGetLastError());
+    return TCV_OK;
 }
 
 template tcv_status launch_dense_grid<TabC64>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);

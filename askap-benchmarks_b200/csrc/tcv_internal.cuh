@@ -116,6 +116,9 @@ struct tcv_plan {
     int32_t* plane_s;              // footprint width per plane (device)
     int32_t* plane_grp;            // plane group per plane (device)
     uint16_t* ssz;                 // per-sample footprint width (device)
+    // sample-parallel kernels: per sorted (sample, tile) pair, the sample's footprint (first column,
+    // first row, cOffset, width), gathered once per binning (nullptr unless a pass uses them)
+    int4* grec;
     std::vector<int32_t> host_plane_s, host_plane_grp;
 };
 
@@ -161,6 +164,8 @@ tcv_status launch_dense_grid(const tcv_plan* p, const float2* data, const void* 
 template <class Tab>
 tcv_status launch_dense_degrid(const tcv_plan* p, const float2* grid, const void* c, float c_scale, float2* out,
                                cudaStream_t st);
+// fill p->grec from the sorted pairs (after each binning of a plan that has it)
+tcv_status gather_pair_records(const tcv_plan* p, cudaStream_t st);
 // fold_kernel<8> over one plane group of a plan (the partial tiles of its split cells)
 tcv_status launch_fold8(const tcv_plan* p, const GridArgs& a, cudaStream_t st);
 // Record the candidates and median times of the last tuning run (read by tcv_autotune_report).

@@ -729,6 +729,7 @@ tcv_status plan_create(tcv_plan* p, void* d_work, size_t work_bytes, cudaStream_
     p->rejected = static_cast<unsigned long long*>(take(sizeof(unsigned long long)));
     p->status = static_cast<unsigned int*>(take(sizeof(unsigned int)));
     p->slots = static_cast<float2*>(take(np * sizeof(float2)));
+    p->grec = (g.var && (g.dense || g.ddense)) ? static_cast<int4*>(take(np * sizeof(int4))) : nullptr;
     p->cub_temp = take(cb);
     p->cub_bytes = cb;
     p->degrid_variant = TCV_DEGRID_TILES;
@@ -872,6 +873,7 @@ size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out)
     b += 3 * align_up(acells * 4) + align_up(4);
     b += align_up(sizeof(unsigned long long)) + align_up(sizeof(unsigned int));
     b += align_up(np * sizeof(float2));
+    if (g.var && (g.dense || g.ddense)) b += align_up(np * sizeof(int4));  // pair records (tcv_dense.cu)
     b += align_up(cb);
     return b;
 }
@@ -916,7 +918,8 @@ tcv_status plan_bin(tcv_plan* p, const int32_t* d_iu, const int32_t* d_iv, const
     p->iu = d_iu;
     p->iv = d_iv;
     p->coff = d_coff;
-    const tcv_status s = p->g.key64 ? build<uint64_t>(p, d_iu, d_iv, d_coff, st) : build<uint32_t>(p, d_iu, d_iv, d_coff, st);
+    tcv_status s = p->g.key64 ? build<uint64_t>(p, d_iu, d_iv, d_coff, st) : build<uint32_t>(p, d_iu, d_iv, d_coff, st);
+    if (s == TCV_OK && p->grec) s = gather_pair_records(p, st);
     p->binned = s == TCV_OK;
     return s;
 }
