@@ -218,13 +218,14 @@ def _check_tuned(b, orc):
 @pytest.mark.parametrize("tuning", [(32, 0, 0, 16), (8, 0, 64, 16), (8, 64, 64, 16), (-1, 256, 128, 16),
                                     (32, 0, 0, 8), (-1, 128, 64, 8), (32, 256, 8, 8),
                                     (32, 0, 0, 8, 3), (-1, 256, 128, 8, 3), (8, 64, 16, 8, 2), (32, 0, 0, 8, 1),
-                                    (32, 16, 64, 8, 1), (32, 40, 64, 8, 3)])
+                                    (32, 16, 64, 8, 1), (32, 40, 64, 8, 3), (8, 64, 64, 8, 3)])
 def test_current_tunings_and_determinism(tcv, orc, cuda_ok, tuning):
     """Plane groups, work units, tile heights and the sample-parallel kernels (fifth entry: 1
     gridding, 2 degridding, 3 both) change the summation order only: every tuning within its bar
     (module docstring; sample-parallel gridding groups each point's sum by warp, so it is judged as
     split cells are), each bit-identical when rerun.  Work units of 16 and 40 samples leave some
-    sample-parallel gridding warps without samples and others with a partial group of 32."""
+    sample-parallel gridding warps without samples and others with a partial group of 32; 8 MiB
+    plane groups run the sample-parallel passes once per group on the same pair records."""
     from tconvolve.current import Benchmark
 
     b = Benchmark()
