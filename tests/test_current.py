@@ -124,9 +124,12 @@ def test_current_run_sequence_and_sort(tcv, orc, cur_golden, cuda_ok):
     b.close()
 
 
-def test_current_wide_kernels_subset(tcv, orc, cur_golden, cuda_ok):
+@pytest.mark.parametrize("tuning", [None, (8, 32, 256, 128, 3)], ids=["tile", "sample-parallel"])
+def test_current_wide_kernels_subset(tcv, orc, cur_golden, cuda_ok, tuning):
     """87 x 87 kernels (4.1e10 updates per pass at full size): the full set-up against the
-    reference, gridding and degridding of the first 150 k samples against the oracle."""
+    reference, gridding and degridding of the first 150 k samples against the oracle, with the
+    tile kernels and with the sample-parallel ones (87-wide rectangles: 32-column strips in
+    degridding, tall steps of one row in each gridding half)."""
     import torch
 
     from tconvolve import raw
@@ -147,7 +150,7 @@ def test_current_wide_kernels_subset(tcv, orc, cur_golden, cuda_ok):
     dv = torch.from_numpy(vis).cuda()
     grid = torch.zeros(g.g_size * g.g_size, dtype=torch.complex64, device="cuda")
     out = torch.empty(m, dtype=torch.complex64, device="cuda")
-    plan = raw.VarPlan(d["iu"], d["iv"], d["co"], d["wp"], s_size, off0, g.g_size, c.size)
+    plan = raw.VarPlan(d["iu"], d["iv"], d["co"], d["wp"], s_size, off0, g.g_size, c.size, tuning=tuning)
     plan.grid(dv, dc, tcv.C64, grid)
     plan.degrid(grid, dc, tcv.C64, out)
     torch.cuda.synchronize()
