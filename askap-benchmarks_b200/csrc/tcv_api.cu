@@ -330,9 +330,9 @@ tcv_status tcv_set_tuning(tcv_ctx* c, const tcv_tuning* t)
     if (!c || !t) return TCV_ERR_ARG;
     const tcv_tuning nt{t->tile_rows ? t->tile_rows : 16, t->group_mib ? t->group_mib : 32, t->split,
                         t->degrid_split, t->kernel};
-    // the sample-parallel kernel bits belong to variable-width plans: a context's plan has one width
+    // the sample-parallel kernel bits (1 gridding, 2 degridding) work on the 64 x 32 tiles of 8-row plans
     if ((nt.tile_rows != 8 && nt.tile_rows != 16 && nt.tile_rows != 32) || nt.group_mib < -1 || nt.split < 0 ||
-        nt.degrid_split < 0 || nt.kernel != 0)
+        nt.degrid_split < 0 || nt.kernel < 0 || nt.kernel > 3 || (nt.kernel != 0 && nt.tile_rows != 8))
         return TCV_ERR_ARG;
     const tcv_tuning prev = c->tuning;
     c->tuning = nt;

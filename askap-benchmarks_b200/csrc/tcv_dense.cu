@@ -434,19 +434,20 @@ dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int4* __r
 }
 
 // The footprint of every sorted (sample, tile) pair, in pair order, so that the sample-parallel
-// kernels stage a sample with one coalesced load instead of gathering its fields by sample index.
+// kernels stage a sample with one coalesced load instead of gathering its fields by sample index
+// (ssz: per-sample widths of a variable-width plan; nullptr: every sample is s_all wide).
 // Blocks stride over the work units, which cover every pair of every non-empty cell.
 __global__ void pair_records_kernel(const uint4* __restrict__ units, const u32* __restrict__ group_ustart,
                                     int n_groups, const u32* __restrict__ order, const int* __restrict__ iu,
                                     const int* __restrict__ iv, const int* __restrict__ coff,
-                                    const unsigned short* __restrict__ ssz, int4* __restrict__ grec)
+                                    const unsigned short* __restrict__ ssz, int s_all, int4* __restrict__ grec)
 {
     const u32 nu = group_ustart[n_groups];
     for (u32 it = blockIdx.x; it < nu; it += gridDim.x) {
         const uint4 u = units[it];
         for (u32 r = threadIdx.x; r < u.z; r += blockDim.x) {
             const u32 pos = u.y + r, k = order[pos];
-            const int sk = int(ssz[k]);
+            const int sk = ssz ? int(ssz[k]) : s_all;  // the plane's width, or the plan's one width
             grec[pos] = make_int4(iu[k] - sk / 2, iv[k], coff[k], sk);
         }
     }
@@ -513,7 +514,7 @@ tcv_status launch_dense_grid(const tcv_plan* p, const float2* data, const void* 
 {
     const PlanGeom& g = p->g;
     if (g.n == 0) return TCV_OK;
-    if (!g.var || g.tw != kDTW || g.th != kDTH || g.s > 4095) return TCV_ERR_UNSUPPORTED;  // widths: 12 bits of a job
+    if (g.tw != kDTW || g.th != kDTH || g.s > 4095) return TCV_ERR_UNSUPPORTED;  // widths: 12 bits of a job
     const void* kernel = reinterpret_cast<const void*>(&dense_grid_kernel<Tab>);
     TCV_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGridSmem)));
     const int ctas = resident(kernel, kGThreads, kGridSmem);
@@ -542,7 +543,7 @@ tcv_status launch_dense_degrid(const tcv_plan* p, const float2* grid, const void
 {
     const PlanGeom& g = p->g;
     if (g.n == 0) return TCV_OK;
-    if (!g.var || g.tw != kDTW || g.th != kDTH) return TCV_ERR_UNSUPPORTED;
+    if (g.tw != kDTW || g.th != kDTH) return TCV_ERR_UNSUPPORTED;
     const void* kernel = reinterpret_cast<const void*>(&dense_degrid_kernel<Tab>);
     if (!p->grec) return TCV_ERR_UNSUPPORTED;
     const int ctas = resident(kernel, kDThreads, 0);
@@ -565,16 +566,23 @@ tcv_status gather_pair_records(const tcv_plan* p, cudaStream_t st)
     const PlanGeom& g = p->g;
     if (!p->grec || g.n == 0) return TCV_OK;
     pair_records_kernel<<<unsigned(8 * sm_count()), 256, 0, st>>>(p->units, p->group_ustart, g.n_groups, p->vals[p->sel],
-                                                                  p->iu, p->iv, p->coff, p->ssz, p->grec);
+                                                                  p->iu, p->iv, p->coff, g.var ? p->ssz : nullptr, g.s,
+                                                                  p->grec);
     TCV_CUDA(cudaGetLastError());
     return TCV_OK;
 }
 
 template tcv_status launch_dense_grid<TabC64>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
+template tcv_status launch_dense_grid<TabR32>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
 template tcv_status launch_dense_grid<TabCBF16>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
+template tcv_status launch_dense_grid<TabRBF16>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
 template tcv_status launch_dense_grid<TabCF16>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
+template tcv_status launch_dense_grid<TabRF16>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
 template tcv_status launch_dense_degrid<TabC64>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
+template tcv_status launch_dense_degrid<TabR32>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
 template tcv_status launch_dense_degrid<TabCBF16>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
+template tcv_status launch_dense_degrid<TabRBF16>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
 template tcv_status launch_dense_degrid<TabCF16>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
+template tcv_status launch_dense_degrid<TabRF16>(const tcv_plan*, const float2*, const void*, float, float2*, cudaStream_t);
 
 }  // namespace tcv

@@ -125,7 +125,7 @@ tcv_status grid_rows(const tcv_plan* p, const float2* data, const void* c, float
         }
         return TCV_ERR_UNSUPPORTED;
     }
-    if (p->g.dense || p->g.ddense) return TCV_ERR_UNSUPPORTED;  // sample-parallel kernels: variable-width plans only
+    if (p->g.dense) return launch_dense_grid<Tab>(p, data, c, c_scale, grid, st);
     switch (p->g.rows) {
         case 8: return launch<Tab, 8>(p, data, c, c_scale, grid, st, c_type);
         case 16: return launch<Tab, 16>(p, data, c, c_scale, grid, st, c_type);
@@ -146,7 +146,7 @@ tcv_status degrid_rows(const tcv_plan* p, const float2* grid, const void* c, flo
         }
         return TCV_ERR_UNSUPPORTED;
     }
-    if (p->g.dense || p->g.ddense) return TCV_ERR_UNSUPPORTED;  // sample-parallel kernels: variable-width plans only
+    if (p->g.ddense) return launch_dense_degrid<Tab>(p, grid, c, c_scale, out, st);
     switch (p->g.rows) {
         case 8: return launch_adjoint<Tab, 8>(p, grid, c, c_scale, out, st, c_type);
         case 16: return launch_adjoint<Tab, 16>(p, grid, c, c_scale, out, st, c_type);

@@ -46,8 +46,8 @@ struct PlanGeom {
     int rows, tw, th;
     int split;          // samples per gridding work unit of a split cell (0: cells are never split)
     int dsplit;         // the same for degridding
-    bool dense;         // variable-width plans: sample-parallel gridding kernel (tcv_dense.cu)
-    bool ddense;        // variable-width plans: sample-parallel degridding kernel
+    bool dense;         // sample-parallel gridding kernel (tcv_dense.cu; 64 x 32 tiles)
+    bool ddense;        // sample-parallel degridding kernel
     int ntx, nty;       // tiles per row / column of a one-job plan
     int64_t ntiles;     // tiles of all jobs
     int max_tiles;      // tiles one footprint can touch
@@ -157,7 +157,7 @@ tcv_status fft_exec(float2* d_grid, int n, bool forward, cudaStream_t st);
 tcv_status fft_prepare(int n);
 tcv_status image_from_grid(float2* d_grid, int n, float scale, float* d_image, float2* d_image_c, cudaStream_t st);
 tcv_status grid_from_image(const float* d_image, int n, float2* d_grid, cudaStream_t st);
-// Sample-parallel kernels of variable-width plans on 64 x 32 tiles (tcv_dense.cu).
+// Sample-parallel kernels on 64 x 32 tiles (tcv_dense.cu), for any plan of 8-row tiles.
 template <class Tab>
 tcv_status launch_dense_grid(const tcv_plan* p, const float2* data, const void* c, float c_scale, float2* grid,
                              cudaStream_t st);

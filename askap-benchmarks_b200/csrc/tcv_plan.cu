@@ -729,7 +729,7 @@ tcv_status plan_create(tcv_plan* p, void* d_work, size_t work_bytes, cudaStream_
     p->rejected = static_cast<unsigned long long*>(take(sizeof(unsigned long long)));
     p->status = static_cast<unsigned int*>(take(sizeof(unsigned int)));
     p->slots = static_cast<float2*>(take(np * sizeof(float2)));
-    p->grec = (g.var && (g.dense || g.ddense)) ? static_cast<int4*>(take(np * sizeof(int4))) : nullptr;
+    p->grec = (g.dense || g.ddense) ? static_cast<int4*>(take(np * sizeof(int4))) : nullptr;
     p->cub_temp = take(cb);
     p->cub_bytes = cb;
     p->degrid_variant = TCV_DEGRID_TILES;
@@ -873,7 +873,7 @@ size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out)
     b += 3 * align_up(acells * 4) + align_up(4);
     b += align_up(sizeof(unsigned long long)) + align_up(sizeof(unsigned int));
     b += align_up(np * sizeof(float2));
-    if (g.var && (g.dense || g.ddense)) b += align_up(np * sizeof(int4));  // pair records (tcv_dense.cu)
+    if (g.dense || g.ddense) b += align_up(np * sizeof(int4));  // pair records (tcv_dense.cu)
     b += align_up(cb);
     return b;
 }
@@ -1080,6 +1080,7 @@ tcv_status tcv_plan_tuning(const tcv_plan* plan, tcv_tuning* tuning_out)
     tuning_out->group_mib = plan->g.group_mib;
     tuning_out->split = plan->g.split;
     tuning_out->degrid_split = plan->g.dsplit;
+    tuning_out->kernel = (plan->g.dense ? 1 : 0) | (plan->g.ddense ? 2 : 0);
     return TCV_OK;
 }
 

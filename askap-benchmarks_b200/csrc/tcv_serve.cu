@@ -341,7 +341,9 @@ void tcv_server_config_default(tcv_server_config* c)
     c->max_batch = 32;
     c->batch_samples = 262144;
     c->hbm_budget = size_t(150e9);
-    c->tuning = tcv_tuning{16, 32, 32, 32};  // 32-sample work units: a request's busy tiles spread over the SMs
+    // 8-row tiles: gridding on the tile kernels in 32-sample work units (a request's busy tiles
+    // spread over the SMs), degridding on the sample-parallel kernel in 128-sample units
+    c->tuning = tcv_tuning{8, 32, 32, 128, 2};
     c->device = 0;
 }
 

@@ -72,7 +72,7 @@ class TcvTuning(ctypes.Structure):
 
     def as_tuple(self):
         """(tile_rows, group_mib, split, degrid_split), with a fifth entry, kernel, when a pass uses
-        the sample-parallel kernels of variable-width plans (bit mask: 1 gridding, 2 degridding)."""
+        the sample-parallel kernels (bit mask: 1 gridding, 2 degridding)."""
         t = (int(self.tile_rows), int(self.group_mib), int(self.split), int(self.degrid_split))
         return t + (int(self.kernel),) if self.kernel else t
 

@@ -29,8 +29,8 @@ def _tuning(t):
         return None
     if isinstance(t, TcvTuning):
         return t
-    rows, mib, split, dsplit = (tuple(t) + (0, 0))[:4]
-    return TcvTuning(int(rows), int(mib), int(split), int(dsplit))
+    rows, mib, split, dsplit, kernel = (tuple(t) + (0, 0, 0))[:5]
+    return TcvTuning(int(rows), int(mib), int(split), int(dsplit), int(kernel))
 
 
 def table_len(c, c_type: int) -> int:

@@ -109,12 +109,14 @@ class Benchmark:
         plan = ctypes.c_void_p(self.device_buffers().plan)
         check(lib().tcv_plan_set_degrid_variant(plan, int(variant)), "tcv_plan_set_degrid_variant")
 
-    def set_tuning(self, tile_rows: int = 16, group_mib: int = 32, split: int = 0, degrid_split: int = 0):
+    def set_tuning(self, tile_rows: int = 16, group_mib: int = 32, split: int = 0, degrid_split: int = 0,
+                   kernel: int = 0):
         """Tile shape (grid rows per warp: 8, 16 or 32), plane-group slice (MiB of complex64
-        table; -1 = the whole table in one group) and work-unit sizes of busy cells for gridding
-        and degridding (samples; 0 = cells whole) of the plan.  Rebuilds the plan (the degridding
-        variant returns to "tiles")."""
-        t = _lib.TcvTuning(int(tile_rows), int(group_mib), int(split), int(degrid_split))
+        table; -1 = the whole table in one group), work-unit sizes of busy cells for gridding
+        and degridding (samples; 0 = cells whole) and the passes that use the sample-parallel
+        kernels (bit mask: 1 gridding, 2 degridding; 8-row tiles) of the plan.  Rebuilds the plan
+        (the degridding variant returns to "tiles")."""
+        t = _lib.TcvTuning(int(tile_rows), int(group_mib), int(split), int(degrid_split), int(kernel))
         check(lib().tcv_set_tuning(self._ctx, ctypes.byref(t)), "tcv_set_tuning", self._ctx)
 
     def tuning(self) -> tuple:

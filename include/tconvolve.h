@@ -190,10 +190,11 @@ typedef struct tcv_tuning {
                       (the units write partial tiles that are folded into the grid in unit
                       order); 0 = cells are never split */
     int degrid_split; /* the same for degridding (units need no fold there) */
-    int kernel;    /* bit mask of the passes that use the sample-parallel kernels of variable-width
-                      plans (one warp per sample, lanes spread densely over the footprint, for
-                      kernels much narrower than 32; tile rows must be 8): 1 gridding,
-                      2 degridding; 0 = the tile kernels (every lane owns grid columns) */
+    int kernel;    /* bit mask of the passes that use the sample-parallel kernels (one warp per
+                      sample and tile region, lanes spread densely over the footprint; they win
+                      for footprints up to a few tens wide; tile rows must be 8): 1 gridding,
+                      2 degridding; 0 = the tile kernels (every lane owns grid columns).  Plans
+                      with a bit set keep a 16-byte record per (sample, tile) pair. */
 } tcv_tuning;
 
 /* Workspace of a batched plan (0 for invalid arguments).  tuning may be NULL (defaults). */
@@ -265,7 +266,8 @@ typedef struct tcv_server_config {
     int32_t max_batch;     /* requests per batch (default 32, at most 128) */
     int64_t batch_samples; /* samples per batch; also the largest request (default 262144) */
     size_t hbm_budget;     /* device bytes the server may hold (default 150e9) */
-    tcv_tuning tuning;     /* tile shape, plane groups, work units (default {16, 32, 32, 32}) */
+    tcv_tuning tuning;     /* tile shape, plane groups, work units, sample-parallel passes
+                              (default {8, 32, 32, 128, 2}) */
     int32_t device;
 } tcv_server_config;
 

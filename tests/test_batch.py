@@ -227,3 +227,39 @@ def test_full_size_batch(tcv):
         torch.cuda.synchronize()
         assert torch.equal(grids[j], alone)
         assert torch.equal(out[sl], o)
+
+
+@pytest.mark.parametrize("tuning", [(8, 32, 0, 128, 2), (8, 32, 128, 128, 3), (8, -1, 64, 64, 3)])
+def test_sample_parallel_passes(tcv, orc, prob, tuning):
+    """The sample-parallel kernels on a fixed-width batch (45^2 footprints): every job within the
+    FP32 bar of the oracle, each job bit-identical to the same job alone with the same tuning, and
+    the batch bit-identical when rerun."""
+    import torch
+
+    from tconvolve import raw
+
+    b, grids, out = _run_batch(tcv, prob, SIZES, tuning=tuning)
+    assert b.tuning() == tuning
+    _, grids2, out2 = _run_batch(tcv, prob, SIZES, tuning=tuning)
+    assert torch.equal(out, out2)
+    h = _host(prob)
+    support, c_len = prob["support"], prob["c_len"]
+    at = 0
+    for j, (n, g) in enumerate(SIZES):
+        assert torch.equal(grids[j], grids2[j])
+        if n:
+            sl = slice(at, at + n)
+            alone = torch.zeros(g * g, dtype=torch.complex64, device="cuda")
+            plan = raw.Plan(prob["iu"][sl].contiguous(), prob["iv"][sl].contiguous(), prob["coff"][sl].contiguous(),
+                            support, g, c_len, tuning=tuning)
+            plan.grid(prob["data"][sl].contiguous(), prob["c64"], tcv.C64, alone)
+            alone_out = torch.empty(n, dtype=torch.complex64, device="cuda")
+            plan.degrid(alone, prob["c64"], tcv.C64, alone_out)
+            torch.cuda.synchronize()
+            assert torch.equal(grids[j], alone), f"job {j} grid differs from the job alone"
+            assert torch.equal(out[sl], alone_out), f"job {j} samples differ from the job alone"
+            ref, ref_o, keep = _oracle_job(orc, h, at, n, g, support, c_len)
+            assert orc.rel_l2(grids[j].cpu().numpy(), ref) <= REL_L2_FP32
+            assert orc.rel_l2(out[sl].cpu().numpy()[keep], ref_o) <= REL_L2_FP32
+            assert np.all(out[sl].cpu().numpy()[~keep] == 0)
+        at += n

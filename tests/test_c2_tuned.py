@@ -7,7 +7,8 @@ here and pinned to the sha256 of the reference's own output (tests/golden/golden
 so every comparison below is against the reference's bits.
 
 Bars (written here, used below):
-  * grid and degridded samples: relative L2 <= 1e-5 (REL_L2_FP32) against the reference;
+  * grid and degridded samples: relative L2 <= 1e-5 (REL_L2_FP32) against the reference (the
+    sample-parallel passes group each point's or sample's sum by warp: FP32 rounding only);
   * r32 and c64 with the same tuning: bit-identical (the attic table's imaginary parts are zero);
   * the same tuning run twice: bit-identical (no atomics; fixed summation order).
 """
@@ -21,10 +22,12 @@ from tconvolve.workload import PROBLEMS, normal_vis
 
 pytestmark = pytest.mark.gpu
 
-# (tile rows, plane-group MiB, gridding work unit, degridding work unit): the autotuner's pick for
-# the timed r32 workload, the same with split gridding cells, a 64-sample gridding split, the
-# whole table in one group, and 8-row tiles with both passes split
-TUNINGS = [(16, 64, 0, 64), (16, 64, 256, 64), (16, 64, 64, 128), (16, -1, 0, 0), (8, 32, 512, 256)]
+# (tile rows, plane-group MiB, gridding work unit, degridding work unit[, sample-parallel passes]):
+# the autotuner's pick for the timed r32 workload, the same with split gridding cells, a 64-sample
+# gridding split, the whole table in one group, 8-row tiles with both passes split, and 8-row
+# tiles with the sample-parallel degridding and with both passes sample-parallel
+TUNINGS = [(16, 64, 0, 64), (16, 64, 256, 64), (16, 64, 64, 128), (16, -1, 0, 0), (8, 32, 512, 256),
+           (8, 64, 0, 128, 2), (8, 64, 256, 128, 3)]
 
 
 @pytest.fixture(scope="module")
