@@ -6,8 +6,8 @@
 // replayed with one launch and no host work.  The autotuner times the candidate tunings
 // (rows per warp 8/16/32, i.e. tiles of 64 x 32/64/128 points, and plane-group slices of
 // 8/16/32/64 MiB or the whole table; then gridding and degridding work units of 512/256/128/64
-// samples for busy cells)
-// on the caller's own batch, into scratch grids, and keeps the fastest.  Neither has a
+// samples for busy cells; then the sample-parallel degridding kernel on 8-row tiles in 256- and
+// 128-sample units) on the caller's own batch, into scratch grids, and keeps the fastest.  Neither has a
 // counterpart in the reference, whose kernels run one job per call
 // (attic/tConvolveMPI/Benchmark.cc:98-106).
 #include "tcv_internal.cuh"
@@ -272,6 +272,11 @@ tcv_status tcv_autotune(const tcv_job* jobs, int n_jobs, const int32_t* d_iu, co
         const tcv_tuning base = best;
         for (int split : {512, 256, 128, 64})
             if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, base.split, split})) != TCV_OK) break;
+    }
+    if (s == TCV_OK) {  // stage 4: the sample-parallel degridding kernel (8-row tiles), for narrow footprints
+        const tcv_tuning base = best;
+        for (int split : {256, 128})
+            if ((s = time_one(tcv_tuning{8, base.group_mib, base.split, split, 2})) != TCV_OK) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
