@@ -59,6 +59,9 @@ struct Slot {
     std::vector<ReqPtr> reqs;           // the batch in flight (grid requests first)
     int64_t n_grid = 0;                 // samples of its grid requests
     int launch_status = TCV_OK;
+    // executable graphs of earlier batches, by shape (gridding and degridding request counts),
+    // updated in place by the next batch of the same shape
+    std::vector<std::pair<uint64_t, cudaGraphExec_t>> execs;
     bool busy = false, launched = false;
     std::condition_variable cv;
     std::thread waiter;
@@ -169,7 +172,10 @@ tcv_status launch(tcv_server* s, Slot& sl)
         at += r->r.n;
     }
     sl.hrej[0] = sl.hrej[1] = 0;
-    if (total > 0) {
+    if (total <= 0) return TCV_OK;
+    // the batch's device work: one H2D copy, offsets, the gridding plan and pass, the degridding
+    // plan and pass, the D2H copies of the degridded samples and the rejected counts
+    auto enqueue = [&]() -> tcv_status {
         TCV_CUDA(cudaMemcpyAsync(sl.din, sl.hin, size_t(3 * total + n_grid) * 8, cudaMemcpyHostToDevice, sl.st));
         tcv_status st = tcv_init_offsets_raw(sl.du, sl.dv, sl.dw, total, s->dfreq, 1, s->cfg.cell_size, s->w_cell,
                                              s->cfg.w_size, s->cfg.g_size, s->support, s->over_sample, sl.diu, sl.div,
@@ -182,8 +188,50 @@ tcv_status launch(tcv_server* s, Slot& sl)
         if (total > n_grid)
             TCV_CUDA(cudaMemcpyAsync(sl.hout + n_grid, sl.dout + n_grid, size_t(total - n_grid) * 8,
                                      cudaMemcpyDeviceToHost, sl.st));
+        return TCV_OK;
+    };
+    if (s->cfg.graphs) {
+        // Captured (this thread only) into a graph and launched once: the slot's executable graph
+        // takes the new node parameters when the batch has the same shape as the last one, and is
+        // rebuilt when it does not.  Nothing runs while capturing, so a capture that fails falls
+        // back to launching the same work one call at a time.
+        if (cudaStreamBeginCapture(sl.st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const tcv_status st = enqueue();
+            cudaGraph_t g = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(sl.st, &g);
+            if (st == TCV_OK && ec == cudaSuccess && g) {
+                const uint64_t shape = (uint64_t(n_gr) << 32) | uint64_t(reqs.size() - n_gr);
+                cudaGraphExec_t* ex = nullptr;
+                for (auto& e : sl.execs)
+                    if (e.first == shape) ex = &e.second;
+                if (ex) {
+                    cudaGraphExecUpdateResultInfo info{};
+                    if (cudaGraphExecUpdate(*ex, g, &info) != cudaSuccess) {
+                        cudaGetLastError();
+                        cudaGraphExecDestroy(*ex);
+                        *ex = nullptr;
+                    }
+                } else {
+                    if (sl.execs.size() >= 16) {  // keep the 16 most recent shapes
+                        cudaGraphExecDestroy(sl.execs.front().second);
+                        sl.execs.erase(sl.execs.begin());
+                    }
+                    sl.execs.emplace_back(shape, nullptr);
+                    ex = &sl.execs.back().second;
+                }
+                cudaError_t e = cudaSuccess;
+                if (!*ex) e = cudaGraphInstantiate(ex, g, 0);
+                cudaGraphDestroy(g);
+                if (e == cudaSuccess) e = cudaGraphLaunch(*ex, sl.st);
+                return tcv::cuda_status(e);
+            }
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();  // the capture's error, if any: launch directly below
+        } else {
+            cudaGetLastError();
+        }
     }
-    return TCV_OK;
+    return enqueue();
 }
 
 void scheduler_loop(tcv_server* s)
@@ -310,6 +358,7 @@ void free_server(tcv_server* s)
         void* h[] = {sl->hin, sl->hout, sl->hrej};
         for (void* p : h)
             if (p) cudaFreeHost(p);
+        for (auto& e : sl->execs) cudaGraphExecDestroy(e.second);
         if (sl->done) cudaEventDestroy(sl->done);
         if (sl->st) cudaStreamDestroy(sl->st);
     }
@@ -345,6 +394,7 @@ void tcv_server_config_default(tcv_server_config* c)
     // spread over the SMs), degridding on the sample-parallel kernel in 128-sample units
     c->tuning = tcv_tuning{8, 32, 32, 128, 2};
     c->device = 0;
+    c->graphs = 1;
 }
 
 tcv_status tcv_server_create(const tcv_server_config* cfg, tcv_server** out)

@@ -82,7 +82,7 @@ class TcvServerConfig(ctypes.Structure):
         ("g_size", ctypes.c_int32), ("w_size", ctypes.c_int32), ("cell_size", ctypes.c_double),
         ("baseline", ctypes.c_int32), ("c_type", ctypes.c_int32), ("streams", ctypes.c_int32),
         ("max_batch", ctypes.c_int32), ("batch_samples", ctypes.c_int64), ("hbm_budget", ctypes.c_size_t),
-        ("tuning", TcvTuning), ("device", ctypes.c_int32),
+        ("tuning", TcvTuning), ("device", ctypes.c_int32), ("graphs", ctypes.c_int32),
     ]
 
 

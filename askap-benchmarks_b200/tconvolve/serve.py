@@ -43,7 +43,7 @@ class Request:
 class Server:
     def __init__(self, g_size: int = 1024, w_size: int = 9, cell_size: float | None = None, baseline: int = 2000,
                  c_type: int | str = "r32", streams: int = 2, max_batch: int = 32, batch_samples: int = 262144,
-                 hbm_budget: float = 150e9, tuning=(8, 32, 32, 128, 2), device: int = 0):
+                 hbm_budget: float = 150e9, tuning=(8, 32, 32, 128, 2), device: int = 0, graphs: bool = True):
         cfg = TcvServerConfig()
         lib().tcv_server_config_default(ctypes.byref(cfg))
         cfg.g_size, cfg.w_size, cfg.baseline = g_size, w_size, baseline
@@ -55,6 +55,7 @@ class Server:
         (cfg.tuning.tile_rows, cfg.tuning.group_mib, cfg.tuning.split, cfg.tuning.degrid_split,
          cfg.tuning.kernel) = (tuple(tuning) + (0, 0, 0))[:5]
         cfg.device = device
+        cfg.graphs = 1 if graphs else 0
         self.cfg = cfg
         self._h = ctypes.c_void_p()
         check(lib().tcv_server_create(ctypes.byref(cfg), ctypes.byref(self._h)), "tcv_server_create")
