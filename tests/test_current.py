@@ -225,8 +225,8 @@ def _check_tuned(b, orc):
 def test_current_tunings_and_determinism(tcv, orc, cuda_ok, tuning):
     """Plane groups, work units, tile heights and the sample-parallel kernels (fifth entry: 1
     gridding, 2 degridding, 3 both) change the summation order only: every tuning within its bar
-    (module docstring; sample-parallel gridding groups each point's sum by warp, so it is judged as
-    split cells are), each bit-identical when rerun.  Work units of 16 and 40 samples leave some
+    (module docstring; sample-parallel gridding groups each point's sum by warp, so it is held to
+    the split-cell bar), each bit-identical when rerun.  Work units of 16 and 40 samples leave some
     sample-parallel gridding warps without samples and others with a partial group of 32; 8 MiB
     plane groups run the sample-parallel passes once per group on the same pair records."""
     from tconvolve.current import Benchmark
