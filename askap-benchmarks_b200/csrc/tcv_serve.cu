@@ -137,6 +137,9 @@ tcv_status run_plan(tcv_server* s, Slot& sl, const std::vector<ReqPtr>& reqs, si
     return st;
 }
 
+// batches of at most this many requests are replayed as CUDA graphs (tcv_server_config.graphs)
+constexpr int kGraphRequests = 4;
+
 // stage and enqueue one batch on its slot (no lock held)
 tcv_status launch(tcv_server* s, Slot& sl)
 {
@@ -190,11 +193,13 @@ tcv_status launch(tcv_server* s, Slot& sl)
                                      cudaMemcpyDeviceToHost, sl.st));
         return TCV_OK;
     };
-    if (s->cfg.graphs) {
+    if (s->cfg.graphs && reqs.size() <= size_t(kGraphRequests)) {
         // Captured (this thread only) into a graph and launched once: the slot's executable graph
-        // takes the new node parameters when the batch has the same shape as the last one, and is
-        // rebuilt when it does not.  Nothing runs while capturing, so a capture that fails falls
-        // back to launching the same work one call at a time.
+        // for this batch shape takes the new node parameters, or is built for a new shape.
+        // Nothing runs while capturing, so a capture that fails falls back to launching the same
+        // work one call at a time.  Only small batches go this way: they are the ones whose
+        // latency the launches set, and under load the shapes vary too much for the graphs to be
+        // reused (building one costs more host time than launching the work).
         if (cudaStreamBeginCapture(sl.st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
             const tcv_status st = enqueue();
             cudaGraph_t g = nullptr;

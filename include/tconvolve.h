@@ -269,10 +269,10 @@ typedef struct tcv_server_config {
     tcv_tuning tuning;     /* tile shape, plane groups, work units, sample-parallel passes
                               (default {8, 32, 32, 128, 2}) */
     int32_t device;
-    int32_t graphs;        /* 1 (default): each batch's copies and launches are captured and
-                              replayed as one CUDA graph launch (the slot's executable graph is
-                              updated in place when the batch has the same shape); 0: launched
-                              one by one */
+    int32_t graphs;        /* 1 (default): the copies and launches of a batch of up to 4
+                              requests are captured and replayed as one CUDA graph launch (the
+                              slot's executable graph for that batch shape is updated in place);
+                              larger batches, and every batch when 0, are launched one by one */
 } tcv_server_config;
 
 enum { TCV_REQ_GRID = 0, TCV_REQ_DEGRID = 1 };

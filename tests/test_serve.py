@@ -158,8 +158,9 @@ def test_poisson_load(tcv, cuda_ok):
 
 @pytest.mark.parametrize("tuning", [(8, 32, 32, 128, 2), (16, 32, 32, 32)], ids=["default", "tile-kernels"])
 def test_graph_replay_matches_direct_launches(tcv, cuda_ok, tuning):
-    """Batches replayed as CUDA graphs (the default) and launched call by call give the same bits;
-    the same batch shapes repeat, so the graph path updates its executable graphs in place."""
+    """Batches replayed as CUDA graphs (the default, for batches of up to 4 requests) and launched
+    call by call give the same bits; the same batch shapes repeat, so the graph path updates its
+    executable graphs in place."""
     from tconvolve._lib import REQ_DEGRID, REQ_GRID
     from tconvolve.serve import request_pool
 
@@ -172,17 +173,18 @@ def test_graph_replay_matches_direct_launches(tcv, cuda_ok, tuning):
         srv.grid_write(gd, image)
         grids, outs = [], []
         for rnd in range(3):  # three rounds of the same shapes
-            ga = [srv.grid_alloc() for _ in range(4)]
-            reqs = [srv.submit(REQ_GRID, ga[i], *pool[i]) for i in range(4)]
-            degs = [srv.submit(REQ_DEGRID, gd, *pool[4 + i][:3]) for i in range(4)]
+            ga = [srv.grid_alloc() for _ in range(2)]
+            reqs = [srv.submit(REQ_GRID, ga[i], *pool[i]) for i in range(2)]
+            degs = [srv.submit(REQ_DEGRID, gd, *pool[4 + i][:3]) for i in range(2)]
             assert all(r.wait().status == 0 for r in reqs + degs)
+            assert max(r.info.batch_requests for r in reqs + degs) <= 4
             grids.append([srv.grid_read(g) for g in ga])
             outs.append([d.vis_out.copy() for d in degs])
         results.append((grids, outs))
         srv.close()
     (g1, o1), (g2, o2) = results
     for rnd in range(3):
-        for i in range(4):
+        for i in range(2):
             assert np.array_equal(g1[rnd][i], g2[rnd][i])
             assert np.array_equal(o1[rnd][i], o2[rnd][i])
             assert np.array_equal(g1[rnd][i], g1[0][i]) and np.array_equal(o1[rnd][i], o1[0][i])
