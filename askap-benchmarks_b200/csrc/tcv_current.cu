@@ -714,7 +714,7 @@ tcv_status tcv_cur_tune(tcv_cur_ctx* c, int reps, tcv_tuning* best_out, float* b
     }
     if (s == TCV_OK) {  // stage 2: gridding work units
         const tcv_tuning base = best;
-        for (int split : {512, 128, 64})  // the partial-tile bound grows as 1 / split
+        for (int split : {1024, 512, 128, 64})  // the partial-tile bound grows as 1 / split
             if ((s = time_one(tcv_tuning{base.tile_rows, base.group_mib, split, base.degrid_split, base.kernel})) !=
                 TCV_OK)
                 break;
