@@ -9,14 +9,16 @@
 // The staging thread of each sample prepares its rectangle once (tile coordinates, table index
 // of its first element, rows per step), so a warp only walks it.
 //
-// Gridding: each 32-column half of the 64 x 32 tile has four warps with private copies of the
-// half in shared memory (8 KB each, no two warps write one copy: no atomics).  The warps work
-// independently: each takes every fourth group of 32 samples of the unit, stages them as jobs
-// for its half (one per sample that meets the half) and adds them into its copy, keeping the next
-// job's first table loads in flight while it adds the current one (a two-stage software
-// pipeline).  At the end of the unit the four warps of a half meet (a named barrier) and add
-// their copies in warp order into the grid, or into the unit's partial tile for a split cell
-// (fold_kernel then adds those in unit order, as for the tile kernels).
+// Gridding: a work item is one 32-column half of a unit's 64 x 32 tile; groups of four warps
+// take items from a counter as they finish their last (no fixed share per CTA, so no CTA is left
+// with a long tail), and each warp adds into a private copy of the half in shared memory (8 KB
+// each, no two warps write one copy: no atomics).  The warps of a group work independently: each
+// takes every fourth group of 32 samples of the unit, stages them as jobs for the half (one per
+// sample that meets the half) and adds them into its copy, keeping the next job's first table
+// loads in flight while it adds the current one (a two-stage software pipeline).  At the end of
+// the item the four warps meet (a named barrier) and add their copies in warp order into the
+// grid, or into the unit's partial tile for a split cell (fold_kernel then adds those in unit
+// order, as for the tile kernels).
 // Degridding: the grid tile is staged in shared memory once per unit; a warp takes four samples
 // at a time and reduces their products across the warp together (one transposing reduction) into
 // the samples' slots for the tile (slot_reduce_kernel adds the slots in tile order).
@@ -151,14 +153,15 @@ __device__ __forceinline__ void half_barrier(int half)
         asm volatile("bar.sync 2, 128;" ::: "memory");
 }
 
-// Gridding.  The tile's two 32-column halves each have kGWarps / 2 warps with private copies of the
-// half.  The warps work independently: warp j of a half takes samples 32 j + 128 i + [0, 32) of
-// the unit (i = 0, 1, ...), stages them as jobs for its half (one per sample that meets it: the
+// Gridding.  The CTA's two groups of kGWarps / 2 warps each take one (unit, 32-column tile half)
+// work item at a time, handed out by a counter, and their warps hold private copies of a half.
+// The warps work independently: warp j of a group takes samples 32 j + 128 i + [0, 32) of the
+// unit (i = 0, 1, ...), stages them as jobs for the item's half (one per sample that meets it: the
 // table index of the first element of the sample's rectangle in the half, and first point |
 // (width - 1) << 10 | (height - 1) << 15 | table row stride << 20, and the scaled data value),
 // packed in sample order by ballot into its own 32-entry list, and adds them into its copy,
 // keeping the next job's first table loads in flight while it adds the current one.  Only the
-// four warps of a half meet, at the end of each unit (a named barrier per half), to add their
+// four warps of a group meet, at the end of each item (a named barrier per group), to add their
 // copies in warp order into the grid or the unit's partial tile.
 template <class Tab>
 __global__ void __launch_bounds__(kGThreads, 3)
@@ -176,13 +179,36 @@ dense_grid_kernel(const float2* __restrict__ pdata, const typename Tab::elem* __
     float2* acc_all = dsm;                                                    // [kGWarps][kHPts]
     int4* jobs_all = reinterpret_cast<int4*>(dsm + kGWarps * kHPts);         // [kGWarps][32]
     __shared__ unsigned short gl[33][32];
+    __shared__ u32 sm_item[2][2];  // per warp group: its current and next work item
+    __shared__ u32 sm_range[2];    // the group's first unit and its number of work items
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int half = warp / kPerHalf, sub = warp % kPerHalf, hx0 = half * kHalf;
+    const int half = warp / kPerHalf, sub = warp % kPerHalf;  // warp group (copies, barrier), warp in it
+    // Work items are (unit, tile half) pairs, 2 i and 2 i + 1 the halves of the group's unit i,
+    // handed out to the warp groups in turn by a counter (a.sched[0]) as each group finishes its
+    // last; the group that finds the list exhausted last (a.sched[1] counts them) sets both counters
+    // to zero again for the next launch.  Which group takes an item does not change any sum.
+    // (the unit range is read back from shared memory where it is used, so that it holds no
+    // registers through the job loop)
+    if (threadIdx.x == 0) {
+        const u32 i0 = group_ustart[a.group];
+        sm_range[0] = i0;
+        sm_range[1] = 2u * (group_ustart[a.group + 1] - i0);
+    }
+    auto fetch = [&](int slot) {  // the group's first lane only
+        const u32 v = atomicAdd(a.sched, 1u);
+        if (v >= sm_range[1] && atomicAdd(a.sched + 1, 1u) == 2u * gridDim.x - 1u) {
+            atomicExch(a.sched, 0u);
+            atomicExch(a.sched + 1, 0u);
+        }
+        sm_item[half][slot] = v;
+    };
     build_grid_lut(gl, threadIdx.x, kGThreads);
     float2* acc = acc_all + warp * kHPts;
     int4* jl = jobs_all + warp * 32;
     for (int i = lane; i < kHPts; i += 32) acc[i] = make_float2(0.f, 0.f);
-    __syncthreads();  // the lane table is built
+    __syncthreads();  // the lane table and the unit range are set
+    if (sub == 0 && lane == 0) fetch(0);
+    half_barrier(half);  // the group's first item is in sm_item
 
     struct Job {
         const E* tp;   // the lane's first table entry
@@ -230,9 +256,11 @@ dense_grid_kernel(const float2* __restrict__ pdata, const typename Tab::elem* __
         }
     };
 
-    const u32 i1 = group_ustart[a.group + 1];
-    for (u32 it = group_ustart[a.group] + blockIdx.x; it < i1; it += gridDim.x) {
-        const uint4 u = units[it];
+    for (int par = 0;; par ^= 1) {
+        const u32 item = sm_item[half][par];  // written before the last barrier of the group
+        if (item >= sm_range[1]) break;       // the group's four warps read the same item
+        const int hx0 = int(item & 1u) * kHalf;
+        const uint4 u = units[sm_range[0] + (item >> 1)];
         const u32 start = u.y, cnt = u.z, pslot = u.w;
         const u32 ti = a.tinfo[u.x - u32(a.group) * u32(a.ntiles)];
         const int tx0 = rec_tx(ti) * kDTW, ty0 = rec_ty(ti) * kDTH;
@@ -288,6 +316,7 @@ dense_grid_kernel(const float2* __restrict__ pdata, const typename Tab::elem* __
             __syncwarp();  // the list is read before the next samples are packed into it
         }
         // the unit is done in this half: its copies in warp order into the grid or the partial tile
+        if (sub == 0 && lane == 0) fetch(par ^ 1);  // read by the group after the barrier below
         half_barrier(half);
         const JobDesc& jd = a.jobs[rec_job(ti)];
         const int gs = jd.g_size;
@@ -503,6 +532,7 @@ GridArgs dense_args(const tcv_plan* p, int grp, float c_scale, float2* grid)
     a.tinfo = p->tinfo;
     a.partial = p->partial;
     a.ssz = p->ssz;
+    a.sched = p->status + kSchedWord;
     return a;
 }
 

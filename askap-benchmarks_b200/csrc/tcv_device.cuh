@@ -52,6 +52,9 @@ struct GridArgs {
     const u32* __restrict__ tinfo;  // per tile: column | row << 11 | job << 22
     float2* partial;                // partial tiles of split cells (gridding), tile after tile
     const unsigned short* __restrict__ ssz;  // per-sample footprint width (variable-width plans)
+    // two work-item counters of the plan, zero at every launch (the sample-parallel gridding
+    // kernel hands out its work items with them and sets them to zero again when it finishes)
+    u32* sched;
 };
 
 // A work unit: a cell's samples [first, first + count) of the sorted order, and the partial tile

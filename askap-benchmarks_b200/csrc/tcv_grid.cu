@@ -42,6 +42,7 @@ GridArgs make_args(const tcv_plan* p, int grp, float c_scale, float2* grid)
     a.tinfo = p->tinfo;
     a.partial = p->partial;
     a.ssz = p->ssz;
+    a.sched = p->status + kSchedWord;
     return a;
 }
 

@@ -97,7 +97,9 @@ struct tcv_plan {
     uint32_t* aitems;              // non-empty anchor cells, group-major
     uint32_t* n_aitems;
     unsigned long long* rejected;  // samples left out as out of bounds
-    unsigned int* status;          // device status word: bit 0 = a bounded wait timed out
+    unsigned int* status;          // device status block (tcv::kStatusWords words): word 0 bit 0 = a
+                                   // bounded wait timed out; words kSchedWord, +1: the sample-parallel
+                                   // gridding kernel's work-item counters (zero between launches)
     float2* slots;                 // degridding partial sums, n * max_tiles
     void* cub_temp;
     size_t cub_bytes;
@@ -123,6 +125,9 @@ struct tcv_plan {
 };
 
 namespace tcv {
+
+constexpr int kStatusWords = 8;  // the plan's status block, zeroed by every binning
+constexpr int kSchedWord = 4;    // first of the two work-item counters in it
 
 // Host helpers implemented in tcv_plan.cu
 // Geometry for jobs of the given grid sides (n samples in all); tuning may be nullptr.  anchors:

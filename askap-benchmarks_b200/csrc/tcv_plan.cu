@@ -602,7 +602,7 @@ tcv_status build(tcv_plan* p, const int32_t* iu, const int32_t* iv, const int32_
     TCV_CUDA(cudaMemsetAsync(p->tile_start, 0, sizeof(uint32_t) * size_t(cells), st));  // run starts
     if (with_anchors) TCV_CUDA(cudaMemsetAsync(p->atile_count, 0, sizeof(uint32_t) * size_t(acells), st));
     TCV_CUDA(cudaMemsetAsync(p->rejected, 0, sizeof(unsigned long long), st));
-    TCV_CUDA(cudaMemsetAsync(p->status, 0, sizeof(unsigned int), st));
+    TCV_CUDA(cudaMemsetAsync(p->status, 0, kStatusWords * sizeof(unsigned int), st));
     if (g.n > 0) {
         const VarPlanes var{p->wplane, p->plane_s, p->plane_grp, p->ssz};
         // staged key writes while a block's pairs fit the default 48 KB of shared memory
@@ -727,7 +727,7 @@ tcv_status plan_create(tcv_plan* p, void* d_work, size_t work_bytes, cudaStream_
     p->aitems = static_cast<uint32_t*>(take(acells * 4));
     p->n_aitems = static_cast<uint32_t*>(take(4));
     p->rejected = static_cast<unsigned long long*>(take(sizeof(unsigned long long)));
-    p->status = static_cast<unsigned int*>(take(sizeof(unsigned int)));
+    p->status = static_cast<unsigned int*>(take(kStatusWords * sizeof(unsigned int)));
     p->slots = static_cast<float2*>(take(np * sizeof(float2)));
     p->grec = (g.dense || g.ddense) ? static_cast<int4*>(take(np * sizeof(int4))) : nullptr;
     p->cub_temp = take(cb);
@@ -871,7 +871,7 @@ size_t plan_bytes(const PlanGeom& g, size_t* cub_bytes_out)
         b += align_up(size_t(g.n_groups + 1) * 4) + 3 * align_up(cells * 4) +
              align_up(max_units(g, g.dsplit) * sizeof(uint4));
     b += 3 * align_up(acells * 4) + align_up(4);
-    b += align_up(sizeof(unsigned long long)) + align_up(sizeof(unsigned int));
+    b += align_up(sizeof(unsigned long long)) + align_up(kStatusWords * sizeof(unsigned int));
     b += align_up(np * sizeof(float2));
     if (g.dense || g.ddense) b += align_up(np * sizeof(int4));  // pair records (tcv_dense.cu)
     b += align_up(cb);
