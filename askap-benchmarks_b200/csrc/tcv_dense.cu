@@ -165,7 +165,7 @@ __device__ __forceinline__ void half_barrier(int half)
 // copies in warp order into the grid or the unit's partial tile.
 template <class Tab>
 __global__ void __launch_bounds__(kGThreads, 3)
-dense_grid_kernel(const float2* __restrict__ pdata, const typename Tab::elem* __restrict__ ctab,
+dense_grid_kernel(const float2* __restrict__ data, const u32* __restrict__ order, const typename Tab::elem* __restrict__ ctab,
                   const int4* __restrict__ grec, const uint4* __restrict__ units,
                   const u32* __restrict__ group_ustart, GridArgs a)
 {
@@ -269,18 +269,18 @@ dense_grid_kernel(const float2* __restrict__ pdata, const typename Tab::elem* __
             int4 jb = make_int4(0, 0, 0, 0);
             if (base + u32(lane) < cnt) {
                 const int4 pr = grec[start + base + u32(lane)];  // (first column, first row, cOffset, width)
+                const float2 d = data[order[start + base + u32(lane)]];  // in flight during the clip below
                 const int fx = pr.x, fy = pr.y, sk = pr.w;
                 const Rect R = clip(fx, fy, sk, tx0, ty0);
                 const int tc = fx + R.c0 - tx0, h = R.r1 - R.r0;
                 const int lo = max(tc, hx0), hi = min(fx + R.c1 - tx0, hx0 + kHalf);
                 has = h > 0 && lo < hi;
                 if (has) {
-                    const float2 d = pdata[start + base + u32(lane)];  // scaled
                     jb.x = pr.z + R.r0 * sk + R.c0 + (lo - tc);
                     jb.y = int(u32((fy + R.r0 - ty0) * kHalf + lo - hx0) | u32(hi - lo - 1) << 10 |
                                u32(h - 1) << 15 | u32(sk) << 20);
-                    jb.z = __float_as_int(d.x);
-                    jb.w = __float_as_int(d.y);
+                    jb.z = __float_as_int(d.x * a.c_scale);
+                    jb.w = __float_as_int(d.y * a.c_scale);
                 }
             }
             const u32 b = __ballot_sync(0xffffffffu, has);
@@ -482,22 +482,6 @@ __global__ void pair_records_kernel(const uint4* __restrict__ units, const u32* 
     }
 }
 
-// The scaled data values of the pairs, in pair order (gridding; per pass, as the data change)
-__global__ void pair_data_kernel(const uint4* __restrict__ units, const u32* __restrict__ group_ustart, int n_groups,
-                                 const u32* __restrict__ order, const float2* __restrict__ data, float c_scale,
-                                 float2* __restrict__ pdata)
-{
-    const u32 nu = group_ustart[n_groups];
-    for (u32 it = blockIdx.x; it < nu; it += gridDim.x) {
-        const uint4 u = units[it];
-        for (u32 r = threadIdx.x; r < u.z; r += blockDim.x) {
-            const u32 pos = u.y + r;
-            const float2 d = data[order[pos]];
-            pdata[pos] = make_float2(d.x * c_scale, d.y * c_scale);
-        }
-    }
-}
-
 int sm_count()
 {
     int dev = 0, sms = 148;
@@ -551,16 +535,11 @@ tcv_status launch_dense_grid(const tcv_plan* p, const float2* data, const void* 
     if (!p->grec) return TCV_ERR_UNSUPPORTED;
     const typename Tab::elem* tab = static_cast<const typename Tab::elem*>(c);
     const unsigned int* order = p->vals[p->sel];
-    // the pairs' scaled data, in pair order, in the plan's degridding slots (unused while gridding)
-    const float2* pdata = p->slots;
-    pair_data_kernel<<<unsigned(8 * sm_count()), 256, 0, st>>>(p->units, p->group_ustart, g.n_groups, order, data,
-                                                               c_scale, p->slots);
-    TCV_CUDA(cudaGetLastError());
     const int4* grec = p->grec;
     for (int grp = 0; grp < g.n_groups; ++grp) {
         GridArgs a = dense_args(p, grp, c_scale, grid);
-        void* args[] = {&pdata, &tab, &grec, const_cast<uint4**>(&p->units), const_cast<uint32_t**>(&p->group_ustart),
-                        &a};
+        void* args[] = {const_cast<float2**>(&data), const_cast<unsigned int**>(&order), &tab, &grec,
+                        const_cast<uint4**>(&p->units), const_cast<uint32_t**>(&p->group_ustart), &a};
         TCV_CUDA(cudaLaunchKernel(kernel, dim3(ctas), dim3(kGThreads), args, kGridSmem, st));
         if (g.split) TCV_CHECK(launch_fold8(p, a, st));
     }
