@@ -119,6 +119,24 @@ __device__ __forceinline__ void cmac(float2& acc, const float2 a, const float2 b
     if (!kReal) acc = __ffma2_rn(make_float2(-a.y, a.x), make_float2(b.y, b.y), acc);  // += i * a * b.im
 }
 
+// The same multiply-add for the degridding tile kernel, where a is the lane's grid value of the
+// row (a register, different for every row): with a complex table the packed form needs the
+// swapped, negated copy of a and duplicated halves of b for every row, so it is written as four
+// scalar fused multiply-adds instead (the negation an operand modifier), which are the same
+// operations with the same roundings, component by component, as cmac.
+template <bool kReal>
+__device__ __forceinline__ void cmac_grid(float2& acc, const float2 a, const float2 b)
+{
+    if (kReal) {
+        cmac<true>(acc, a, b);
+    } else {
+        acc.x = fmaf(a.x, b.x, acc.x);
+        acc.y = fmaf(a.y, b.x, acc.y);
+        acc.x = fmaf(-a.y, b.y, acc.x);
+        acc.y = fmaf(a.x, b.y, acc.y);
+    }
+}
+
 // CTAs per SM the register budget of a tile kernel is sized for: kR accumulators (gridding) or
 // grid values (degridding) per lane, two floats each.
 template <class Tab, int kR>
@@ -384,15 +402,15 @@ degrid_tile_kernel(const typename Tab::elem* __restrict__ ctab,
                         if (colok) {
 #pragma unroll
                             for (int r = 0; r < kR; r += 2) {
-                                cmac<Tab::kReal>(p0, gv[r], Tab::load(ctab + (ci + r * s)));
-                                cmac<Tab::kReal>(p1, gv[r + 1], Tab::load(ctab + (ci + (r + 1) * s)));
+                                cmac_grid<Tab::kReal>(p0, gv[r], Tab::load(ctab + (ci + r * s)));
+                                cmac_grid<Tab::kReal>(p1, gv[r + 1], Tab::load(ctab + (ci + (r + 1) * s)));
                             }
                         }
                     } else {
 #pragma unroll
                         for (int r = 0; r < kR; ++r) {
                             if (colok && unsigned(dy0 + r) < unsigned(s))
-                                cmac<Tab::kReal>((r & 1) ? p1 : p0, gv[r], Tab::load(ctab + (ci + r * s)));
+                                cmac_grid<Tab::kReal>((r & 1) ? p1 : p0, gv[r], Tab::load(ctab + (ci + r * s)));
                         }
                     }
                     v[e] = __fadd2_rn(p0, p1);
