@@ -475,8 +475,21 @@ fold_kernel(const u32* __restrict__ items, const u32* __restrict__ group_start, 
         {
             const int p = int(w % kSlices) * kTileThreads + threadIdx.x;
             const int gx = rec_tx(ti) * kTileW + (p % kTileW), gy = rec_ty(ti) * kTH + (p / kTileW);
+            const bool inside = gx < gs && gy < gs;
+            float2* gp = grid + (inside ? (unsigned long long)(gy) * gs + gx : 0ull);
+            const float2 g0 = inside ? *gp : make_float2(0.f, 0.f);  // in flight with the partials
             float2 v = pt[p];
             u32 q = 1;
+            for (; q + 8 <= nu; q += 8) {  // eight loads in flight, added in unit order
+                float2 w8[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) w8[e] = pt[(unsigned long long)(q + e) * kPoints + p];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    v.x += w8[e].x;
+                    v.y += w8[e].y;
+                }
+            }
             for (; q + 4 <= nu; q += 4) {  // four loads in flight, added in unit order
                 float2 w4[4];
 #pragma unroll
@@ -492,9 +505,8 @@ fold_kernel(const u32* __restrict__ items, const u32* __restrict__ group_start, 
                 v.x += w1.x;
                 v.y += w1.y;
             }
-            if (gx < gs && gy < gs) {
-                float2* gp = grid + ((unsigned long long)(gy) * gs + gx);
-                float2 o = *gp;
+            if (inside) {
+                float2 o = g0;
                 o.x += v.x;
                 o.y += v.y;
                 *gp = o;
