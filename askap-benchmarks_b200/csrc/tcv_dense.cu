@@ -132,17 +132,6 @@ __device__ __forceinline__ void dchunk_load(DChunk& c, u32 it, u32 i1, const uin
         c.m = int(c.cnt < u32(kChunk) ? c.cnt : u32(kChunk));
     }
 }
-template <int kChunk>
-__device__ __forceinline__ void dchunk_next(DChunk& c, u32 i1, const uint4* __restrict__ units, const GridArgs& a)
-{
-    if (c.base + u32(kChunk) < c.cnt) {
-        c.base += u32(kChunk);
-        const u32 left = c.cnt - c.base;
-        c.m = int(left < u32(kChunk) ? left : u32(kChunk));
-    } else {
-        dchunk_load<kChunk>(c, c.it + gridDim.x, i1, units, a);
-    }
-}
 
 // the named barrier of one tile half's four gridding warps (barrier 0 is the CTA's)
 __device__ __forceinline__ void half_barrier(int half)
@@ -366,9 +355,45 @@ dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int4* __r
     __shared__ DenseRec rec[2][kDThreads];
     __shared__ unsigned long long rslot[2][kDThreads];  // slot index of (sample, this tile)
     __shared__ DenseLut L;
+    // Work units are handed out by a counter (a.sched[0]) as CTAs finish their last, one unit
+    // ahead: sm_unit[q] is the CTA's next unit, drawn by thread 0 when the unit before it
+    // started (the units' work differs by the footprint widths, up to 121² against 7² updates per
+    // sample, which a fixed share per CTA left as a tail).  The CTA that draws past the end last
+    // (a.sched[1] counts them) sets both counters to zero again.  Which CTA takes a unit changes
+    // no sum: every unit writes its own samples' slots.
+    __shared__ u32 sm_unit[3];  // two unit slots, and the group's first unit
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 i1 = group_ustart[a.group + 1];
+    auto fetch = [&]() -> u32 {  // thread 0 only
+        const u32 v = sm_unit[2] + atomicAdd(a.sched, 1u);
+        if (v >= i1 && atomicAdd(a.sched + 1, 1u) == gridDim.x - 1u) {
+            atomicExch(a.sched, 0u);
+            atomicExch(a.sched + 1, 0u);
+        }
+        return v;
+    };
+    if (threadIdx.x == 0) {
+        sm_unit[2] = group_ustart[a.group];
+        const u32 v = fetch();
+        sm_unit[0] = v;
+        sm_unit[1] = v < i1 ? fetch() : v;  // no draw after the first past the end
+    }
     build_lut(L, threadIdx.x, kDThreads);
-    __syncthreads();  // the lane table is built (the staging reads it)
+    __syncthreads();  // the lane table is built (the staging reads it); the first units are drawn
+    int q = 1;        // slot of the next unit (uniform)
+    auto next_chunk = [&](DChunk& c) {
+        if (c.base + u32(kDThreads) < c.cnt) {
+            c.base += u32(kDThreads);
+            const u32 left = c.cnt - c.base;
+            c.m = int(left < u32(kDThreads) ? left : u32(kDThreads));
+        } else {
+            // the slot was written before the last barrier; the other slot was last read before it
+            const u32 v = sm_unit[q];
+            if (threadIdx.x == 0 && v < i1) sm_unit[q ^ 1] = fetch();
+            q ^= 1;
+            dchunk_load<kDThreads>(c, v, i1, units, a);
+        }
+    };
     auto stage = [&](const DChunk& c, int buf) {
         if (int(threadIdx.x) < c.m) {
             const u32 pos = c.start + c.base + threadIdx.x;
@@ -417,16 +442,15 @@ dense_degrid_kernel(const typename Tab::elem* __restrict__ ctab, const int4* __r
         }
         return make_float2(p0.x + p1.x, p0.y + p1.y);
     };
-    const u32 i1 = group_ustart[a.group + 1];
     DChunk cur;
-    dchunk_load<kDThreads>(cur, group_ustart[a.group] + blockIdx.x, i1, units, a);
+    dchunk_load<kDThreads>(cur, sm_unit[0], i1, units, a);
     stage(cur, 0);
     if (cur.m > 0) load_tile(cur.ti);
-    __syncthreads();
+    __syncthreads();  // slot 0 is read before thread 0 can draw into it again
     int buf = 0;
     while (cur.m > 0) {
         DChunk nxt = cur;
-        dchunk_next<kDThreads>(nxt, i1, units, a);
+        next_chunk(nxt);
         stage(nxt, buf ^ 1);  // the next chunk, while this one is read
         for (int g0 = warp * 4; g0 < cur.m; g0 += kDWarps * 4) {
             float2 v[4];
