@@ -154,7 +154,8 @@ __device__ __forceinline__ void half_barrier(int half)
 // copies in warp order into the grid or the unit's partial tile.
 template <class Tab>
 __global__ void __launch_bounds__(kGThreads, 3)
-dense_grid_kernel(const float2* __restrict__ data, const u32* __restrict__ order, const typename Tab::elem* __restrict__ ctab,
+dense_grid_kernel(const float2* __restrict__ data, const u32* __restrict__ order,
+                  const typename Tab::elem* __restrict__ ctab,
                   const int4* __restrict__ grec, const uint4* __restrict__ units,
                   const u32* __restrict__ group_ustart, GridArgs a)
 {
