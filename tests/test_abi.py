@@ -123,6 +123,16 @@ def test_workspace_grows_with_samples(tcv):
     assert b < 64 << 20
 
 
+def test_static_scratch_limit_is_the_documented_one(tcv):
+    """The allocation-free entry's limit that the header states (n <= 269,745 samples of a 129 x 129
+    footprint on a 4096 grid with the 33-plane table) is the one tcv_plan_workspace_bytes gives."""
+    L = tcv.lib()
+    limit = L.tcv_static_scratch_bytes()
+    assert limit == 64 << 20
+    assert L.tcv_plan_workspace_bytes(269745, 64, 4096, 35145792) <= limit
+    assert L.tcv_plan_workspace_bytes(269746, 64, 4096, 35145792) > limit
+
+
 def test_batch_argument_validation(tcv):
     """Batched plans, tuning and graphs: invalid arguments are refused on the host."""
     from tconvolve._lib import TcvJob, TcvTuning
